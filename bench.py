@@ -1,0 +1,456 @@
+"""Benchmark of the cone-beam OS-MOM hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+
+Workload (default, c2): OS-MOM reconstruction (osMOMSolverD semantics,
+positivity, no regulariser) of a 256^3 seeded ellipsoid phantom from 360
+views over 360 degrees on a 512x384 detector at 0.8 mm with an 80 mm half-fan
+offset, Poisson noise at I0 = 1e5, log transform; 10 subsets, 20 iterations,
+FP32.  Voxel size 1 mm and SAD/SDD = 1000/1500 mm are assumptions (the
+workload does not state them).  A step is one full reconstruction
+(preconditioner + 20 x 10 subset steps).
+
+value  = GUPS: (forward ray samples + back-projection voxel-view updates) per
+         second, all ranks, device-timed with CUDA events, inputs resident.
+e2e    = the same metric through the public API with host buffers: each step
+         copies the measured projections host->device (pinned) and the
+         reconstruction device->host inside the timed region.
+N > 1  = independent replicas (one reconstruction per GPU, no collective),
+         weak scaling; time is the max over ranks.
+--impl reference times the reference algorithm's CPU restatement (the oracle,
+FP32, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
+
+
+def _package():
+    name = "gt_tomography_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "gt-tomography_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ------------------------------------------------------------------ workload
+class Workload:
+    def __init__(self, name: str):
+        self.name = name
+        if name == "c2":
+            self.n = (256, 256, 256)
+            self.voxel = 1.0
+            self.P = 360
+            self.W, self.H, self.pitch = 512, 384, 0.8
+            self.offset = 80.0
+            self.S, self.iters = 10, 20
+            self.I0 = 1e5
+            self.n_ell = 10
+        elif name == "c1":
+            self.n = (128, 128, 128)
+            self.voxel = 1.0
+            self.P = 180
+            self.W, self.H, self.pitch = 256, 192, 1.5
+            self.offset = 0.0
+            self.S, self.iters = 1, 0
+            self.I0 = 0
+            self.n_ell = 10
+        else:
+            raise ValueError(name)
+        self.SAD, self.SDD = 1000.0, 1500.0
+        self.L = tuple(v * self.voxel for v in self.n)
+        self.spp = 1.5
+        self.Nsamp = int(np.float32(self.spp) * np.float32(self.n[0]))
+        self.seed = 1234
+
+    def config(self):
+        if self.name == "c2":
+            wl = (f"osmom {self.n[0]}^3 from {self.P} views {self.W}x{self.H}@{self.pitch}mm, "
+                  f"offset {self.offset:g}mm, {self.S} subsets x {self.iters} iterations, fp32")
+        else:
+            wl = (f"forward + FDK {self.n[0]}^3 from {self.P} views {self.W}x{self.H}@{self.pitch}mm, "
+                  "Hann ramp, fp32")
+        return {
+            "workload": wl,
+            "volume": list(self.n), "voxel_mm": self.voxel, "views": self.P, "detector": [self.W, self.H],
+            "pixel_mm": self.pitch, "offset_mm": self.offset, "SAD_mm": self.SAD, "SDD_mm": self.SDD,
+            "subsets": self.S, "iterations": self.iters, "I0": self.I0, "samples_per_ray": self.Nsamp,
+            "ellipsoids": self.n_ell, "seed": self.seed, "storage": "fp32",
+            "assumed": ["voxel_mm", "SAD_mm", "SDD_mm"],
+            "step": "one full reconstruction" if self.name == "c2" else "one forward pass + one FDK",
+            "l2": "flushed between steps (256 MiB write); projections exceed L2",
+            "parallelism": "replicas",
+        }
+
+    def geometry(self, gtb):
+        return gtb._lib.CbctGeometry(self.SAD, self.SDD, self.W * self.pitch, self.H * self.pitch, self.W, self.H,
+                                     *self.n, *self.L, self.spp)
+
+    def updates_per_step(self):
+        """(forward samples, back-projection voxel-view updates) per step."""
+        rays = self.W * self.H * self.P
+        nvox = self.n[0] * self.n[1] * self.n[2]
+        if self.name == "c2":
+            passes = self.iters + 1      # + preconditioner A^T A 1
+            return rays * self.Nsamp * passes, nvox * self.P * passes
+        return rays * self.Nsamp, nvox * self.P
+
+    def launches_per_step(self):
+        if self.name == "c2":
+            # fill + S forward + 1 back-projection (preconditioner), then per subset
+            # step: forward-residual, norm finalise, back-projection with the update.
+            return 1 + self.S + 1 + self.iters * self.S * 3
+        return 1 + 1 + 1            # forward, FDK filter, FDK back-projection
+
+
+def make_inputs(wl: Workload, gtb, dev):
+    """Seeded phantom, exact line integrals on the device, Poisson noise, log."""
+    import torch
+    ang = gtb.phantom.circular_orbit(wl.P)
+    off = np.tile(np.array([[wl.offset, 0.0]], np.float32), (wl.P, 1))
+    ell = gtb.phantom.ellipsoids(wl.seed, wl.L, n=wl.n_ell)
+    order, sizes = gtb.subset_partition(wl.P, wl.S)
+    a, o = ang[order] - ang.min(), off[order]
+    g = wl.geometry(gtb)
+    fw = float(wl.W * wl.pitch)
+    oc = [int(abs(float(o[f:f + n, 0].mean())) > 0.1 * fw) if n else 0
+          for f, n in zip(np.concatenate([[0], np.cumsum(sizes)[:-1]]), sizes)]
+    plan = gtb.Plan(g, a, o, sizes, oc)
+    ell_d = torch.from_numpy(ell.reshape(-1)).to(dev)
+    exact = torch.empty(plan.proj_shape(), dtype=torch.float32, device=dev)
+    plan.phantom_project(ell_d, exact)
+    b = gtb.phantom.poisson_log(exact, wl.I0, wl.seed + 1) if wl.I0 else exact
+    torch.cuda.synchronize()
+    return plan, b.contiguous(), ell_d, (a, o, sizes, oc)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"cbct_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ helpers
+def peaks():
+    try:
+        d = json.load(open(PEAKS_PATH))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_for(kernel: str, workload: str):
+    try:
+        d = json.load(open(TRAFFIC_PATH))
+        return d.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)
+
+
+def dist_setup(n_gpus: int):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(v: float, world: int):
+    import torch
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample(wl: Workload, budget_s: float = 6.0):
+    """The reference algorithm's CPU restatement (oracle, FP32, all host threads)
+    on a bounded sample: forward + back-projection of k views of the workload."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_num_threads(threads)
+    g = O.Geometry(*wl.n, *wl.L, wl.W, wl.H, wl.W * wl.pitch, wl.H * wl.pitch, wl.SAD, wl.SDD)
+    rng = np.random.default_rng(0)
+    vol = rng.uniform(0, 0.02, wl.n[::-1]).astype(np.float32)
+    ang = np.arange(wl.P, dtype=np.float32) * (360.0 / wl.P)
+    off = np.tile(np.array([[wl.offset, 0.0]], np.float32), (wl.P, 1))
+
+    def run(k):
+        t0 = time.perf_counter()
+        p = O.forward(g, vol, ang[:k], off[:k], spp=wl.spp, dtype=np.float32)
+        O.backproject(g, p, ang[:k], off[:k], dtype=np.float32)
+        return time.perf_counter() - t0
+
+    t1 = run(1)
+    k = int(max(1, min(wl.P, budget_s / max(t1, 1e-3))))
+    return O, g, vol, ang, off, k, threads, run
+
+
+def cpu_gups(wl, k, t):
+    rays = wl.W * wl.H * k
+    nvox = wl.n[0] * wl.n[1] * wl.n[2]
+    return (rays * wl.Nsamp + nvox * k) / t / 1e9
+
+
+def reference_arm(args, wl: Workload):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    O, g, vol, ang, off, k, threads, run = cpu_sample(wl, budget_s=4.0)
+    for _ in range(args.warmup):
+        run(k)
+    times = [run(k) for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    v = cpu_gups(wl, k, t)
+    sample = f"forward + back-projection of {k} of {wl.P} views per step (oracle port, fp32)"
+    line = {
+        "metric": "GUPS fwd+back projection (OS-MOM reconstruction)", "value": round(v, 4), "unit": "GUPS",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": wl.config(),
+        "cpu_baseline": {"value": round(v, 4), "unit": "GUPS", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 4), "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def ours(args, wl: Workload):
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    gtb = _package()
+    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev)
+    nvox = wl.n[0] * wl.n[1] * wl.n[2]
+    z = torch.empty(plan.vol_shape, dtype=torch.float32, device=dev)
+    resid = torch.zeros(max(wl.iters * wl.S, 1), dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    filt = gtb.hann_ramp_filter(wl.W)
+
+    def step():
+        if wl.name == "c2":
+            plan.osmom(b, z, None, wl.iters, nonneg=True, use_graph=True, resid=resid)
+        else:
+            tmp = proj_tmp
+            plan.forward(vol_c1, tmp)
+            plan.fdk(b, z, filt, 0)
+
+    if wl.name == "c1":
+        vol_c1 = torch.empty(plan.vol_shape, dtype=torch.float32, device=dev)
+        gtb.phantom_voxelize(wl.geometry(gtb), ell_d, vol_c1, 4)
+        proj_tmp = torch.empty_like(b)
+
+    # ---- device-timed region (inputs resident)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = []
+    barrier(world)
+    for _ in range(args.steps):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(sum(times) / len(times), world)
+    fs, bv = wl.updates_per_step()
+    gups = (fs + bv) * world / (ms * 1e-3) / 1e9
+
+    # ---- end-to-end through the public API with host buffers
+    b_host = b.cpu().pin_memory()
+    z_host = torch.empty(plan.vol_shape, dtype=torch.float32).pin_memory()
+    b_dev = torch.empty_like(b)
+    e2e_times = []
+
+    def e2e_step():
+        b_dev.copy_(b_host, non_blocking=True)
+        if wl.name == "c2":
+            plan.osmom(b_dev, z, None, wl.iters, nonneg=True, use_graph=True, resid=resid)
+        else:
+            plan.forward(vol_c1, proj_tmp)
+            plan.fdk(b_dev, z, filt, 0)
+        z_host.copy_(z, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    for _ in range(args.steps):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    barrier(world)
+    ms_e2e = max_over_ranks(sum(e2e_times) / len(e2e_times), world)
+    gups_e2e = (fs + bv) * world / (ms_e2e * 1e-3) / 1e9
+
+    # ---- dominant kernel: forward residual of one subset, timed alone
+    s0 = 0
+    n0 = int(sizes[s0])
+    r = torch.empty(plan.proj_shape(s0), dtype=torch.float32, device=dev)
+    bs = b[:n0]
+    n2 = torch.zeros(1, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        plan.forward_residual(z, bs, r, s0, 1.0, bool(oc[s0]), n2)
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        plan.forward_residual(z, bs, r, s0, 1.0, bool(oc[s0]), None)
+    e1.record(stream)
+    e1.synchronize()
+    t_fwd = e0.elapsed_time(e1) / reps * 1e-3
+    rays0 = wl.W * wl.H * n0
+    alg_bytes = 4 * nvox + 4 * rays0 * 3        # volume + b read + r write (+ per-pixel offset weight computed)
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / t_fwd / 1e9
+    samples_s = rays0 * wl.Nsamp / t_fwd
+
+    line = {
+        "metric": "GUPS fwd+back projection (OS-MOM reconstruction)",
+        "value": round(gups, 3), "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": wl.config(),
+        "recon_per_s": round(world * 1e3 / ms, 4) if wl.name == "c2" else None,
+        "e2e": {"value": round(gups_e2e, 3), "unit": "GUPS", "ms_per_step": round(ms_e2e, 3),
+                "h2d_bytes_per_step": int(b.numel() * 4), "d2h_bytes_per_step": int(nvox * 4)},
+        "roofline": {"bound": "hbm", "kernel": "fwd_slab_kernel (forward residual, one subset)",
+                     "achieved": round(achieved, 2), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 5), "traffic": traffic_for("forward_residual", wl.name),
+                     "launch_ms": round(t_fwd * 1e3, 4), "alg_bytes_per_launch": alg_bytes,
+                     "gsamples_per_s": round(samples_s / 1e9, 2),
+                     "note": "gather/issue-bound kernel: HBM fraction of compulsory bytes is small by design"},
+        "gpu_launches": wl.launches_per_step() * args.steps,
+        "forward_variant": plan.forward_variant(),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            O, g, vol, ang, off, k, threads, run = cpu_sample(wl, budget_s=8.0)
+            t = run(k)
+            line["cpu_baseline"] = {"value": round(cpu_gups(wl, k, t), 4), "unit": "GUPS", "cores": threads,
+                                    "kind": "port",
+                                    "sample": f"forward + back-projection of {k} of {wl.P} views (oracle, fp32)"}
+            # accuracy of the FP32 device path against the FP64 oracle at full size (2 views)
+            pl2 = gtb.Plan(wl.geometry(gtb), ang[:2], off[:2])
+            vt = torch.from_numpy(vol).to(dev)
+            pg = torch.empty(pl2.proj_shape(), dtype=torch.float32, device=dev)
+            pl2.forward(vt, pg)
+            ref = O.forward(g, vol.astype(np.float64), ang[:2], off[:2], spp=wl.spp)
+            bg = torch.empty(pl2.vol_shape, dtype=torch.float32, device=dev)
+            pl2.backproject(torch.from_numpy(ref.astype(np.float32)).to(dev), bg, -1, 0, False)
+            refb = O.backproject(g, ref, ang[:2], off[:2])
+            line["rel_l2_vs_fp64"] = {"forward_2views": O.rel_l2(pg.cpu().numpy(), ref),
+                                      "backproject_2views": O.rel_l2(bg.cpu().numpy(), refb)}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "GUPS", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    wl = Workload(args.config)
+    if args.impl == "reference":
+        reference_arm(args, wl)
+    else:
+        ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,525 @@
+// abi.cu -- C ABI of the B200 cone-beam library (declared in include/cbct.h).
+//
+// Every entry point converts internal exceptions into a cbct_status and a
+// thread-local message; nothing throws across the boundary.  Host-side setup
+// logic restates the reference's operator setup (cited per function).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+
+#include "device_common.cuh"
+
+namespace cbct {
+
+void fdk_state_free(cbct_plan* p);
+void graph_cache_free(cbct_plan* p);
+void fill_launch(float* x, size_t n, float v, cudaStream_t st);
+void convert_launch(const float* src, void* dst, size_t n, cbct_dtype dt, cudaStream_t st);
+void backproject_recip_launch(cbct_plan* p, int s, const float* proj, float* out, cudaStream_t st);
+void osmom_solve(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+                 double* resid, cudaStream_t st);
+void ossart_solve(cbct_plan* p, const float* b, const float* x0, float* x, const cbct_solver_params& prm,
+                  double* cost, cudaStream_t st);
+void fdk_run(cbct_plan* p, const float* proj, float* vol, const float* filter, uint32_t flags, float* work,
+             cudaStream_t st);
+void phantom_voxelize_launch(const GridConst& gc, const float* ell, int K, int ss, float* vol, cudaStream_t st);
+void phantom_project_launch(cbct_plan* p, int s, const float* ell, int K, float* proj, cudaStream_t st);
+
+static thread_local std::string g_last_error;
+
+void ensure_smem_attr(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  CBCT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = done[{dev, func}];
+  if (cur >= bytes) return;
+  CBCT_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  });
+  if (!fn) throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+// hoCuConebeamProjectionOperator::compute_default_frequency_filter
+// (hoCuConebeamProjectionOperator.cpp:26-62): Guo et al. filter on W+1 bins,
+// evaluated in float, normalised to an absolute sum of W+1.
+void default_filter(int W, float* out) {
+  const int K = W + 1;
+  const float A2 = float(0.2 * double(K) * double(K));
+  double sum = 0.0;
+  for (int i = 0; i < K; ++i) {
+    const float k = float(i);
+    out[i] = (k * k < A2) ? k * A2 / (A2 - k * k) * std::exp(-A2 / (A2 - k * k)) : 0.f;
+    sum += std::fabs(double(out[i]));
+  }
+  for (int i = 0; i < K; ++i) out[i] = float(double(out[i]) * (double(K) / sum));
+}
+
+// CBSubsetOperator<ARRAY>::setup, CBSubsetOperator.cpp:66-104.
+void subset_partition(int n_views, const int* view_bin, int n_subsets, int* order, int* sizes, int* n_out) {
+  std::map<unsigned, unsigned> bins;
+  for (int i = 0; i < n_views; ++i) {
+    const int b = view_bin ? view_bin[i] : 0;
+    if (b >= 0) bins[(unsigned)i] = (unsigned)b;
+  }
+  std::vector<std::vector<unsigned>> sub(n_subsets);
+  int k = 0;
+  for (int i = 0; i < n_views; ++i)
+    if (bins.find((unsigned)i) != bins.end()) sub[k++ % n_subsets].push_back((unsigned)i);
+  for (auto& s : sub)
+    std::sort(s.begin(), s.end(), [&](unsigned a, unsigned b) { return bins[a] < bins[b]; });
+  int n = 0;
+  for (int s = 0; s < n_subsets; ++s) {
+    sizes[s] = (int)sub[s].size();
+    for (unsigned v : sub[s]) order[n++] = (int)v;
+  }
+  *n_out = n;
+}
+
+static void validate_geometry(const cbct_geometry* g) {
+  CBCT_REQUIRE(g != nullptr, "geometry is NULL");
+  CBCT_REQUIRE(g->width > 0 && g->height > 0, "detector size must be positive");
+  CBCT_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0, "volume size must be positive");
+  CBCT_REQUIRE(g->lx > 0 && g->ly > 0 && g->lz > 0, "volume size in mm must be positive");
+  CBCT_REQUIRE(g->fov_u > 0 && g->fov_v > 0, "detector size in mm must be positive");
+  CBCT_REQUIRE(g->SAD > 0 && g->SDD > g->SAD, "need 0 < SAD < SDD");
+  CBCT_REQUIRE(g->samples_per_pixel > 0, "samples_per_pixel must be positive");
+  CBCT_REQUIRE((long)(g->samples_per_pixel * float(g->nx)) >= 1, "fewer than one sample per ray");
+}
+
+static GridConst make_grid(const cbct_geometry& g) {
+  GridConst c{};
+  c.nx = g.nx; c.ny = g.ny; c.nz = g.nz;
+  c.W = g.width; c.H = g.height;
+  c.N = (int)(g.samples_per_pixel * float(g.nx));  // conebeam_projection.cu:625
+  c.hx = g.lx * 0.5f; c.hy = g.ly * 0.5f; c.hz = g.lz * 0.5f;
+  c.kx = float(double(g.nx) / g.lx); c.ky = float(double(g.ny) / g.ly); c.kz = float(double(g.nz) / g.lz);
+  c.bx = g.nx * 0.5f - 0.5f; c.by = g.ny * 0.5f - 0.5f; c.bz = g.nz * 0.5f - 0.5f;
+  c.vx = float(double(g.lx) / g.nx); c.vy = float(double(g.ly) / g.ny); c.vz = float(double(g.lz) / g.nz);
+  c.SAD = g.SAD; c.SDD = g.SDD;
+  c.fov_u = g.fov_u; c.fov_v = g.fov_v;
+  c.ku = float(double(g.width) / g.fov_u); c.kv = float(double(g.height) / g.fov_v);
+  c.bu = g.width * 0.5f - 0.5f; c.bv = g.height * 0.5f - 0.5f;
+  c.invN = 1.f / float(c.N);
+  return c;
+}
+
+// Per-view constants in FP64 (conebeam_projection.cu:441-473 restated so the
+// detector point is affine in the pixel indices).
+static ViewParams make_view(const cbct_geometry& g, double angle_deg, double ox, double oy) {
+  const double pi = 3.14159265358979323846;
+  const double th = angle_deg * (pi / 180.0);
+  const double cs = std::cos(th), sn = std::sin(th);
+  const double SAD = g.SAD, SDD = g.SDD, ADD = SDD - SAD;
+  const double du = double(g.fov_u) / g.width, dv = double(g.fov_v) / g.height;
+  const double q0 = (0.5 / g.width - 0.5) * g.fov_u + ox;
+  const double r0 = (0.5 / g.height - 0.5) * g.fov_v + oy;
+  const double Sx = SAD * sn, Sy = -SAD * cs;
+  ViewParams v{};
+  v.cs = float(cs); v.sn = float(sn);
+  v.Sx = float(Sx); v.Sy = float(Sy);
+  v.D0x = float(cs * q0 - sn * ADD - Sx);
+  v.D0y = float(sn * q0 + cs * ADD - Sy);
+  v.D0z = float(r0);
+  v.Eux = float(cs * du); v.Euy = float(sn * du);
+  v.Evz = float(dv);
+  v.ox = float(ox); v.oy = float(oy);
+  // central ray direction is R (0,1,0) = (-sn, cs, 0)
+  if (std::fabs(cs) >= std::fabs(sn)) { v.dom = 1; v.dsgn = cs >= 0 ? 1 : -1; }
+  else { v.dom = 0; v.dsgn = -sn >= 0 ? 1 : -1; }
+  return v;
+}
+
+static void plan_free(cbct_plan* p) {
+  if (!p) return;
+  fdk_state_free(p);
+  graph_cache_free(p);
+  cudaFree(p->d_views);
+  cudaFree(p->d_proj_scratch);
+  cudaFree(p->d_partials);
+  cudaFree(p->d_flags);
+  cudaFree(p->d_fdk_work);
+  cudaFree(p->ws);
+  delete p;
+}
+
+static cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float* offsets, int n_views,
+                              const int* subset_sizes, int n_subsets, const int* offcorr) {
+  validate_geometry(g);
+  CBCT_REQUIRE(n_views > 0, "n_views must be positive");
+  CBCT_REQUIRE(angles && offsets, "angles/offsets are NULL");
+  CBCT_REQUIRE(n_subsets >= 1, "n_subsets must be >= 1");
+  CBCT_REQUIRE(n_subsets == 1 || subset_sizes, "subset_sizes is NULL with several subsets");
+  std::unique_ptr<cbct_plan, void (*)(cbct_plan*)> p(new cbct_plan(), plan_free);
+  p->g = *g;
+  p->gc = make_grid(*g);
+  p->n_views = n_views;
+  p->n_subsets = n_subsets;
+  int acc = 0;
+  for (int s = 0; s < n_subsets; ++s) {
+    const int c = subset_sizes ? subset_sizes[s] : n_views;
+    CBCT_REQUIRE(c >= 0, "negative subset size");
+    p->first.push_back(acc);
+    p->count.push_back(c);
+    p->offcorr.push_back(offcorr ? (offcorr[s] != 0) : 0);
+    acc += c;
+    p->max_subset = std::max(p->max_subset, c);
+  }
+  CBCT_REQUIRE(acc == n_views, "subset sizes do not sum to n_views");
+  // index n_subsets addresses every view
+  p->first.push_back(0);
+  p->count.push_back(n_views);
+  p->offcorr.push_back(0);
+  p->angles.assign(angles, angles + n_views);
+  p->offsets.assign(offsets, offsets + 2 * (size_t)n_views);
+  for (int i = 0; i < n_views; ++i) {
+    CBCT_REQUIRE(std::isfinite(angles[i]) && std::isfinite(offsets[2 * i]) && std::isfinite(offsets[2 * i + 1]),
+                 "non-finite angle or offset");
+    p->hviews.push_back(make_view(*g, angles[i], offsets[2 * i], offsets[2 * i + 1]));
+  }
+  CBCT_CUDA(cudaGetDevice(&p->device));
+  CBCT_CUDA(cudaMalloc(&p->d_views, sizeof(ViewParams) * n_views));
+  CBCT_CUDA(cudaMemcpy(p->d_views, p->hviews.data(), sizeof(ViewParams) * n_views, cudaMemcpyHostToDevice));
+  const size_t tiles = (size_t)((g->width + kTU - 1) / kTU) * ((g->height + kTV - 1) / kTV);
+  p->n_partials = std::max<size_t>(tiles * n_views, 148 * 4);
+  CBCT_CUDA(cudaMalloc(&p->d_partials, sizeof(double) * p->n_partials));
+  CBCT_CUDA(cudaMalloc(&p->d_flags, sizeof(int) * 4));
+  CBCT_CUDA(cudaMemset(p->d_flags, 0, sizeof(int) * 4));
+  forward_choose_variant(p.get());
+  forward_prepare(p.get());
+  backproject_prepare(p.get());
+  return p.release();
+}
+
+static int subset_index(const cbct_plan* p, int s) {
+  CBCT_REQUIRE(p != nullptr, "plan is NULL");
+  CBCT_REQUIRE(s >= -1 && s < p->n_subsets, "subset index out of range");
+  return s < 0 ? p->n_subsets : s;
+}
+
+static float* proj_scratch(cbct_plan* p, size_t elems) {
+  if (p->proj_scratch_elems < elems) {
+    cudaFree(p->d_proj_scratch);
+    p->d_proj_scratch = nullptr;
+    p->proj_scratch_elems = 0;
+    CBCT_CUDA(cudaMalloc(&p->d_proj_scratch, elems * sizeof(float)));
+    p->proj_scratch_elems = elems;
+  }
+  return p->d_proj_scratch;
+}
+
+template <class F>
+cbct_status guard(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return CBCT_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return CBCT_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return CBCT_ERR_INTERNAL;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return CBCT_ERR_INTERNAL;
+  }
+}
+
+static cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace cbct
+
+using namespace cbct;
+
+extern "C" {
+
+const char* cbct_status_string(cbct_status s) {
+  switch (s) {
+    case CBCT_OK: return "CBCT_OK";
+    case CBCT_ERR_INVALID_ARGUMENT: return "CBCT_ERR_INVALID_ARGUMENT";
+    case CBCT_ERR_CUDA: return "CBCT_ERR_CUDA";
+    case CBCT_ERR_OUT_OF_MEMORY: return "CBCT_ERR_OUT_OF_MEMORY";
+    case CBCT_ERR_UNSUPPORTED: return "CBCT_ERR_UNSUPPORTED";
+    case CBCT_ERR_DEVICE_CHECK: return "CBCT_ERR_DEVICE_CHECK";
+    case CBCT_ERR_TIMEOUT: return "CBCT_ERR_TIMEOUT";
+    case CBCT_ERR_BUDGET: return "CBCT_ERR_BUDGET";
+    case CBCT_ERR_CANCELLED: return "CBCT_ERR_CANCELLED";
+    case CBCT_ERR_INTERNAL: return "CBCT_ERR_INTERNAL";
+  }
+  return "CBCT_ERR_UNKNOWN";
+}
+
+const char* cbct_last_error(void) { return g_last_error.c_str(); }
+const char* cbct_version(void) { return "gt-tomography_b200 0.1 (sm_100a)"; }
+
+cbct_status cbct_subset_partition(int32_t n_views, const int32_t* view_bin, int32_t n_subsets, int32_t* order_out,
+                                  int32_t* subset_sizes_out, int32_t* n_out) {
+  return guard([&] {
+    CBCT_REQUIRE(n_views >= 0 && n_subsets >= 1, "bad sizes");
+    CBCT_REQUIRE(order_out && subset_sizes_out && n_out, "NULL output");
+    subset_partition(n_views, view_bin, n_subsets, order_out, subset_sizes_out, n_out);
+  });
+}
+
+cbct_status cbct_default_frequency_filter(int32_t W, float* out) {
+  return guard([&] {
+    CBCT_REQUIRE(W > 0 && out, "bad arguments");
+    default_filter(W, out);
+  });
+}
+
+cbct_status cbct_cosine_weights(const cbct_geometry* g, float* out) {
+  return guard([&] {
+    validate_geometry(g);
+    CBCT_REQUIRE(out, "NULL output");
+    const double SAD = g->SAD, SDD = g->SDD;
+    for (int y = 0; y < g->height; ++y)
+      for (int x = 0; x < g->width; ++x) {
+        const double xx = (double(x) / g->width - 0.5) * g->fov_u, yy = (double(y) / g->height - 0.5) * g->fov_v;
+        const double s = SAD * xx / SDD, v = SAD * yy / SDD;
+        out[(size_t)y * g->width + x] = float(SAD / std::sqrt(SAD * SAD + s * s + v * v));
+      }
+  });
+}
+
+cbct_status cbct_is_short_scan(const cbct_geometry* g, const float* angles, int32_t n, int32_t* out) {
+  return guard([&] {
+    CBCT_REQUIRE(g && angles && out && n > 0, "bad arguments");
+    const float span = *std::max_element(angles, angles + n);
+    const float delta = std::atan(g->fov_u / (2.0f * g->SDD));
+    const float pi = 3.14159265358979f;
+    *out = (span * pi / 180.0f > pi + 3.0f * delta) ? 0 : 1;
+  });
+}
+
+cbct_status cbct_offset_override(const cbct_geometry* g, const float* offsets, int32_t n, int32_t* out) {
+  return guard([&] {
+    CBCT_REQUIRE(g && offsets && out && n > 0, "bad arguments");
+    float mx = 0.f;
+    for (int i = 0; i < n; ++i) mx += offsets[2 * i];
+    mx /= float(n);
+    *out = std::fabs(mx) > g->fov_u * 0.1f ? 1 : 0;
+  });
+}
+
+cbct_status cbct_plan_create(const cbct_geometry* g, const float* angles_deg, const float* offsets_xy,
+                             int32_t n_views, const int32_t* subset_sizes, int32_t n_subsets,
+                             const int32_t* offset_correction, cbct_plan** plan_out) {
+  return guard([&] {
+    CBCT_REQUIRE(plan_out, "plan_out is NULL");
+    *plan_out = nullptr;
+    *plan_out = plan_create(g, angles_deg, offsets_xy, n_views, subset_sizes, n_subsets, offset_correction);
+  });
+}
+
+cbct_status cbct_plan_destroy(cbct_plan* plan) {
+  return guard([&] { plan_free(plan); });
+}
+
+cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_out, int32_t* count_out) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    if (first_out) *first_out = plan->first[i];
+    if (count_out) *count_out = plan->count[i];
+  });
+}
+
+const char* cbct_plan_forward_variant(const cbct_plan* plan) {
+  if (!plan) return "";
+  return plan->fwd_variant == 1 ? "tma-slab" : "gather";
+}
+
+cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value) {
+  return guard([&] {
+    CBCT_REQUIRE(plan, "plan is NULL");
+    if (option == CBCT_OPT_DEBUG_CHECKS) {
+      plan->debug_checks = value != 0;
+    } else if (option == CBCT_OPT_FORCE_GATHER) {
+      plan->force_gather = value != 0;
+      forward_choose_variant(plan);
+      forward_prepare(plan);
+    } else {
+      throw Error(CBCT_ERR_INVALID_ARGUMENT, "unknown option");
+    }
+  });
+}
+
+cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t reset) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && flags_out, "bad arguments");
+    CBCT_CUDA(cudaDeviceSynchronize());
+    int h[4];
+    CBCT_CUDA(cudaMemcpy(h, plan->d_flags, sizeof(h), cudaMemcpyDeviceToHost));
+    flags_out[0] = h[0];
+    flags_out[1] = h[1];
+    if (reset) CBCT_CUDA(cudaMemset(plan->d_flags, 0, sizeof(h)));
+  });
+}
+
+cbct_status cbct_forward(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol, float* proj,
+                         int32_t accumulate, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(vol && proj, "NULL array");
+    forward_launch(plan, i, vol_dtype, vol, proj, nullptr, 1.f, 0, 0, accumulate, nullptr, S(stream));
+  });
+}
+
+cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, float* vol, uint32_t flags,
+                             int32_t use_plan_offset, int32_t accumulate, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(vol && proj, "NULL array");
+    CBCT_REQUIRE((flags & ~(CBCT_BP_OFFSET_WEIGHT | CBCT_BP_FDK_WEIGHT)) == 0, "unknown flags");
+    const bool off = (flags & CBCT_BP_OFFSET_WEIGHT) || (use_plan_offset && plan->offcorr[i]);
+    const float* in = proj;
+    if (off) {
+      // mult_MH copies the input and weights the copy (cuConebeamProjectionOperator.cpp:101-102).
+      float* w = proj_scratch(plan, (size_t)plan->g.width * plan->g.height * plan->count[i]);
+      offset_weight_launch(plan, i, proj, w, 0, S(stream));
+      in = w;
+    }
+    backproject_launch(plan, i, in, vol, (flags & CBCT_BP_FDK_WEIGHT) ? 1 : 0, accumulate, 1.f, S(stream));
+  });
+}
+
+cbct_status cbct_offset_correct(cbct_plan* plan, int32_t s, float* proj, int32_t variant, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(proj, "NULL array");
+    CBCT_REQUIRE(variant == 0 || variant == 1, "variant must be 0 or 1");
+    offset_weight_launch(plan, i, proj, proj, variant, S(stream));
+  });
+}
+
+cbct_status cbct_fdk_filter(cbct_plan* plan, int32_t s, const float* proj_in, float* proj_out, const float* filter,
+                            uint32_t flags, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(proj_in && proj_out, "NULL array");
+    fdk_filter_launch(plan, i, proj_in, proj_out, filter, flags, S(stream));
+  });
+}
+
+cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float* filter, uint32_t flags,
+                     float* work, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && proj && vol, "NULL argument");
+    fdk_run(plan, proj, vol, filter, flags, work, S(stream));
+  });
+}
+
+cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol, const float* b,
+                                  float* r, float scale, int32_t apply_offset, double* norm2_out, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(vol && b && r, "NULL array");
+    forward_launch(plan, i, vol_dtype, vol, r, b, scale, 1, apply_offset, 0, norm2_out, S(stream));
+  });
+}
+
+cbct_status cbct_osmom_update(float* z, float* xold, const float* precon, const float* g, size_t n, float step,
+                              float mom, int32_t nonneg, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(z && xold && precon && g, "NULL array");
+    osmom_update_launch(z, xold, precon, g, n, step, mom, nonneg, S(stream));
+  });
+}
+
+cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t n, double* out_dev, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(kind >= 0 && kind <= 2, "kind must be 0, 1 or 2");
+    CBCT_REQUIRE(a && out_dev && (kind != 0 || b), "NULL array");
+    // A small per-call partials buffer; reductions are rare outside the solvers.
+    static thread_local double* partials = nullptr;
+    static thread_local int dev = -1;
+    int cur;
+    CBCT_CUDA(cudaGetDevice(&cur));
+    if (!partials || dev != cur) {
+      CBCT_CUDA(cudaMalloc(&partials, sizeof(double) * 148 * 4));
+      dev = cur;
+    }
+    reduce_launch(kind, a, b, n, partials, 148 * 4, out_dev, S(stream));
+  });
+}
+
+static cbct_solver_params solver_defaults(const cbct_solver_params* p) {
+  cbct_solver_params d{};
+  d.iterations = 10;
+  d.beta = 1.f;
+  d.gamma = 0.f;
+  d.non_negativity = 0;
+  d.use_graph = 0;
+  d.storage = CBCT_F32;
+  d.refine_every = 0;
+  return p ? *p : d;
+}
+
+cbct_status cbct_osmom_solve(cbct_plan* plan, const float* b, const float* x0, float* z_out,
+                             const cbct_solver_params* params, double* resid_norm2_out, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && b && z_out, "NULL argument");
+    const cbct_solver_params prm = solver_defaults(params);
+    CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
+    osmom_solve(plan, b, x0, z_out, prm, resid_norm2_out, S(stream));
+  });
+}
+
+cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, float* x_out,
+                              const cbct_solver_params* params, double* cost_out, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && b && x_out, "NULL argument");
+    const cbct_solver_params prm = solver_defaults(params);
+    CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
+    ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
+  });
+}
+
+cbct_status cbct_phantom_voxelize(const cbct_geometry* g, const float* ell, int32_t n, int32_t ss, float* vol,
+                                  void* stream) {
+  return guard([&] {
+    validate_geometry(g);
+    CBCT_REQUIRE(ell && vol && n >= 0 && ss >= 1, "bad arguments");
+    phantom_voxelize_launch(make_grid(*g), ell, n, ss, vol, S(stream));
+  });
+}
+
+cbct_status cbct_phantom_project(cbct_plan* plan, int32_t s, const float* ell, int32_t n, float* proj, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(ell && proj && n >= 0, "bad arguments");
+    phantom_project_launch(plan, i, ell, n, proj, S(stream));
+  });
+}
+
+cbct_status cbct_convert(const float* src, void* dst, size_t n, cbct_dtype dt, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(src && dst, "NULL array");
+    convert_launch(src, dst, n, dt, S(stream));
+  });
+}
+
+}  // extern "C"

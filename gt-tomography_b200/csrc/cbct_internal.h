@@ -1,0 +1,169 @@
+// cbct_internal.h -- shared declarations of the B200 cone-beam library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cbct.h"
+
+namespace cbct {
+
+// ---------------------------------------------------------------- errors
+// Internal code throws cbct::Error; the C ABI (abi.cu) converts it into a
+// status code and a thread-local message.  Nothing throws across the ABI.
+struct Error : std::runtime_error {
+  cbct_status status;
+  Error(cbct_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define CBCT_CUDA(call)                                                                 \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      throw ::cbct::Error(e_ == cudaErrorMemoryAllocation ? CBCT_ERR_OUT_OF_MEMORY      \
+                                                          : CBCT_ERR_CUDA,              \
+                          std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+#define CBCT_REQUIRE(cond, msg)                                                         \
+  do {                                                                                  \
+    if (!(cond)) throw ::cbct::Error(CBCT_ERR_INVALID_ARGUMENT, msg);                   \
+  } while (0)
+
+inline void check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Error(CBCT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------- geometry
+// Per-view constants, computed in FP64 on the host and stored as float.
+// A ray of detector pixel (u,v) runs from S to E(u,v) = S + D0 + u*Eu + v*Ev
+// (conebeam_projection.cu:441-473 with the detector point expanded linearly
+// in u and v).  Back-projection uses the inverse rotation of :975-984.
+struct ViewParams {
+  float cs, sn;          // cos(theta), sin(theta)
+  float Sx, Sy;          // source position (S_z = 0)
+  float D0x, D0y, D0z;   // direction E(0,0) - S
+  float Eux, Euy;        // dE/du (in plane)
+  float Evz;             // dE/dv (along z)
+  float ox, oy;          // detector offsets, mm
+  int dom;               // dominant in-plane axis of the view's rays: 0 = x, 1 = y
+  int dsgn;              // sign of the ray direction along that axis (+1/-1)
+  float pad0, pad1;
+};
+static_assert(sizeof(ViewParams) == 64, "ViewParams is 64 bytes");
+
+// Kernel-side constants of the volume grid and detector.
+struct GridConst {
+  int nx, ny, nz;
+  int W, H;
+  int N;                  // samples per ray
+  float hx, hy, hz;       // half volume size, mm
+  float kx, ky, kz;       // voxels per mm: texel = world*k + b
+  float bx, by, bz;       // n/2 - 0.5
+  float vx, vy, vz;       // voxel size, mm
+  float SAD, SDD;
+  float fov_u, fov_v;
+  float ku, kv;           // pixels per mm on the detector
+  float bu, bv;           // W/2 - 0.5, H/2 - 0.5
+  float invN;
+};
+
+// Box configuration of the TMA slab forward projector for one dominant axis.
+struct SlabBox {
+  int bx, by, bz;         // TMA box (elements) in memory order x, y, z
+  int valid;
+};
+
+// Forward projector tiling (compile-time): CTA = TU x TV rays of one view,
+// slabs of TS voxels along the dominant axis, NSTAGE-deep TMA pipeline.
+constexpr int kTU = 16;
+constexpr int kTV = 16;
+constexpr int kTS = 16;
+constexpr int kNStage = 2;
+constexpr int kSlabBase = -4;      // slab m covers texel rows [kSlabBase + m*kTS, +kTS)
+constexpr int kMaxSlabs = 160;
+constexpr int kSmemBudget = 200 * 1024;
+
+}  // namespace cbct
+
+// ---------------------------------------------------------------- the plan
+struct cbct_plan {
+  cbct_geometry g{};
+  cbct::GridConst gc{};
+  int n_views = 0, n_subsets = 0;
+  std::vector<int> first, count, offcorr;
+  std::vector<float> angles, offsets;
+  std::vector<cbct::ViewParams> hviews;
+  cbct::ViewParams* d_views = nullptr;
+  int device = 0;
+  int max_subset = 0;
+
+  // forward variant: 0 = gather (global loads), 1 = TMA slab
+  int fwd_variant = 0;
+  cbct::SlabBox slab[2]{};  // [0] x-dominant views, [1] y-dominant views
+  size_t slab_smem = 0;     // dynamic shared memory of the slab kernel (bytes)
+
+  // scratch owned by the plan (allocated at creation or first use, reused)
+  float* d_proj_scratch = nullptr;  // weighted copies of projections (mult_MH with offset weight)
+  size_t proj_scratch_elems = 0;
+  double* d_partials = nullptr;     // per-block FP64 partial sums
+  size_t n_partials = 0;
+  int* d_flags = nullptr;           // [0] device range-check violations, [1] wait timeouts
+  void* fdk_state = nullptr;        // FDK tables (weights.cu)
+  float* d_fdk_work = nullptr;      // filtered projections for cbct_fdk
+  size_t fdk_work_elems = 0;
+  void* graph_cache = nullptr;      // captured solver graph (solver.cu)
+
+  // solver workspace (allocated on first solve, reused)
+  float* ws = nullptr;
+  size_t ws_elems = 0;
+
+  int debug_checks = 0;
+  int force_gather = 0;
+};
+
+namespace cbct {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+// Raises a kernel's dynamic shared-memory limit once (no-op when already high
+// enough, so it is safe to call before launches that may be captured).
+void ensure_smem_attr(const void* func, size_t bytes);
+
+// forward.cu
+void forward_prepare(cbct_plan* p);
+void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
+                       const float* pw, float scale, int mode, int apply_offset, int accumulate,
+                       double* norm2_out, cudaStream_t st);
+void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out,
+                    const float* b, float scale, int mode, int apply_offset, int accumulate,
+                    double* norm2_out, cudaStream_t st);
+void forward_choose_variant(cbct_plan* p);
+// backproject.cu
+void backproject_prepare(cbct_plan* p);
+void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int fdk_weight,
+                        int accumulate, float out_scale, cudaStream_t st);
+// weights.cu
+void offset_weight_launch(cbct_plan* p, int s, const float* in, float* out, int variant,
+                          cudaStream_t st);
+void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const float* filter,
+                       uint32_t flags, cudaStream_t st);
+// solver.cu
+void reduce_launch(int kind, const float* a, const float* b, size_t n, double* partials,
+                   size_t n_partials, double* out, cudaStream_t st);
+void finalize_partials(const double* partials, int n, double* out, cudaStream_t st);
+void osmom_update_launch(float* z, float* xold, const float* precon, const float* g, size_t n,
+                         float step, float mom, int nonneg, cudaStream_t st);
+
+// host helpers (abi.cu)
+void default_filter(int W, float* out);
+void subset_partition(int n_views, const int* view_bin, int n_subsets, int* order,
+                      int* sizes, int* n_out);
+
+}  // namespace cbct

@@ -1,0 +1,291 @@
+// weights.cu -- detector-space weights and the FDK row filter for sm_100a.
+//
+// Offset (Wang) weights: conebeam_projection.cu:233-262 (sin^2, zeroing) and
+// :303-331 (sin).  Parker weights: :151-194.  Cosine weights:
+// hoCuConebeamProjectionOperator.cpp:64-102.  Row filter: :1504-1511 with
+// cb_fft/cb_ifft :87-139.
+//
+// The reference filters each detector row by zero-padding it to 2W, an R2C
+// FFT, a multiply by the real filter H[0..W], a C2R FFT and a division by 2W,
+// then crops the centre W samples.  Because input and output both occupy the
+// centre W samples of the 2W frame, this is exactly a linear convolution with
+// the real even kernel h[j] = IDFT_2W(H)[j], |j| <= W-1 (the wrapped taps are
+// never reached).  The kernel below evaluates that convolution with a
+// hand-written power-of-two FFT of length L >= 2W-1 in shared memory: two rows
+// ride in one complex transform (row a in the real part, row b in the
+// imaginary part); since the spectrum of h is real and even, the product's
+// inverse keeps the two rows apart.  The spectrum (with the 1/L scale) is
+// computed once per filter on the host in FP64.
+#include <cmath>
+#include <vector>
+
+#include "device_common.cuh"
+
+namespace cbct {
+
+namespace {
+
+__global__ void offset_weight_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                     const ViewParams* __restrict__ views, GridConst gc, int n_views,
+                                     int variant) {
+  const size_t n = (size_t)gc.W * gc.H * n_views;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int u = int(idx % gc.W);
+    const int p = int(idx / ((size_t)gc.W * gc.H));
+    const float o = views[p].ox;
+    const float w = variant == 0 ? offset_weight_full(gc.fov_u, gc.W, u, o)
+                                 : offset_weight_sqrt(gc.fov_u, gc.W, u, o);
+    // The sin^2 variant multiplies by 0 (not a store of 0) where t < -omega,
+    // and leaves pixels alone when no branch applies; w = 1 reproduces that.
+    out[idx] = in[idx] * w;
+  }
+}
+
+constexpr int kFftThreads = 256;
+
+// One CTA filters pairs of rows.  rows = H * n_views, row r = (p, v).
+//   pre[u + W*v]     cosine weight (nullable)
+//   parker[u + W*p]  Parker weight (nullable)
+//   post[u + W*p]    sin^2 offset weight (nullable)
+__global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(
+    const float* in, float* out, int W, int H, long rows, int L, int logL,
+    const float* __restrict__ spec, const float2* __restrict__ tw, const float* __restrict__ pre,
+    const float* __restrict__ parker, const float* __restrict__ post) {
+  extern __shared__ float2 fsm[];
+  float2* a = fsm;                  // L
+  float2* t = fsm + L;              // L/2 twiddles
+  float* hs = reinterpret_cast<float*>(fsm + L + L / 2);  // L spectrum
+  const int tid = threadIdx.x;
+  for (int i = tid; i < L / 2; i += kFftThreads) t[i] = tw[i];
+  for (int i = tid; i < L; i += kFftThreads) hs[i] = spec[i];
+  const long npairs = (rows + 1) / 2;
+  for (long pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
+    const long ra = 2 * pr, rb = 2 * pr + 1;
+    const bool hasb = rb < rows;
+    const int pa = int(ra / H), va = int(ra % H);
+    const int pb = int(rb / H), vb = int(rb % H);
+    __syncthreads();
+    // Bit-reversed load with the pre-weights fused.
+    for (int n = tid; n < L; n += kFftThreads) {
+      float xa = 0.f, xb = 0.f;
+      if (n < W) {
+        xa = in[ra * W + n];
+        if (pre) xa *= pre[(size_t)va * W + n];
+        if (parker) xa *= parker[(size_t)pa * W + n];
+        if (hasb) {
+          xb = in[rb * W + n];
+          if (pre) xb *= pre[(size_t)vb * W + n];
+          if (parker) xb *= parker[(size_t)pb * W + n];
+        }
+      }
+      a[__brev(n) >> (32 - logL)] = make_float2(xa, xb);
+    }
+    __syncthreads();
+    // Forward DIT, twiddle exp(-2 pi i k / L).
+    for (int len = 2; len <= L; len <<= 1) {
+      const int half = len >> 1, ts = L / len;
+      for (int b = tid; b < L / 2; b += kFftThreads) {
+        const int grp = b / half, pos = b - grp * half;
+        const int i0 = grp * len + pos, i1 = i0 + half;
+        const float2 w = t[pos * ts];
+        const float2 v = a[i1];
+        const float2 x = a[i0];
+        const float2 m = make_float2(w.x * v.x - w.y * v.y, w.x * v.y + w.y * v.x);
+        a[i0] = make_float2(x.x + m.x, x.y + m.y);
+        a[i1] = make_float2(x.x - m.x, x.y - m.y);
+      }
+      __syncthreads();
+    }
+    for (int k = tid; k < L; k += kFftThreads) {
+      const float h = hs[k];
+      a[k] = make_float2(a[k].x * h, a[k].y * h);
+    }
+    __syncthreads();
+    // Inverse DIF (natural order in, bit-reversed order out), twiddle exp(+2 pi i k / L).
+    for (int len = L; len >= 2; len >>= 1) {
+      const int half = len >> 1, ts = L / len;
+      for (int b = tid; b < L / 2; b += kFftThreads) {
+        const int grp = b / half, pos = b - grp * half;
+        const int i0 = grp * len + pos, i1 = i0 + half;
+        const float2 w = t[pos * ts];
+        const float2 x = a[i0], v = a[i1];
+        const float2 d = make_float2(x.x - v.x, x.y - v.y);
+        a[i0] = make_float2(x.x + v.x, x.y + v.y);
+        a[i1] = make_float2(w.x * d.x + w.y * d.y, w.x * d.y - w.y * d.x);  // d * conj(w)
+      }
+      __syncthreads();
+    }
+    for (int n = tid; n < W; n += kFftThreads) {
+      const float2 y = a[__brev(n) >> (32 - logL)];
+      float ya = y.x;
+      if (post) ya *= post[(size_t)pa * W + n];
+      out[ra * W + n] = ya;
+      if (hasb) {
+        float yb = y.y;
+        if (post) yb *= post[(size_t)pb * W + n];
+        out[rb * W + n] = yb;
+      }
+    }
+  }
+}
+
+// FP64 spectrum of the row filter on an L-point grid, scaled by 1/L.
+std::vector<float> filter_spectrum(const float* H, int W, int L) {
+  std::vector<double> h(W);
+  const double pi = 3.14159265358979323846;
+  for (int j = 0; j < W; ++j) {
+    double s = H[0] + ((j & 1) ? -1.0 : 1.0) * H[W];
+    for (int k = 1; k < W; ++k) s += 2.0 * H[k] * std::cos(pi * double((long)j * k % (2L * W)) / W);
+    h[j] = s / (2.0 * W);
+  }
+  std::vector<float> spec(L);
+  for (int k = 0; k < L; ++k) {
+    double s = h[0];
+    for (int j = 1; j < W; ++j) s += 2.0 * h[j] * std::cos(2.0 * pi * double((long)j * k % L) / L);
+    spec[k] = float(s / L);
+  }
+  return spec;
+}
+
+struct FdkTables {
+  float* spec = nullptr;
+  float2* tw = nullptr;
+  float* cosw = nullptr;
+  float* parker = nullptr;  // per view of the plan
+  float* post = nullptr;    // per view of the plan
+};
+
+}  // namespace
+
+// Per-plan FDK tables, created on first use (host-side allocation; not inside
+// stream capture).
+struct FdkState {
+  FdkTables t;
+  std::vector<float> filter;
+  int L = 0, logL = 0;
+};
+
+void fdk_state_free(cbct_plan* p) {
+  FdkState* f = static_cast<FdkState*>(p->fdk_state);
+  if (!f) return;
+  cudaFree(f->t.spec);
+  cudaFree(f->t.tw);
+  cudaFree(f->t.cosw);
+  cudaFree(f->t.parker);
+  cudaFree(f->t.post);
+  delete f;
+  p->fdk_state = nullptr;
+}
+
+static FdkState* fdk_state(cbct_plan* p, const float* filter) {
+  const int W = p->g.width, H = p->g.height, P = p->n_views;
+  FdkState* f = static_cast<FdkState*>(p->fdk_state);
+  if (!f) {
+    f = new FdkState();
+    p->fdk_state = f;
+    int L = 1, logL = 0;
+    while (L < 2 * W - 1) { L <<= 1; ++logL; }
+    if (L < 2) { L = 2; logL = 1; }
+    f->L = L;
+    f->logL = logL;
+    std::vector<float2> tw(L / 2);
+    const double pi = 3.14159265358979323846;
+    for (int k = 0; k < L / 2; ++k)
+      tw[k] = make_float2(float(std::cos(2 * pi * k / L)), float(-std::sin(2 * pi * k / L)));
+    CBCT_CUDA(cudaMalloc(&f->t.tw, sizeof(float2) * tw.size()));
+    CBCT_CUDA(cudaMemcpy(f->t.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+    CBCT_CUDA(cudaMalloc(&f->t.spec, sizeof(float) * L));
+    // Cosine weights (hoCuConebeamProjectionOperator.cpp:84-97): double, stored float.
+    std::vector<float> cw((size_t)W * H);
+    const double SAD = p->g.SAD, SDD = p->g.SDD;
+    for (int y = 0; y < H; ++y)
+      for (int x = 0; x < W; ++x) {
+        const double xx = (double(x) / W - 0.5) * p->g.fov_u, yy = (double(y) / H - 0.5) * p->g.fov_v;
+        const double s = SAD * xx / SDD, v = SAD * yy / SDD;
+        cw[(size_t)y * W + x] = float(SAD / std::sqrt(SAD * SAD + s * s + v * v));
+      }
+    CBCT_CUDA(cudaMalloc(&f->t.cosw, sizeof(float) * cw.size()));
+    CBCT_CUDA(cudaMemcpy(f->t.cosw, cw.data(), sizeof(float) * cw.size(), cudaMemcpyHostToDevice));
+    // Parker weights per (view, u) in FP64 (conebeam_projection.cu:169-194).
+    std::vector<float> pk((size_t)W * P), po((size_t)W * P);
+    const double eps = 0.001, q = 0.1;
+    const double delta = std::atan(p->g.fov_u / (2.0 * SDD));
+    const double tand = std::tan(delta);
+    auto S = [&](double b) { return b <= -0.5 ? 0.0 : (b < 0.5 ? 0.5 * (1 + std::sin(pi * b)) : 1.0); };
+    for (int v = 0; v < P; ++v) {
+      const double beta = p->angles[v] * (pi / 180.0);
+      const double o = p->offsets[2 * v];
+      const double sg = o / std::fabs(o);
+      const double omega = p->g.fov_u / 2.0 - std::fabs(o);
+      for (int u = 0; u < W; ++u) {
+        const double alpha = -std::atan((double(u) / W - 0.5) * 2.0 * tand);
+        const double bp = q * (2 * (delta - alpha) + eps), bm = q * (2 * (delta + alpha) + eps);
+        const double om = 0.5 * (S(beta / bp - 0.5) + S((beta + 2 * (alpha - delta) - eps) / bp + 0.5) -
+                                 S((beta - pi + 2 * alpha) / bm - 0.5) -
+                                 S((beta - pi - 2 * delta - eps) / bm + 0.5));
+        pk[(size_t)v * W + u] = float(om);
+        // sin^2 offset weight (conebeam_projection.cu:245-259)
+        const double t = (p->g.fov_u * (double(u) / W - 0.5) + o) * sg;
+        double w = 1.0;
+        if (std::fabs(t) <= omega) {
+          const double sw = std::sin(pi * (t + omega) / (4 * omega));
+          w = sw * sw;
+        }
+        if (t < -omega) w = 0.0;
+        po[(size_t)v * W + u] = float(w);
+      }
+    }
+    CBCT_CUDA(cudaMalloc(&f->t.parker, sizeof(float) * pk.size()));
+    CBCT_CUDA(cudaMemcpy(f->t.parker, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice));
+    CBCT_CUDA(cudaMalloc(&f->t.post, sizeof(float) * po.size()));
+    CBCT_CUDA(cudaMemcpy(f->t.post, po.data(), sizeof(float) * po.size(), cudaMemcpyHostToDevice));
+  }
+  std::vector<float> want(W + 1);
+  if (filter) std::copy(filter, filter + W + 1, want.begin());
+  else default_filter(W, want.data());
+  if (want != f->filter) {
+    std::vector<float> spec = filter_spectrum(want.data(), W, f->L);
+    CBCT_CUDA(cudaMemcpy(f->t.spec, spec.data(), sizeof(float) * f->L, cudaMemcpyHostToDevice));
+    f->filter = want;
+  }
+  return f;
+}
+
+void offset_weight_launch(cbct_plan* p, int s, const float* in, float* out, int variant,
+                          cudaStream_t st) {
+  const int first = p->first[s], cnt = p->count[s];
+  const size_t n = (size_t)p->g.width * p->g.height * cnt;
+  if (n == 0) return;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  offset_weight_kernel<<<blocks, 256, 0, st>>>(in, out, p->d_views + first, p->gc, cnt, variant);
+  check_launch("offset_weight_kernel");
+}
+
+void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const float* filter,
+                       uint32_t flags, cudaStream_t st) {
+  const int first = p->first[s], cnt = p->count[s];
+  const int W = p->g.width, H = p->g.height;
+  if (cnt == 0) return;
+  FdkState* f = fdk_state(p, filter);
+  const long rows = (long)H * cnt;
+  const float* pre = (flags & CBCT_FDK_COSINE) ? f->t.cosw : nullptr;
+  const float* pk = (flags & CBCT_FDK_PARKER) ? f->t.parker + (size_t)first * W : nullptr;
+  const float* post = (flags & CBCT_FDK_OFFSET) ? f->t.post + (size_t)first * W : nullptr;
+  if (!(flags & CBCT_FDK_RAMP)) {
+    // Weights only: run the filter with a unit spectrum would waste work; use
+    // the element-wise path instead.
+    throw Error(CBCT_ERR_UNSUPPORTED, "cbct_fdk_filter without CBCT_FDK_RAMP is not implemented");
+  }
+  const int L = f->L;
+  const size_t smem = sizeof(float2) * (L + L / 2) + sizeof(float) * L;
+  if (smem > 200 * 1024) throw Error(CBCT_ERR_UNSUPPORTED, "detector too wide for the FDK filter");
+  ensure_smem_attr((const void*)fdk_filter_kernel, smem);
+  const long npairs = (rows + 1) / 2;
+  const int blocks = (int)std::min<long>(npairs, 148L * 8);
+  fdk_filter_kernel<<<blocks, kFftThreads, smem, st>>>(in, out, W, H, rows, L, f->logL, f->t.spec, f->t.tw,
+                                                       pre, pk, post);
+  check_launch("fdk_filter_kernel");
+}
+
+}  // namespace cbct

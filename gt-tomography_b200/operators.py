@@ -1,0 +1,789 @@
+"""Reference-shaped operator surface over the C ABI.
+
+Mirrors gt-tomography's operator classes for the cone-beam path so that code
+written against them reads the same:
+
+  CBCT_geometry / CBCT_acquisition / CBCT_binning   xray/CBCT_acquisition.h:24-340,
+                                                    xray/CBCT_binning.h:18-172
+  cuConebeamProjectionOperator                      xray/cuConebeamProjectionOperator.{h,cpp}
+  CBSubsetOperator                                  xray/CBSubsetOperator.{h,cpp}
+  hoCuConebeamProjectionOperator                    xray/hoCuConebeamProjectionOperator.{h,cpp}
+  osMOMSolverD                                      solvers/osMOMSolverD.h
+  osSARTSolver                                      solvers/osSARTSolver.h
+  fdk_reconstruct_3d                                xray/FDK_reconstruct_3d.cpp:135-161
+
+Device arrays are torch CUDA tensors (torch is used for device memory and
+streams only); every computation runs in libcbct.so.  Array shapes are the
+reverse of Gadgetron's dimension lists: a volume of Gadgetron dims
+(nx, ny, nz) is a tensor of shape (nz, ny, nx); projections (W, H, P) are
+(P, H, W).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+_torch = None
+
+
+def torch():
+    global _torch
+    if _torch is None:
+        import torch as t
+        _torch = t
+    return _torch
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def _stream(stream=None) -> int:
+    if stream is not None:
+        return int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+    return int(torch().cuda.current_stream().cuda_stream)
+
+
+def _need_cuda_f32(t, shape, what):
+    T = torch()
+    if not isinstance(t, T.Tensor) or not t.is_cuda:
+        raise TypeError(f"{what} must be a CUDA tensor")
+    if t.dtype != T.float32:
+        raise TypeError(f"{what} must be float32, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{what} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+
+
+# ----------------------------------------------------------------- data model
+@dataclass
+class CBCT_geometry:
+    """CBCT_geometry (xray/CBCT_acquisition.h:24-120): mm and degrees."""
+    SAD: float = 0.0
+    SDD: float = 0.0
+    FOV: tuple = (0.0, 0.0)
+    angles: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    offsets: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
+
+    def get_angles(self):
+        return self.angles
+
+    def set_angles(self, a):
+        self.angles = np.asarray(a, dtype=np.float32).copy()
+
+    def get_offsets(self):
+        return self.offsets
+
+    def set_offsets(self, o):
+        self.offsets = np.asarray(o, dtype=np.float32).reshape(-1, 2).copy()
+
+
+@dataclass
+class CBCT_acquisition:
+    """CBCT_acquisition: geometry plus projections of shape (P, H, W) (host, float32)."""
+    geometry: CBCT_geometry
+    projections: Optional[np.ndarray] = None
+
+    def get_geometry(self):
+        return self.geometry
+
+    def get_projections(self):
+        return self.projections
+
+    def set_projections(self, p):
+        self.projections = p
+
+
+class CBCT_binning:
+    """CBCT_binning (xray/CBCT_binning.h:18-172): lists of view indices per bin."""
+
+    def __init__(self, bins: Optional[Sequence[Sequence[int]]] = None):
+        self.bins = [list(map(int, b)) for b in (bins or [])]
+
+    def set_as_default_3d_bin(self, n: int):
+        self.bins = [list(range(n))]
+
+    def get_number_of_bins(self) -> int:
+        return len(self.bins)
+
+    def get_bin(self, b: int):
+        return self.bins[b]
+
+    def get_bins(self):
+        return self.bins
+
+    def get_3d_binning(self):
+        allv = sorted({v for b in self.bins for v in b})
+        return CBCT_binning([allv])
+
+
+# ----------------------------------------------------------------- host helpers
+def _cgeom(acq_geom: CBCT_geometry, W: int, H: int, is_dims, is_dims_in_mm, spp: float) -> L.CbctGeometry:
+    nx, ny, nz = (int(v) for v in is_dims)
+    lx, ly, lz = (float(v) for v in is_dims_in_mm)
+    return L.CbctGeometry(float(acq_geom.SAD), float(acq_geom.SDD), float(acq_geom.FOV[0]),
+                          float(acq_geom.FOV[1]), int(W), int(H), nx, ny, nz, lx, ly, lz, float(spp))
+
+
+def subset_partition(n_views: int, n_subsets: int, view_bin=None):
+    """CBSubsetOperator::setup's subset assignment (CBSubsetOperator.cpp:66-104)."""
+    vb = None if view_bin is None else np.ascontiguousarray(view_bin, dtype=np.int32)
+    order = np.zeros(max(n_views, 1), np.int32)
+    sizes = np.zeros(n_subsets, np.int32)
+    n = C.c_int32()
+    L.call("cbct_subset_partition", n_views, None if vb is None else vb.ctypes.data, n_subsets,
+           order.ctypes.data, sizes.ctypes.data, C.byref(n))
+    return order[:n.value], sizes
+
+
+def default_frequency_filter(W: int) -> np.ndarray:
+    out = np.zeros(W + 1, np.float32)
+    L.call("cbct_default_frequency_filter", W, out.ctypes.data)
+    return out
+
+
+def cosine_weights(g: L.CbctGeometry) -> np.ndarray:
+    out = np.zeros((g.height, g.width), np.float32)
+    L.call("cbct_cosine_weights", C.byref(g), out.ctypes.data)
+    return out
+
+
+def is_short_scan(g: L.CbctGeometry, angles) -> bool:
+    a = np.ascontiguousarray(angles, np.float32)
+    r = C.c_int32()
+    L.call("cbct_is_short_scan", C.byref(g), a.ctypes.data, a.size, C.byref(r))
+    return bool(r.value)
+
+
+def offset_override(g: L.CbctGeometry, offsets) -> bool:
+    o = np.ascontiguousarray(offsets, np.float32).reshape(-1)
+    r = C.c_int32()
+    L.call("cbct_offset_override", C.byref(g), o.ctypes.data, o.size // 2, C.byref(r))
+    return bool(r.value)
+
+
+def hann_ramp_filter(W: int) -> np.ndarray:
+    """Hann-windowed ramp on the W+1 bins of the FDK filter, normalised like the
+    default filter (absolute sum W+1; hoCuConebeamProjectionOperator.cpp:59-61)."""
+    k = np.arange(W + 1, dtype=np.float64)
+    h = k * 0.5 * (1.0 + np.cos(np.pi * k / W))
+    return (h * ((W + 1) / np.abs(h).sum())).astype(np.float32)
+
+
+# ----------------------------------------------------------------- plans
+class Plan:
+    """A device-resident geometry (cbct_plan) for views in subset-contiguous order."""
+
+    def __init__(self, g: L.CbctGeometry, angles, offsets, subset_sizes=None, offset_correction=None):
+        self.g = g
+        self.angles = np.ascontiguousarray(angles, np.float32)
+        self.offsets = np.ascontiguousarray(offsets, np.float32).reshape(-1, 2)
+        P = self.angles.size
+        assert self.offsets.shape[0] == P
+        self.subset_sizes = (np.array([P], np.int32) if subset_sizes is None
+                             else np.ascontiguousarray(subset_sizes, np.int32))
+        S = self.subset_sizes.size
+        oc = (np.zeros(S, np.int32) if offset_correction is None
+              else np.ascontiguousarray(offset_correction, np.int32))
+        self.offset_correction = oc
+        h = C.c_void_p()
+        L.call("cbct_plan_create", C.byref(g), self.angles.ctypes.data, self.offsets.ctypes.data, P,
+               self.subset_sizes.ctypes.data, S, oc.ctypes.data, C.byref(h))
+        self._h = h
+        self.n_views = P
+        self.n_subsets = S
+        self.first = np.concatenate([[0], np.cumsum(self.subset_sizes)[:-1]]).astype(np.int64)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            L.lib().cbct_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def vol_shape(self):
+        return (self.g.nz, self.g.ny, self.g.nx)
+
+    def proj_shape(self, s=-1):
+        n = self.n_views if s < 0 else int(self.subset_sizes[s])
+        return (n, self.g.height, self.g.width)
+
+    def forward_variant(self) -> str:
+        return L.lib().cbct_plan_forward_variant(self._h).decode()
+
+    def set_option(self, opt: int, value: int):
+        L.call("cbct_plan_set_option", self._h, opt, int(value))
+
+    def read_flags(self, reset=True):
+        f = (C.c_int32 * 2)()
+        L.call("cbct_plan_read_flags", self._h, C.cast(f, C.c_void_p), int(reset))
+        return int(f[0]), int(f[1])
+
+    # -- operators
+    def forward(self, vol, out, s=-1, accumulate=False, vol_dtype=L.CBCT_F32, stream=None):
+        T = torch()
+        if vol_dtype == L.CBCT_F32:
+            _need_cuda_f32(vol, self.vol_shape, "volume")
+        else:
+            want = T.float16 if vol_dtype == L.CBCT_F16 else T.bfloat16
+            if vol.dtype != want or tuple(vol.shape) != self.vol_shape or not vol.is_contiguous():
+                raise TypeError("volume does not match vol_dtype/shape")
+        _need_cuda_f32(out, self.proj_shape(s), "projections")
+        L.call("cbct_forward", self._h, s, vol_dtype, _ptr(vol), _ptr(out), int(accumulate), _stream(stream))
+        return out
+
+    def backproject(self, proj, out, s=-1, flags=0, use_plan_offset=True, accumulate=False, stream=None):
+        _need_cuda_f32(proj, self.proj_shape(s), "projections")
+        _need_cuda_f32(out, self.vol_shape, "volume")
+        L.call("cbct_backproject", self._h, s, _ptr(proj), _ptr(out), flags, int(use_plan_offset),
+               int(accumulate), _stream(stream))
+        return out
+
+    def offset_correct(self, proj, s=-1, variant=1, stream=None):
+        _need_cuda_f32(proj, self.proj_shape(s), "projections")
+        L.call("cbct_offset_correct", self._h, s, _ptr(proj), variant, _stream(stream))
+        return proj
+
+    def fdk_filter(self, proj_in, proj_out, s=-1, filt=None, flags=L.CBCT_FDK_RAMP | L.CBCT_FDK_COSINE,
+                   stream=None):
+        _need_cuda_f32(proj_in, self.proj_shape(s), "projections")
+        _need_cuda_f32(proj_out, self.proj_shape(s), "projections")
+        f = None if filt is None else np.ascontiguousarray(filt, np.float32)
+        if f is not None and f.size != self.g.width + 1:
+            raise ValueError("filter must have W+1 entries")
+        L.call("cbct_fdk_filter", self._h, s, _ptr(proj_in), _ptr(proj_out),
+               None if f is None else f.ctypes.data, flags, _stream(stream))
+        return proj_out
+
+    def fdk(self, proj, out, filt=None, flags=0, work=None, stream=None):
+        _need_cuda_f32(proj, self.proj_shape(-1), "projections")
+        _need_cuda_f32(out, self.vol_shape, "volume")
+        f = None if filt is None else np.ascontiguousarray(filt, np.float32)
+        L.call("cbct_fdk", self._h, _ptr(proj), _ptr(out), None if f is None else f.ctypes.data, flags,
+               _ptr(work), _stream(stream))
+        return out
+
+    def forward_residual(self, vol, b, r, s=-1, scale=1.0, apply_offset=False, norm2=None,
+                         vol_dtype=L.CBCT_F32, stream=None):
+        _need_cuda_f32(b, self.proj_shape(s), "b")
+        _need_cuda_f32(r, self.proj_shape(s), "r")
+        L.call("cbct_forward_residual", self._h, s, vol_dtype, _ptr(vol), _ptr(b), _ptr(r), float(scale),
+               int(apply_offset), _ptr(norm2), _stream(stream))
+        return r
+
+    def phantom_project(self, ell_dev, out, s=-1, stream=None):
+        _need_cuda_f32(out, self.proj_shape(s), "projections")
+        n = ell_dev.numel() // 10
+        L.call("cbct_phantom_project", self._h, s, _ptr(ell_dev), n, _ptr(out), _stream(stream))
+        return out
+
+    def osmom(self, b, z_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
+              storage=L.CBCT_F32, refine_every=0, resid=None, stream=None):
+        prm = L.CbctSolverParams(int(iterations), float(beta), float(gamma), int(nonneg), int(use_graph),
+                                 int(storage), int(refine_every))
+        L.call("cbct_osmom_solve", self._h, _ptr(b), _ptr(x0), _ptr(z_out), C.byref(prm), _ptr(resid),
+               _stream(stream))
+        return z_out
+
+    def ossart(self, b, x_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
+               cost=None, stream=None):
+        prm = L.CbctSolverParams(int(iterations), float(beta), float(gamma), int(nonneg), int(use_graph),
+                                 L.CBCT_F32, 0)
+        L.call("cbct_ossart_solve", self._h, _ptr(b), _ptr(x0), _ptr(x_out), C.byref(prm), _ptr(cost),
+               _stream(stream))
+        return x_out
+
+
+def phantom_voxelize(g: L.CbctGeometry, ell_dev, out, supersample=4, stream=None):
+    _need_cuda_f32(out, (g.nz, g.ny, g.nx), "volume")
+    n = ell_dev.numel() // 10
+    L.call("cbct_phantom_voxelize", C.byref(g), _ptr(ell_dev), n, int(supersample), _ptr(out), _stream(stream))
+    return out
+
+
+def reduce_f64(kind: int, a, b=None, stream=None):
+    """kind 0 = dot(a,b), 1 = sum of squares, 2 = asum; returns a CUDA float64 scalar tensor."""
+    T = torch()
+    out = T.zeros(1, dtype=T.float64, device=a.device)
+    L.call("cbct_reduce_f64", kind, _ptr(a), _ptr(b), a.numel(), _ptr(out), _stream(stream))
+    return out
+
+
+def osmom_update(z, xold, precon, g, step, mom, nonneg=False, stream=None):
+    L.call("cbct_osmom_update", _ptr(z), _ptr(xold), _ptr(precon), _ptr(g), z.numel(), float(step), float(mom),
+           int(nonneg), _stream(stream))
+
+
+def convert(src, dst, dtype, stream=None):
+    L.call("cbct_convert", _ptr(src), _ptr(dst), src.numel(), dtype, _stream(stream))
+    return dst
+
+
+# ----------------------------------------------------------------- operators
+class cuConebeamProjectionOperator:
+    """Device-array cone-beam operator of one bin set (cuConebeamProjectionOperator.h:21-53).
+
+    Differences from the reference, on purpose: use_offset_correction starts
+    False (the reference leaves it uninitialised unless the override fires,
+    .cpp:15-21), and the default binning holds every view (the reference sizes
+    it from an empty member vector, .cpp:183-187)."""
+
+    def __init__(self):
+        self.samples_per_pixel = 1.5
+        self.allow_offset_correction_override = True
+        self.use_offset_correction = False
+        self.short_scan = False
+        self.preprocessed = False
+        self.domain_dims = None
+        self.plans = []
+        self.mask = None
+
+    def setup(self, acquisition: CBCT_acquisition, binning: Optional[CBCT_binning] = None,
+              is_dims_in_mm=None, transform_angles: bool = True, is_dims=None):
+        """cuConebeamProjectionOperator::setup (.cpp:148-206)."""
+        geo = acquisition.geometry
+        angles = geo.angles
+        if transform_angles:
+            geo.set_angles(angles - angles.min())
+        g0 = _cgeom(geo, 1, 1, (1, 1, 1), (1, 1, 1), self.samples_per_pixel)
+        self.short_scan = is_short_scan(g0, geo.angles)
+        if self.allow_offset_correction_override and offset_override(g0, geo.offsets):
+            self.use_offset_correction = True
+        self.binning = binning if binning is not None else CBCT_binning([list(range(geo.angles.size))])
+        self.acquisition = acquisition
+        self.is_dims_in_mm = tuple(float(v) for v in is_dims_in_mm)
+        self.bin_angles = [geo.angles[np.asarray(b, np.int64)] for b in self.binning.bins]
+        self.bin_offsets = [geo.offsets[np.asarray(b, np.int64)] for b in self.binning.bins]
+        proj = acquisition.projections
+        if proj is not None:
+            order = np.asarray([v for b in self.binning.bins for v in b], np.int64)
+            acquisition.set_projections(np.ascontiguousarray(proj[order]))
+        self.preprocessed = True
+        if is_dims is not None:
+            self.set_domain_dimensions(is_dims)
+
+    def set_domain_dimensions(self, dims):
+        """dims in Gadgetron order: (nx, ny, nz[, bins])."""
+        self.domain_dims = tuple(int(d) for d in dims)
+        self._make_plans()
+
+    def _make_plans(self):
+        if not self.preprocessed or self.domain_dims is None:
+            return
+        for p in self.plans:
+            p.close()
+        self.plans = []
+        proj = self.acquisition.projections
+        H, W = (proj.shape[1], proj.shape[2]) if proj is not None else self._detector
+        for a, o in zip(self.bin_angles, self.bin_offsets):
+            g = _cgeom(self.acquisition.geometry, W, H, self.domain_dims[:3], self.is_dims_in_mm,
+                       self.samples_per_pixel)
+            self.plans.append(Plan(g, a, o, None, [int(self.use_offset_correction)]) if a.size else None)
+
+    def set_detector(self, W: int, H: int):
+        self._detector = (H, W)
+
+    def set_use_offset_correction(self, use: bool):
+        self.use_offset_correction = bool(use)
+        self.allow_offset_correction_override = False
+        self._make_plans()
+
+    def get_use_offset_correction(self) -> bool:
+        return self.use_offset_correction
+
+    def set_mask(self, mask):
+        raise NotImplementedError("voxel masks (apply_mask) are not implemented in this build")
+
+    def _views(self, arr, per_bin, is_volume):
+        out, off = [], 0
+        for b, pl in enumerate(self.plans):
+            if is_volume:
+                out.append(arr[b] if arr.dim() == 4 else arr)
+            else:
+                n = len(self.binning.bins[b])
+                out.append(arr[off:off + n])
+                off += n
+        return out
+
+    def mult_M(self, x, out, accumulate=False, vol_dtype=L.CBCT_F32):
+        """cuConebeamProjectionOperator::mult_M (.cpp:38-80): no offset weight."""
+        vols = self._views(x, True, True)
+        projs = self._views(out, True, False)
+        for pl, v, p in zip(self.plans, vols, projs):
+            if pl is not None:
+                pl.forward(v, p, -1, accumulate, vol_dtype)
+        return out
+
+    def mult_MH(self, proj, out, accumulate=False):
+        """cuConebeamProjectionOperator::mult_MH (.cpp:82-116): sin^2 offset weight on a copy."""
+        vols = self._views(out, True, True)
+        projs = self._views(proj, True, False)
+        for pl, v, p in zip(self.plans, vols, projs):
+            if pl is not None:
+                pl.backproject(p, v, -1, 0, True, accumulate)
+        return out
+
+    def offset_correct(self, proj):
+        """apply_offset_correct: sqrt (sin) weight in place (conebeam_projection.cu:394-404)."""
+        for pl, p in zip(self.plans, self._views(proj, True, False)):
+            if pl is not None:
+                pl.offset_correct(p, -1, 1)
+        return proj
+
+
+class CBSubsetOperator:
+    """Ordered-subset cone-beam operator (CBSubsetOperator.h:30-72) on device arrays."""
+
+    def __init__(self, subsets: int = 1):
+        self.number_of_subsets = int(subsets)
+        self.samples_per_pixel = 1.5
+        self.domain_dims = None
+        self.plan: Optional[Plan] = None
+        self.use_offset_override = None
+
+    def setup(self, acq: CBCT_acquisition, binning: Optional[CBCT_binning] = None, is_dims_in_mm=None,
+              is_dims=None):
+        """CBSubsetOperator::setup (.cpp:52-158): permutes the acquisition in place."""
+        geo = acq.geometry
+        P = geo.angles.size
+        if binning is None:
+            binning = CBCT_binning([list(range(P))])
+        if binning.get_number_of_bins() != 1:
+            raise NotImplementedError("4-D binning is not supported by this build")
+        all_angles = geo.angles - geo.angles.min()
+        view_bin = np.full(P, -1, np.int32)
+        for b, views in enumerate(binning.bins):
+            view_bin[np.asarray(views, np.int64)] = b
+        order, sizes = subset_partition(P, self.number_of_subsets, view_bin)
+        self.permutation = order
+        self.subset_sizes = sizes
+        if acq.projections is not None:
+            acq.set_projections(np.ascontiguousarray(acq.projections[order]))
+        geo.set_angles(all_angles[order])
+        geo.set_offsets(geo.offsets[order])
+        self.acq = acq
+        self.is_dims_in_mm = tuple(float(v) for v in is_dims_in_mm)
+        # Per-subset offset-correction override (cuConebeamProjectionOperator.cpp:176-181).
+        g0 = _cgeom(geo, 1, 1, (1, 1, 1), (1, 1, 1), self.samples_per_pixel)
+        first = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        self.offcorr = np.array([
+            int(offset_override(g0, geo.offsets[f:f + n])) if n else 0 for f, n in zip(first, sizes)], np.int32)
+        if self.use_offset_override is not None:
+            self.offcorr[:] = int(self.use_offset_override)
+        self.first = first
+        if is_dims is not None:
+            self.set_domain_dimensions(is_dims)
+
+    def set_domain_dimensions(self, dims):
+        self.domain_dims = tuple(int(d) for d in dims)
+        self._make_plan()
+
+    def _make_plan(self):
+        if self.plan is not None:
+            self.plan.close()
+        proj = self.acq.projections
+        H, W = proj.shape[1], proj.shape[2]
+        g = _cgeom(self.acq.geometry, W, H, self.domain_dims[:3], self.is_dims_in_mm, self.samples_per_pixel)
+        self.plan = Plan(g, self.acq.geometry.angles, self.acq.geometry.offsets, self.subset_sizes, self.offcorr)
+
+    def set_use_offset_correction(self, use: bool):
+        self.use_offset_override = bool(use)
+        if hasattr(self, "offcorr"):
+            self.offcorr[:] = int(use)
+            if self.domain_dims is not None:
+                self._make_plan()
+
+    def get_number_of_subsets(self):
+        return self.number_of_subsets
+
+    def get_codomain_dimensions(self, subset: int):
+        return (self.plan.g.width, self.plan.g.height, int(self.subset_sizes[subset]))
+
+    def projection_subsets(self, projections):
+        """Contiguous views of each subset's projections (subsetOperator::projection_subsets)."""
+        return [projections[f:f + n] for f, n in zip(self.first, self.subset_sizes)]
+
+    def mult_M(self, x, out, subset: int = -1, accumulate=False):
+        if subset < 0:
+            for s, o in enumerate(self.projection_subsets(out)):
+                self.plan.forward(x, o, s, accumulate)
+            return out
+        return self.plan.forward(x, out, subset, accumulate)
+
+    def mult_MH(self, proj, out, subset: int = -1, accumulate=False):
+        if subset < 0:
+            if not accumulate:
+                out.zero_()
+            for s, p in enumerate(self.projection_subsets(proj)):
+                self.plan.backproject(p, out, s, 0, True, True)
+            return out
+        return self.plan.backproject(proj, out, subset, 0, True, accumulate)
+
+    def mult_MH_M(self, x, out, subset: int, accumulate=False):
+        T = torch()
+        tmp = T.empty(self.plan.proj_shape(subset), dtype=T.float32, device=x.device)
+        self.mult_M(x, tmp, subset, False)
+        return self.mult_MH(tmp, out, subset, accumulate)
+
+    def offset_correct(self, projections):
+        """CBSubsetOperator::offset_correct (.cpp:44-50): sqrt weight on subsets with correction."""
+        for s, p in enumerate(self.projection_subsets(projections)):
+            if self.offcorr[s]:
+                self.plan.offset_correct(p, s, 1)
+        return projections
+
+
+class hoCuConebeamProjectionOperator:
+    """Host-array operator with optional FDK (hoCuConebeamProjectionOperator.h:17-156).
+
+    Host arrays are numpy float32 of shape (P, H, W) / (nz, ny, nx).  Whole
+    bins are staged on the device at once (B200 HBM holds the configs' data);
+    the reference's 20-view batching (.h:23) is accepted and ignored."""
+
+    def __init__(self):
+        self.samples_per_pixel = 1.5
+        self.projections_per_batch = 20
+        self.use_fbp = False
+        self.short_scan = False
+        self.preprocessed = False
+        self.use_offset_correction = False
+        self.allow_offset_correction_override = True
+        self.frequency_filter = None
+        self.domain_dims = None
+
+    def setup(self, acquisition: CBCT_acquisition, binning: Optional[CBCT_binning] = None, is_dims_in_mm=None,
+              transform_angles=True, is_dims=None):
+        geo = acquisition.geometry
+        if transform_angles:
+            geo.set_angles(geo.angles - geo.angles.min())
+        g0 = _cgeom(geo, 1, 1, (1, 1, 1), (1, 1, 1), self.samples_per_pixel)
+        self.short_scan = is_short_scan(g0, geo.angles)
+        if self.allow_offset_correction_override and offset_override(g0, geo.offsets):
+            self.use_offset_correction = True
+        self.acquisition = acquisition
+        self.binning = binning if binning is not None else CBCT_binning([list(range(geo.angles.size))])
+        self.is_dims_in_mm = tuple(float(v) for v in is_dims_in_mm)
+        self.preprocessed = True
+        if is_dims is not None:
+            self.domain_dims = tuple(int(d) for d in is_dims)
+
+    def set_domain_dimensions(self, dims):
+        self.domain_dims = tuple(int(d) for d in dims)
+
+    def set_use_filtered_backprojection(self, use: bool):
+        self.use_fbp = bool(use)
+
+    def set_use_offset_correction(self, use: bool):
+        self.use_offset_correction = bool(use)
+        self.allow_offset_correction_override = False
+
+    def get_use_offset_correction(self):
+        return self.use_offset_correction
+
+    def set_num_projections_per_batch(self, n: int):
+        self.projections_per_batch = int(n)
+
+    def set_num_samples_per_pixel(self, spp: float):
+        self.samples_per_pixel = float(spp)
+
+    def set_frequency_filter(self, filt):
+        self.frequency_filter = np.ascontiguousarray(filt, np.float32)
+
+    def _plan(self, views, W, H):
+        geo = self.acquisition.geometry
+        g = _cgeom(geo, W, H, self.domain_dims[:3], self.is_dims_in_mm, self.samples_per_pixel)
+        idx = np.asarray(views, np.int64)
+        return Plan(g, geo.angles[idx], geo.offsets[idx], None, [int(self.use_offset_correction)])
+
+    def mult_M(self, image: np.ndarray, projections: np.ndarray, accumulate=False):
+        """hoCuConebeamProjectionOperator::mult_M (.cpp:104-176)."""
+        T = torch()
+        P, H, W = projections.shape
+        result = np.zeros_like(projections) if accumulate else projections
+        vol3 = image if image.ndim == 3 else None
+        for b, views in enumerate(self.binning.bins):
+            if not views:
+                continue
+            pl = self._plan(views, W, H)
+            v = T.from_numpy(np.ascontiguousarray(vol3 if vol3 is not None else image[b])).cuda()
+            out = T.empty(pl.proj_shape(), dtype=T.float32, device="cuda")
+            pl.forward(v, out)
+            if self.use_offset_correction and not self.use_fbp:
+                pl.offset_correct(out, -1, 1)
+            result[np.asarray(views, np.int64)] = out.cpu().numpy()
+        if accumulate:
+            projections += result
+        return projections
+
+    def mult_MH(self, projections: np.ndarray, image: np.ndarray, accumulate=False):
+        """hoCuConebeamProjectionOperator::mult_MH (.cpp:178-265), FDK when FBP is on."""
+        T = torch()
+        P, H, W = projections.shape
+        for b, views in enumerate(self.binning.bins):
+            tgt = image if image.ndim == 3 else image[b]
+            if not views:
+                if not accumulate:
+                    tgt[...] = 0
+                continue
+            pl = self._plan(views, W, H)
+            p = T.from_numpy(np.ascontiguousarray(projections[np.asarray(views, np.int64)])).cuda()
+            out = T.empty(pl.vol_shape, dtype=T.float32, device="cuda")
+            if self.use_fbp:
+                flags = (L.CBCT_FDK_PARKER if self.short_scan else 0) | \
+                        (L.CBCT_FDK_OFFSET if self.use_offset_correction else 0)
+                pl.fdk(p, out, self.frequency_filter, flags)
+                res = out.cpu().numpy()
+                if accumulate:
+                    tgt *= 2.0 / float(len(views))
+                    tgt += res
+                else:
+                    tgt[...] = res
+            else:
+                if self.use_offset_correction:
+                    pl.offset_correct(p, -1, 1)
+                if accumulate:
+                    out.copy_(T.from_numpy(np.ascontiguousarray(tgt)))
+                pl.backproject(p, out, -1, 0, False, accumulate)
+                tgt[...] = out.cpu().numpy()
+        return image
+
+
+# ----------------------------------------------------------------- solvers
+class osMOMSolverD:
+    """osMOMSolverD<cuNDArray<float>> without regularisers (solvers/osMOMSolverD.h:19-329).
+
+    solve() runs the whole loop on the device (cbct_osmom_solve).  The
+    per-iteration dump files of the reference (:184-189) are not written;
+    set_dump is accepted for interface compatibility."""
+
+    def __init__(self):
+        self._iterations = 10
+        self._beta = 1.0
+        self._gamma = 0.0
+        self.non_negativity = False
+        self.x0 = None
+        self.E: Optional[CBSubsetOperator] = None
+        self.use_graph = False
+        self.storage = L.CBCT_F32
+        self.refine_every = 0
+        self.residual_norms = None
+
+    def set_max_iterations(self, i):
+        self._iterations = int(i)
+
+    def get_max_iterations(self):
+        return self._iterations
+
+    def set_non_negativity_constraint(self, v=True):
+        self.non_negativity = bool(v)
+
+    def set_beta(self, b):
+        self._beta = float(b)
+
+    def set_gamma(self, g):
+        self._gamma = float(g)
+
+    def set_dump(self, d):
+        pass
+
+    def set_x0(self, x0):
+        self.x0 = x0
+
+    def set_encoding_operator(self, E):
+        self.E = E
+
+    def add_regularization_operator(self, *a, **k):
+        raise NotImplementedError("regularised OS-MOM is outside this build's scope")
+
+    def solve(self, projections):
+        T = torch()
+        E = self.E
+        if E is None:
+            raise RuntimeError("osMOMSolverD: no encoding operator is set")
+        if E.domain_dims is None:
+            raise RuntimeError("osMOMSolverD: encoding operator has not set domain dimension")
+        z = T.empty(E.plan.vol_shape, dtype=T.float32, device=projections.device)
+        S = E.get_number_of_subsets()
+        self.residual_norms = T.zeros(self._iterations * S, dtype=T.float64, device=projections.device)
+        E.plan.osmom(projections, z, self.x0, self._iterations, self._beta, self._gamma, self.non_negativity,
+                     self.use_graph, self.storage, self.refine_every, self.residual_norms)
+        return z
+
+
+class osSARTSolver:
+    """osSARTSolver<cuNDArray<float>> (solvers/osSARTSolver.h:11-137); the per-iteration
+    .real files of the reference (:117-121) are not written."""
+
+    def __init__(self):
+        self._iterations = 10
+        self._beta = 1.0
+        self._gamma = 0.0
+        self.non_negativity = False
+        self.x0 = None
+        self.E = None
+        self.use_graph = False
+        self.costs = None
+
+    def set_max_iterations(self, i):
+        self._iterations = int(i)
+
+    def set_non_negativity_constraint(self, v=True):
+        self.non_negativity = bool(v)
+
+    def set_beta(self, b):
+        self._beta = float(b)
+
+    def set_gamma(self, g):
+        self._gamma = float(g)
+
+    def set_x0(self, x0):
+        self.x0 = x0
+
+    def set_encoding_operator(self, E):
+        self.E = E
+
+    def solve(self, projections):
+        T = torch()
+        E = self.E
+        x = T.empty(E.plan.vol_shape, dtype=T.float32, device=projections.device)
+        self.costs = T.zeros(self._iterations, dtype=T.float64, device=projections.device)
+        E.plan.ossart(projections, x, self.x0, self._iterations, self._beta, self._gamma, self.non_negativity,
+                      self.use_graph, self.costs)
+        return x
+
+
+def fdk_reconstruct_3d(acquisition: CBCT_acquisition, is_dims, is_dims_in_mm, filt=None, binning=None):
+    """The FDK recipe of FDK_reconstruct_3d.cpp:135-161: FDK, then a least-squares
+    rescale s = <A x, p>/<A x, A x>.  Runs on the device; returns a host volume."""
+    T = torch()
+    E = hoCuConebeamProjectionOperator()
+    E.setup(acquisition, binning, is_dims_in_mm, is_dims=is_dims)
+    E.set_use_filtered_backprojection(True)
+    if filt is not None:
+        E.set_frequency_filter(filt)
+    P, H, W = acquisition.projections.shape
+    views = list(range(P))
+    pl = E._plan(views, W, H)
+    p = T.from_numpy(np.ascontiguousarray(acquisition.projections)).cuda()
+    x = T.empty(pl.vol_shape, dtype=T.float32, device="cuda")
+    flags = (L.CBCT_FDK_PARKER if E.short_scan else 0) | (L.CBCT_FDK_OFFSET if E.use_offset_correction else 0)
+    pl.fdk(p, x, E.frequency_filter, flags)
+    tmp = T.empty_like(p)
+    pl.forward(x, tmp)
+    s = (reduce_f64(0, tmp, p) / reduce_f64(0, tmp, tmp)).item()
+    return (x.cpu().numpy() * np.float32(s)).astype(np.float32)

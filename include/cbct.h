@@ -1,0 +1,275 @@
+/* cbct.h -- C ABI of the B200 cone-beam projector and ordered-subset core.
+ *
+ * This is the drop-in boundary for gt-tomography's circular-orbit cone-beam
+ * hot path.  Every entry point replaces one reference function or operator
+ * method (cited below by file:line within the gt-tomography project).  No C++
+ * types or exceptions cross this boundary: arguments are plain pointers and
+ * sizes, results are cbct_status codes.
+ *
+ * Layouts (identical to the reference's cuNDArray<float> arrays):
+ *   volume       (nx, ny, nz)   x fastest:  index = (k*ny + j)*nx + i
+ *   projections  (W, H, P)      u fastest:  index = (p*H + v)*W + u
+ *   offsets      (P, 2)         per view (offset_x, offset_y) in mm
+ * Views are held in subset-contiguous order: subset s owns views
+ * [first_s, first_s + size_s) where first_s is the sum of the sizes before it
+ * (the order CBSubsetOperator::setup leaves behind, CBSubsetOperator.cpp:100-115).
+ *
+ * Device pointers are CUDA global-memory pointers of the current device.
+ * All device work is enqueued on the caller's stream (0 = legacy default
+ * stream); no entry point synchronises the device unless documented.
+ */
+#ifndef CBCT_H_
+#define CBCT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CBCT_API __attribute__((visibility("default")))
+#else
+#define CBCT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CBCT_OK = 0,
+  CBCT_ERR_INVALID_ARGUMENT = 1, /* bad pointer, rank or size (conebeam_projection.cu:547-561) */
+  CBCT_ERR_CUDA = 2,             /* a CUDA runtime call failed (CHECK_FOR_CUDA_ERROR in the reference) */
+  CBCT_ERR_OUT_OF_MEMORY = 3,
+  CBCT_ERR_UNSUPPORTED = 4,      /* geometry or dtype outside what this build implements */
+  CBCT_ERR_DEVICE_CHECK = 5,     /* a kernel's own range check recorded a violation */
+  CBCT_ERR_TIMEOUT = 6,          /* a bounded device-side wait expired */
+  CBCT_ERR_BUDGET = 7,           /* request exceeds the memory budget (serving loop) */
+  CBCT_ERR_CANCELLED = 8,
+  CBCT_ERR_INTERNAL = 9
+} cbct_status;
+
+typedef enum { CBCT_F32 = 0, CBCT_F16 = 1, CBCT_BF16 = 2 } cbct_dtype;
+
+/* Geometry in the units of CBCT_geometry (xray/CBCT_acquisition.h:24-120)
+ * plus the image grid of the operator setup (is_dims_in_mm). */
+typedef struct {
+  float SAD;               /* source-to-axis distance, mm */
+  float SDD;               /* source-to-detector distance, mm */
+  float fov_u, fov_v;      /* detector size in mm (CBCT_geometry::get_FOV) */
+  int32_t width, height;   /* detector pixels W, H */
+  int32_t nx, ny, nz;      /* volume voxels */
+  float lx, ly, lz;        /* volume size in mm (is_dims_in_mm) */
+  float samples_per_pixel; /* rays take (int)(spp*nx) samples; reference default 1.5
+                              (cuConebeamProjectionOperator.cpp:18) */
+} cbct_geometry;
+
+typedef struct cbct_plan cbct_plan;
+
+/* Flags of cbct_backproject. */
+#define CBCT_BP_OFFSET_WEIGHT 0x1u /* multiply the input by the sin^2 Wang weight first
+                                      (offset_correct_kernel, conebeam_projection.cu:233-262) */
+#define CBCT_BP_FDK_WEIGHT 0x2u    /* FDK 1/U^2 distance weight (conebeam_projection.cu:1009-1024) */
+
+/* Flags of cbct_fdk_filter / cbct_fdk. */
+#define CBCT_FDK_COSINE 0x1u   /* cosine pre-weight (hoCuConebeamProjectionOperator.cpp:64-102) */
+#define CBCT_FDK_PARKER 0x2u   /* Parker short-scan weight (conebeam_projection.cu:151-194) */
+#define CBCT_FDK_OFFSET 0x4u   /* sin^2 offset weight after filtering (conebeam_projection.cu:1516-1517) */
+#define CBCT_FDK_RAMP 0x8u     /* the row filter itself (conebeam_projection.cu:1504-1511) */
+
+/* ----------------------------------------------------------------------------
+ * Status and diagnostics
+ * ------------------------------------------------------------------------- */
+CBCT_API const char* cbct_status_string(cbct_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+CBCT_API const char* cbct_last_error(void);
+/* Library version string. */
+CBCT_API const char* cbct_version(void);
+
+/* ----------------------------------------------------------------------------
+ * Host-side setup helpers (pure host code; no device work)
+ * ------------------------------------------------------------------------- */
+
+/* Subset assignment of CBSubsetOperator<ARRAY>::setup (CBSubsetOperator.cpp:52-115):
+ * views with view_bin[i] >= 0 are dealt round-robin to n_subsets subsets in index
+ * order, each subset is sorted by bin, and order_out receives the concatenation.
+ * view_bin may be NULL (one bin holding every view).  *n_out = views placed. */
+CBCT_API cbct_status cbct_subset_partition(int32_t n_views, const int32_t* view_bin, int32_t n_subsets,
+                                  int32_t* order_out, int32_t* subset_sizes_out, int32_t* n_out);
+
+/* Default FDK frequency filter, length W+1, normalised to sum W+1
+ * (hoCuConebeamProjectionOperator::compute_default_frequency_filter, .cpp:26-62). */
+CBCT_API cbct_status cbct_default_frequency_filter(int32_t W, float* out);
+
+/* Cosine weights (W x H) of hoCuConebeamProjectionOperator::compute_cosine_weights (.cpp:64-102). */
+CBCT_API cbct_status cbct_cosine_weights(const cbct_geometry* g, float* out);
+
+/* Short-scan test (span <= pi + 3*delta) of hoCuConebeamProjectionOperator.h:57-65
+ * and cuConebeamProjectionOperator.cpp:166-174.  Angles must already start at 0. */
+CBCT_API cbct_status cbct_is_short_scan(const cbct_geometry* g, const float* angles_deg, int32_t n,
+                               int32_t* short_scan_out);
+
+/* Offset-correction override rule (|mean offset_x| > 0.1*fov_u) of
+ * cuConebeamProjectionOperator.cpp:176-181 / hoCuConebeamProjectionOperator.h:72-76. */
+CBCT_API cbct_status cbct_offset_override(const cbct_geometry* g, const float* offsets_xy, int32_t n,
+                                 int32_t* use_offset_correction_out);
+
+/* ----------------------------------------------------------------------------
+ * Plans: geometry resident on the device
+ * ------------------------------------------------------------------------- */
+
+/* Creates a plan for n_views views held in subset-contiguous order.
+ * angles_deg / offsets_xy are host arrays (n_views and 2*n_views floats).
+ * subset_sizes (n_subsets ints, summing to n_views) may be NULL for one subset.
+ * offset_correction (n_subsets ints, 0/1) selects the sin^2 input weight of
+ * cbct_backproject per subset (use_offset_correction_ of each
+ * cuConebeamProjectionOperator); NULL = all off.
+ * Replaces cuConebeamProjectionOperator::setup (.cpp:148-206) and the per-call
+ * thrust uploads of conebeam_projection.cu:600-601,1225-1226.  Allocates device
+ * memory; must not be called during stream capture. */
+CBCT_API cbct_status cbct_plan_create(const cbct_geometry* g, const float* angles_deg,
+                             const float* offsets_xy, int32_t n_views,
+                             const int32_t* subset_sizes, int32_t n_subsets,
+                             const int32_t* offset_correction, cbct_plan** plan_out);
+CBCT_API cbct_status cbct_plan_destroy(cbct_plan* plan);
+
+/* Number of views in subset s (s = -1: all views) and index of its first view. */
+CBCT_API cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_out,
+                             int32_t* count_out);
+
+/* Name of the forward-projector variant the plan selected ("tma-slab" or "gather"). */
+CBCT_API const char* cbct_plan_forward_variant(const cbct_plan* plan);
+
+/* Plan options (no reference counterpart; diagnostics of this library).
+ * CBCT_OPT_DEBUG_CHECKS: kernels record index-range violations and unconsumed
+ *   samples in the plan's flag word instead of only clamping.
+ * CBCT_OPT_FORCE_GATHER: use the global-gather forward projector. */
+#define CBCT_OPT_DEBUG_CHECKS 1
+#define CBCT_OPT_FORCE_GATHER 2
+CBCT_API cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value);
+
+/* Reads (and optionally clears) the plan's device flag words:
+ * flags_out[0] = range-check violations, flags_out[1] = expired bounded waits.
+ * Synchronises the device. */
+CBCT_API cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t reset);
+
+/* ----------------------------------------------------------------------------
+ * Operators
+ * ------------------------------------------------------------------------- */
+
+/* mult_M: forward projection of vol into the projections of subset s
+ * (s = -1: every view).  proj points at the subset's first projection.
+ * vol_dtype selects the volume storage type (CBCT_F32, CBCT_F16, CBCT_BF16);
+ * interpolation and accumulation are FP32; proj is float.
+ * Replaces conebeam_forwards_projection (conebeam_projection.cu:530-635) as
+ * called by cuConebeamProjectionOperator::mult_M (.cpp:38-80). */
+CBCT_API cbct_status cbct_forward(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol,
+                         float* proj, int32_t accumulate, void* stream);
+
+/* mult_MH: back-projection of the subset's projections into vol.
+ * flags: CBCT_BP_OFFSET_WEIGHT (weighted copy of the input, the input itself is
+ * not modified), CBCT_BP_FDK_WEIGHT.
+ * Replaces conebeam_backwards_projection (conebeam_projection.cu:1172-1299) as
+ * called by cuConebeamProjectionOperator::mult_MH (.cpp:82-116).  With
+ * use_plan_offset = 1 the plan's per-subset offset_correction flag is OR-ed in. */
+CBCT_API cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, float* vol,
+                             uint32_t flags, int32_t use_plan_offset, int32_t accumulate,
+                             void* stream);
+
+/* Wang offset weight in place on the subset's projections.
+ * variant 0: sin^2 with zeroing (offset_correct_kernel, conebeam_projection.cu:233-262);
+ * variant 1: sin (offset_correct_kernel_sqrt, :303-331; apply_offset_correct, :369-404). */
+CBCT_API cbct_status cbct_offset_correct(cbct_plan* plan, int32_t s, float* proj, int32_t variant,
+                                void* stream);
+
+/* FDK pre-processing of the subset's projections, proj_in -> proj_out (may alias):
+ * [cosine] -> [Parker] -> [ramp filter] -> [sin^2 offset], per the flags.
+ * filter: host array of W+1 floats, or NULL for the default filter.
+ * Replaces the per-batch FBP block of conebeam_projection.cu:1483-1521 (with
+ * cb_fft/cb_ifft :87-139); the filter is a hand-written shared-memory FFT. */
+CBCT_API cbct_status cbct_fdk_filter(cbct_plan* plan, int32_t s, const float* proj_in, float* proj_out,
+                            const float* filter, uint32_t flags, void* stream);
+
+/* Whole FDK of hoCuConebeamProjectionOperator::mult_MH with filtered
+ * back-projection (hoCuConebeamProjectionOperator.cpp:235-254): every view of
+ * the plan is one bin; FDK pre-processing as cbct_fdk_filter with
+ * flags | CBCT_FDK_RAMP | CBCT_FDK_COSINE, 1/U^2-weighted back-projection,
+ * then vol *= 2/P.  work: device scratch of at least W*H*P floats (the
+ * filtered projections), or NULL to use a plan-owned buffer. */
+CBCT_API cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float* filter,
+                     uint32_t flags, float* work, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Solver building blocks
+ * ------------------------------------------------------------------------- */
+
+/* Fused residual forward projection used by the ordered-subset solvers:
+ *   r = w_off(u) * (A_s vol - b_s) * scale          (weight when apply_offset)
+ * and, when norm2_out is not NULL, norm2_out[0] = sum (A_s vol - b_s)^2 in FP64
+ * (the VERBOSE residual norm of osMOMSolverD.h:147-149).
+ * Replaces mult_M + "-= subsets[s]" + the offset-weighted copy inside mult_MH
+ * (osMOMSolverD.h:144-145, cuConebeamProjectionOperator.cpp:101-102). */
+CBCT_API cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype,
+                                  const void* vol, const float* b, float* r, float scale,
+                                  int32_t apply_offset, double* norm2_out, void* stream);
+
+/* One OS-MOM update (osMOMSolverD.h:155-175 without regularisers):
+ *   zt = z - step * precon * g ; x = nonneg ? max(zt,0) : zt
+ *   z  = x*(1+mom) - mom*xold ; xold = x                                  */
+CBCT_API cbct_status cbct_osmom_update(float* z, float* xold, const float* precon, const float* g,
+                              size_t n, float step, float mom, int32_t nonneg, void* stream);
+
+/* FP64 reductions: kind 0 = dot(a,b), 1 = nrm2(a)^2 (sum of squares),
+ * 2 = asum(a).  out_dev: one double in device memory. */
+CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t n,
+                            double* out_dev, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Solvers (device-resident loops)
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+  int32_t iterations;      /* default 10 (osMOMSolverD.h:23) */
+  float beta;              /* default 1 */
+  float gamma;             /* default 0 */
+  int32_t non_negativity;  /* clamp x at 0 after each update */
+  int32_t use_graph;       /* capture one iteration in a CUDA graph and replay it */
+  cbct_dtype storage;      /* storage type of the forward projector's volume input */
+  int32_t refine_every;    /* mixed precision: FP32 forward every n iterations (0 = never) */
+} cbct_solver_params;
+
+/* osMOMSolverD<cuNDArray<float>>::solve without regularisers
+ * (solvers/osMOMSolverD.h:82-196) on the plan's subsets.
+ * b: measured projections (subset-contiguous), x0: initial image or NULL,
+ * z_out: result (the momentum point z, as the reference returns).
+ * resid_norm2_out: NULL or device array of iterations*n_subsets doubles that
+ * receives ||A_s x - b_s||^2 of every subset step. */
+CBCT_API cbct_status cbct_osmom_solve(cbct_plan* plan, const float* b, const float* x0, float* z_out,
+                             const cbct_solver_params* params, double* resid_norm2_out,
+                             void* stream);
+
+/* osSARTSolver<cuNDArray<float>>::solve (solvers/osSARTSolver.h:33-126):
+ * cost_out: NULL or device array of `iterations` doubles, ||A x - b||^2 after
+ * each iteration (the "Function value" print of :110-116). */
+CBCT_API cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, float* x_out,
+                              const cbct_solver_params* params, double* cost_out, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Synthetic phantoms (seeded ellipsoids; used by the benchmarks and tests)
+ * Ellipsoid record (10 floats): cx cy cz ax ay az phi theta psi density,
+ * rotation R = Rz(phi) Ry(theta) Rx(psi).
+ * ------------------------------------------------------------------------- */
+CBCT_API cbct_status cbct_phantom_voxelize(const cbct_geometry* g, const float* ellipsoids_dev,
+                                  int32_t n_ellipsoids, int32_t supersample, float* vol,
+                                  void* stream);
+/* Exact line integrals of the box-truncated phantom along every ray of subset s. */
+CBCT_API cbct_status cbct_phantom_project(cbct_plan* plan, int32_t s, const float* ellipsoids_dev,
+                                 int32_t n_ellipsoids, float* proj, void* stream);
+
+/* Element-wise conversion of n floats to a 16-bit storage type (dst_dtype). */
+CBCT_API cbct_status cbct_convert(const float* src, void* dst, size_t n, cbct_dtype dst_dtype,
+                         void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CBCT_H_ */

@@ -436,6 +436,39 @@ def ours(args, wl: Workload):
         torch.distributed.destroy_process_group()
 
 
+def kernel_only(args, wl: Workload):
+    """Runs one kernel of the workload `--steps` times after `--warmup` launches
+    (for profiler captures): forward = forward residual of subset 0,
+    backproject = back-projection with the OS-MOM update of subset 0."""
+    import torch
+    dev = torch.device("cuda", 0)
+    gtb = _package()
+    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev)
+    n0 = int(sizes[0])
+    vol = torch.full(plan.vol_shape, 0.01, dtype=torch.float32, device=dev)
+    r = torch.empty(plan.proj_shape(0), dtype=torch.float32, device=dev)
+    bs = b[:n0].contiguous()
+    stream = torch.cuda.current_stream()
+
+    def one():
+        if args.only == "forward":
+            plan.forward_residual(vol, bs, r, 0, 1.0, bool(oc[0]), None)
+        else:
+            plan.backproject(bs, vol, 0, 0, False, True)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one()
+    e1.record(stream)
+    e1.synchronize()
+    print(json.dumps({"kernel": args.only, "ms_per_launch": e0.elapsed_time(e1) / max(args.steps, 1),
+                      "variant": plan.forward_variant(), "views": n0}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,8 +477,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", choices=["forward", "backproject"], default=None,
+                    help="time one kernel of the workload (profiling)")
     args = ap.parse_args()
     wl = Workload(args.config)
+    if args.only:
+        kernel_only(args, wl)
+        return
     if args.impl == "reference":
         reference_arm(args, wl)
     else:

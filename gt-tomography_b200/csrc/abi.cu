@@ -158,6 +158,7 @@ static void plan_free(cbct_plan* p) {
   cudaFree(p->d_partials);
   cudaFree(p->d_flags);
   cudaFree(p->d_fdk_work);
+  cudaFree(p->d_volT);
   cudaFree(p->ws);
   delete p;
 }
@@ -206,6 +207,7 @@ static cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const
   CBCT_CUDA(cudaMemset(p->d_flags, 0, sizeof(int) * 4));
   forward_choose_variant(p.get());
   forward_prepare(p.get());
+  backproject_choose_variant(p.get());
   backproject_prepare(p.get());
   return p.release();
 }
@@ -361,6 +363,8 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
       plan->force_gather = value != 0;
       forward_choose_variant(plan);
       forward_prepare(plan);
+      backproject_choose_variant(plan);
+      backproject_prepare(plan);
     } else {
       throw Error(CBCT_ERR_INVALID_ARGUMENT, "unknown option");
     }
@@ -394,12 +398,27 @@ cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, floa
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(vol && proj, "NULL array");
     CBCT_REQUIRE((flags & ~(CBCT_BP_OFFSET_WEIGHT | CBCT_BP_FDK_WEIGHT)) == 0, "unknown flags");
-    const bool off = (flags & CBCT_BP_OFFSET_WEIGHT) || (use_plan_offset && plan->offcorr[i]);
+    const size_t plane = (size_t)plan->g.width * plan->g.height;
+    // Which views get the weight: every view of the call with the explicit flag,
+    // else the subsets whose offset correction is on (all subsets when s = -1).
+    bool any = (flags & CBCT_BP_OFFSET_WEIGHT) != 0;
+    if (!any && use_plan_offset) {
+      if (i < plan->n_subsets) any = plan->offcorr[i] != 0;
+      else for (int k = 0; k < plan->n_subsets; ++k) any = any || plan->offcorr[k] != 0;
+    }
     const float* in = proj;
-    if (off) {
+    if (any) {
       // mult_MH copies the input and weights the copy (cuConebeamProjectionOperator.cpp:101-102).
-      float* w = proj_scratch(plan, (size_t)plan->g.width * plan->g.height * plan->count[i]);
-      offset_weight_launch(plan, i, proj, w, 0, S(stream));
+      float* w = proj_scratch(plan, plane * plan->count[i]);
+      if ((flags & CBCT_BP_OFFSET_WEIGHT) || i < plan->n_subsets) {
+        offset_weight_launch(plan, i, proj, w, 0, S(stream));
+      } else {
+        for (int k = 0; k < plan->n_subsets; ++k) {
+          const size_t o = plane * plan->first[k], n = plane * plan->count[k];
+          if (plan->offcorr[k]) offset_weight_launch(plan, k, proj + o, w + o, 0, S(stream));
+          else if (n) CBCT_CUDA(cudaMemcpyAsync(w + o, proj + o, n * sizeof(float), cudaMemcpyDeviceToDevice, S(stream)));
+        }
+      }
       in = w;
     }
     backproject_launch(plan, i, in, vol, (flags & CBCT_BP_FDK_WEIGHT) ? 1 : 0, accumulate, 1.f, S(stream));

@@ -19,6 +19,10 @@
 //  kRecip : vol = 1 / max(sum, 1e-6)                                (precon, osMOMSolverD.h:115-120)
 //  kMom   : OS-MOM update of z and xold                              (osMOMSolverD.h:155-175)
 //  kSart  : x = x + step * V * sum, optional clamp                   (osSARTSolver.h:99-104)
+#include <climits>
+#include <cmath>
+#include <cstring>
+
 #include "device_common.cuh"
 
 namespace cbct {
@@ -39,6 +43,24 @@ struct BpEpi {
   int nonneg;
   int accumulate;
 };
+
+template <int EPI>
+__device__ __forceinline__ void bp_store(const BpEpi& e, size_t idx, float g) {
+  if (EPI == kStore) {
+    e.vol[idx] = e.scale * ((e.accumulate ? e.vol[idx] : 0.f) + g);
+  } else if (EPI == kRecip) {
+    e.vol[idx] = 1.f / fmaxf(g, 1e-6f);
+  } else if (EPI == kMom) {
+    const float zt = fmaf(-e.scale, e.aux[idx] * g, e.vol[idx]);
+    const float xc = e.nonneg ? fmaxf(zt, 0.f) : zt;
+    e.vol[idx] = fmaf(-e.mom, e.xold[idx], xc * (1.f + e.mom));
+    e.xold[idx] = xc;
+  } else {  // kSart
+    float xn = fmaf(e.scale, e.aux[idx] * g, e.vol[idx]);
+    if (e.nonneg) xn = fmaxf(xn, 0.f);
+    e.vol[idx] = xn;
+  }
+}
 
 template <int EPI, bool FDK>
 __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__ proj,
@@ -111,28 +133,220 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__
 #pragma unroll
   for (int q = 0; q < kZB; ++q) {
     if (k0 + q >= gc.nz) break;
-    const size_t idx = base + q * sz;
-    const float g = acc[q];
-    if (EPI == kStore) {
-      e.vol[idx] = e.scale * ((e.accumulate ? e.vol[idx] : 0.f) + g);
-    } else if (EPI == kRecip) {
-      e.vol[idx] = 1.f / fmaxf(g, 1e-6f);
-    } else if (EPI == kMom) {
-      const float zt = fmaf(-e.scale, e.aux[idx] * g, e.vol[idx]);
-      const float xc = e.nonneg ? fmaxf(zt, 0.f) : zt;
-      e.vol[idx] = fmaf(-e.mom, e.xold[idx], xc * (1.f + e.mom));
-      e.xold[idx] = xc;
-    } else {  // kSart
-      float xn = fmaf(e.scale, e.aux[idx] * g, e.vol[idx]);
-      if (e.nonneg) xn = fmaxf(xn, 0.f);
-      e.vol[idx] = xn;
+    bp_store<EPI>(e, base + q * sz, acc[q]);
+  }
+}
+
+// ------------------------------------------------------------------ TMA-staged
+// A CTA owns a 32 x 4 x kZT voxel block.  For each view the block's footprint
+// on the detector (the bounding box of its eight projected corners, a convex
+// image of a convex block) is staged into shared memory by a 3-D TMA load
+// whose out-of-detector texels arrive as zeros, so the bilinear taps need no
+// bounds checks.  Views are pipelined over two stages.
+constexpr int kZT = 16;
+constexpr uint32_t kBpWaitLimit = 1u << 22;
+
+struct BpView {
+  float cs, sn, ox, oy;
+};
+
+template <int EPI, bool FDK, int BU>
+__global__ void __launch_bounds__(kBX * kBY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                           const ViewParams* __restrict__ views, int n_views,
+                                                           GridConst gc, BpEpi e, int BV, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ uint64_t bars[2];
+  __shared__ int abort_flag;
+  unsigned char* base_ptr =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  const uint32_t box_bytes = uint32_t(BU * BV * 4);
+  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
+  float* stage0 = reinterpret_cast<float*>(base_ptr);
+  BpView* tv = reinterpret_cast<BpView*>(base_ptr + 2 * stage_stride);
+  int2* org = reinterpret_cast<int2*>(tv + n_views);     // per view: (u origin, v origin)
+  int2* ext = org + n_views;                             // per view: (max u, max v) for checks
+  const int tid = threadIdx.y * kBX + threadIdx.x;
+  const int nthr = kBX * kBY;
+  const int i0 = blockIdx.x * kBX, j0 = blockIdx.y * kBY, k0 = blockIdx.z * kZT;
+
+  for (int q = tid; q < n_views; q += nthr) {
+    const ViewParams& vp = views[q];
+    tv[q] = BpView{vp.cs, vp.sn, vp.ox, vp.oy};
+    org[q] = make_int2(INT_MAX, INT_MAX);
+    ext[q] = make_int2(INT_MIN, INT_MIN);
+  }
+  if (tid == 0) {
+    abort_flag = 0;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // Footprints: 8 corners of the block (voxel centres) per view.
+  const int ie = min(i0 + kBX, gc.nx) - 1, je = min(j0 + kBY, gc.ny) - 1, ke = min(k0 + kZT, gc.nz) - 1;
+  for (int q = tid; q < n_views * 8; q += nthr) {
+    const int pv = q >> 3, c = q & 7;
+    const BpView w = tv[pv];
+    const float x = fmaf(float((c & 1) ? ie : i0) + 0.5f, gc.vx, -gc.hx);
+    const float y = fmaf(float((c & 2) ? je : j0) + 0.5f, gc.vy, -gc.hy);
+    const float z = fmaf(float((c & 4) ? ke : k0) + 0.5f, gc.vz, -gc.hz);
+    const float xr = fmaf(w.cs, x, w.sn * y);
+    const float yr = fmaf(-w.sn, x, w.cs * y);
+    const float inv = __frcp_rn(yr + gc.SAD);
+    const float cu = fmaf(fmaf(gc.SDD * xr, inv, -w.ox), gc.ku, gc.bu);
+    const float cv = fmaf(fmaf(gc.SDD * z, inv, -w.oy), gc.kv, gc.bv);
+    const int fu = int(floorf(fminf(fmaxf(cu, -1.0e5f), 1.0e5f)));
+    const int fv = int(floorf(fminf(fmaxf(cv, -1.0e5f), 1.0e5f)));
+    atomicMin(&org[pv].x, fu);
+    atomicMin(&org[pv].y, fv);
+    atomicMax(&ext[pv].x, fu);
+    atomicMax(&ext[pv].y, fv);
+  }
+  __syncthreads();
+  for (int q = tid; q < n_views; q += nthr) {
+    int2 o = org[q];
+    o.x = (o.x - 1) & ~3;      // 16-byte aligned x start
+    o.y = o.y - 1;
+    if (ext[q].x + 2 - o.x >= BU || ext[q].y + 2 - o.y >= BV) atomicAdd(&flags[0], 1);
+    org[q] = o;
+  }
+  __syncthreads();
+  auto issue = [&](int pv) {
+    uint64_t* bar = &bars[pv & 1];
+    mbar_arrive_expect_tx(bar, box_bytes);
+    tma_load_3d(base_ptr + (pv & 1) * stage_stride, &map, org[pv].x, org[pv].y, pv, bar);
+  };
+  if (tid == 0) {
+    for (int pv = 0; pv < min(2, n_views); ++pv) issue(pv);
+  }
+
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const float x = fmaf(float(min(i, gc.nx - 1)) + 0.5f, gc.vx, -gc.hx);
+  const float y = fmaf(float(min(j, gc.ny - 1)) + 0.5f, gc.vy, -gc.hy);
+  const float z0 = fmaf(float(k0) + 0.5f, gc.vz, -gc.hz);
+  const unsigned maxidx = unsigned(BU * (BV - 1) - 2);
+  float acc[kZT];
+#pragma unroll
+  for (int q = 0; q < kZT; ++q) acc[q] = 0.f;
+  int done = 0;
+  for (int pv = 0; pv < n_views; ++pv) {
+    const bool ok = mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kBpWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) { atomicAdd(&flags[1], 1); abort_flag = 1; }
+      break;
+    }
+    done = pv + 1;
+    const BpView w = tv[pv];
+    const int2 o = org[pv];
+    const float* sp = reinterpret_cast<const float*>(base_ptr + (pv & 1) * stage_stride);
+    const float xr = fmaf(w.cs, x, w.sn * y);
+    const float yr = fmaf(-w.sn, x, w.cs * y);
+    const float inv = __frcp_rn(yr + gc.SAD);
+    const float cu = fmaf(fmaf(gc.SDD * xr, inv, -w.ox), gc.ku, gc.bu) - float(o.x);
+    const float A = gc.SDD * inv * gc.kv;
+    float cv = fmaf(fmaf(A, z0, -w.oy * gc.kv), 1.f, gc.bv) - float(o.y);
+    const float dz = A * gc.vz;
+    float wt = 1.f;
+    if (FDK) {
+      const float U = 1.f - yr / gc.SAD;
+      wt = 1.f / (U * U);
+    }
+    const float fu = floorf(cu);
+    const float au = cu - fu;
+    const float2 tu = make_float2(au, au);
+    const float fub = fu;
+#pragma unroll
+    for (int q = 0; q < kZT; ++q) {
+      const float fv = floorf(cv);
+      const float av = cv - fv;
+      const int idx0 = int(fmaf(fv, float(BU), fub));
+      const unsigned idx = min((unsigned)idx0, maxidx);
+      const float* t = sp + idx;
+      const float2 r0 = make_float2(t[0], t[BU]);        // (u0,v0) (u0,v1)
+      const float2 r1 = make_float2(t[1], t[BU + 1]);    // (u1,v0) (u1,v1)
+      const float2 h = __ffma2_rn(tu, r1, __ffma2_rn(make_float2(-au, -au), r0, r0));
+      const float smp = fmaf(av, h.y - h.x, h.x);
+      acc[q] = FDK ? fmaf(wt, smp, acc[q]) : acc[q] + smp;
+      cv += dz;
+    }
+    __syncthreads();
+    if (tid == 0 && pv + 2 < n_views) {
+      fence_proxy_async();
+      issue(pv + 2);
     }
   }
+  if (abort_flag && tid == 0) {
+    for (int pv = done; pv < min(done + 2, n_views); ++pv)
+      (void)mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kBpWaitLimit);
+  }
+  if (i >= gc.nx || j >= gc.ny) return;
+  const size_t base = ((size_t)k0 * gc.ny + j) * gc.nx + i;
+  const size_t sz = (size_t)gc.nx * gc.ny;
+#pragma unroll
+  for (int q = 0; q < kZT; ++q) {
+    if (k0 + q >= gc.nz) break;
+    bp_store<EPI>(e, base + q * sz, acc[q]);
+  }
+}
+
+size_t bp_tma_smem(const cbct_plan* p, int n_views) {
+  const size_t stage = ((size_t)p->bp_box.bx * p->bp_box.by * 4 + 127) & ~size_t(127);
+  return 128 + 2 * stage + (size_t)n_views * (sizeof(BpView) + 2 * sizeof(int2));
+}
+
+template <int EPI, bool FDK, int BU>
+void launch_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const BpEpi& e, cudaStream_t st) {
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[3] = {(cuuint64_t)p->g.width, (cuuint64_t)p->g.height, (cuuint64_t)cnt};
+  cuuint64_t strides[2] = {(cuuint64_t)p->g.width * 4, (cuuint64_t)p->g.width * p->g.height * 4};
+  cuuint32_t box[3] = {(cuuint32_t)BU, (cuuint32_t)p->bp_box.by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult res = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(proj), dims,
+                                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (res != CUDA_SUCCESS) throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled (projections) failed");
+  dim3 block(kBX, kBY);
+  dim3 grid((p->g.nx + kBX - 1) / kBX, (p->g.ny + kBY - 1) / kBY, (p->g.nz + kZT - 1) / kZT);
+  const size_t smem = bp_tma_smem(p, cnt);
+  auto k = bp_tma_kernel<EPI, FDK, BU>;
+  ensure_smem_attr((const void*)k, smem);
+  k<<<grid, block, smem, st>>>(m, p->d_views + first, cnt, p->gc, e, p->bp_box.by, p->d_flags);
+  check_launch("bp_tma_kernel");
+}
+
+template <int EPI, bool FDK>
+bool try_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const BpEpi& e, cudaStream_t st) {
+  if (p->bp_variant != 1 || cnt > p->bp_max_views || (reinterpret_cast<uintptr_t>(proj) % 16) != 0) return false;
+  switch (p->bp_box.bx) {
+    case 40: launch_bp_tma<EPI, FDK, 40>(p, first, cnt, proj, e, st); return true;
+    case 56: launch_bp_tma<EPI, FDK, 56>(p, first, cnt, proj, e, st); return true;
+    case 72: launch_bp_tma<EPI, FDK, 72>(p, first, cnt, proj, e, st); return true;
+    case 104: launch_bp_tma<EPI, FDK, 104>(p, first, cnt, proj, e, st); return true;
+    case 136: launch_bp_tma<EPI, FDK, 136>(p, first, cnt, proj, e, st); return true;
+    default: return false;
+  }
+}
+
+template <int EPI, bool FDK, int BU>
+void prepare_bp_width(size_t smem) {
+  ensure_smem_attr((const void*)bp_tma_kernel<EPI, FDK, BU>, smem);
+}
+
+template <int BU>
+void prepare_bp_all(size_t smem) {
+  prepare_bp_width<kStore, false, BU>(smem);
+  prepare_bp_width<kStore, true, BU>(smem);
+  prepare_bp_width<kRecip, false, BU>(smem);
+  prepare_bp_width<kMom, false, BU>(smem);
+  prepare_bp_width<kSart, false, BU>(smem);
 }
 
 template <int EPI, bool FDK>
 void launch_bp(cbct_plan* p, int s, const float* proj, const BpEpi& e, cudaStream_t st) {
   const int first = p->first[s], cnt = p->count[s];
+  if (cnt == 0) return;
+  if (try_bp_tma<EPI, FDK>(p, first, cnt, proj, e, st)) return;
   if (cnt > kMaxViewsSmem) throw Error(CBCT_ERR_UNSUPPORTED, "more than 1024 views in one back-projection");
   dim3 block(kBX, kBY);
   dim3 grid((p->g.nx + kBX - 1) / kBX, (p->g.ny + kBY - 1) / kBY, (p->g.nz + kZB - 1) / kZB);
@@ -145,7 +359,76 @@ void launch_bp(cbct_plan* p, int s, const float* proj, const BpEpi& e, cudaStrea
 
 }  // namespace
 
+// Chooses the TMA-staged back-projector and its detector box: the largest
+// footprint of any 32 x 4 x kZT block in any view (FP64, corner projections),
+// plus margins.
+void backproject_choose_variant(cbct_plan* p) {
+  const cbct_geometry& g = p->g;
+  p->bp_variant = 0;
+  p->bp_box = SlabBox{0, 0, 0, 0};
+  p->bp_max_views = 0;
+  if (p->force_gather || (g.width * 4) % 16 != 0) return;
+  const double vx = double(g.lx) / g.nx, vy = double(g.ly) / g.ny, vz = double(g.lz) / g.nz;
+  const double ku = g.width / double(g.fov_u), kv = g.height / double(g.fov_v);
+  const double bu = g.width / 2.0 - 0.5, bv = g.height / 2.0 - 0.5;
+  int eu = 0, ev = 0;
+  const int bxn = (g.nx + kBX - 1) / kBX, byn = (g.ny + kBY - 1) / kBY, bzn = (g.nz + kZT - 1) / kZT;
+  for (int iv = 0; iv < p->n_views; ++iv) {
+    const double th = double(p->angles[iv]) * (3.14159265358979323846 / 180.0);
+    const double cs = std::cos(th), sn = std::sin(th);
+    const double ox = p->offsets[2 * iv], oy = p->offsets[2 * iv + 1];
+    for (int bi = 0; bi < bxn; ++bi)
+      for (int bj = 0; bj < byn; ++bj) {
+        const int i0 = bi * kBX, ie = std::min(i0 + kBX, g.nx) - 1;
+        const int j0 = bj * kBY, je = std::min(j0 + kBY, g.ny) - 1;
+        double umn = 1e30, umx = -1e30, imn = 1e30, imx = -1e30;
+        for (int c = 0; c < 4; ++c) {
+          const double x = (((c & 1) ? ie : i0) + 0.5) * vx - g.lx / 2.0;
+          const double y = (((c & 2) ? je : j0) + 0.5) * vy - g.ly / 2.0;
+          const double xr = cs * x + sn * y, yr = -sn * x + cs * y;
+          const double inv = 1.0 / (yr + g.SAD);
+          const double u = (g.SDD * xr * inv - ox) * ku + bu;
+          umn = std::min(umn, u); umx = std::max(umx, u);
+          imn = std::min(imn, inv); imx = std::max(imx, inv);
+        }
+        eu = std::max(eu, (int)(std::floor(umx) - std::floor(umn)) + 3 + 2);
+        // rows: z spans of every z block, at the nearest and farthest magnification
+        for (int bk = 0; bk < bzn; ++bk) {
+          const int k0 = bk * kZT, ke = std::min(k0 + kZT, g.nz) - 1;
+          const double z0 = (k0 + 0.5) * vz - g.lz / 2.0, z1 = (ke + 0.5) * vz - g.lz / 2.0;
+          double vmn = 1e30, vmx = -1e30;
+          for (double inv : {imn, imx})
+            for (double z : {z0, z1}) {
+              const double v = (g.SDD * z * inv - oy) * kv + bv;
+              vmn = std::min(vmn, v); vmx = std::max(vmx, v);
+            }
+          ev = std::max(ev, (int)(std::floor(vmx) - std::floor(vmn)) + 3 + 2);
+        }
+      }
+  }
+  int w = 0;
+  for (int c : kBoxWidths)
+    if (c >= eu + 3) { w = c; break; }
+  if (w == 0 || ev > 256) return;
+  p->bp_box = SlabBox{w, std::max(ev, 2), 1, 1};
+  const int maxv = std::min(p->n_views, 1024);
+  if (bp_tma_smem(p, maxv) > (size_t)kSmemBudget) return;
+  p->bp_max_views = maxv;
+  p->bp_variant = 1;
+}
+
 void backproject_prepare(cbct_plan* p) {
+  if (p->bp_variant == 1) {
+    const size_t sm = bp_tma_smem(p, p->bp_max_views);
+    switch (p->bp_box.bx) {
+      case 40: prepare_bp_all<40>(sm); break;
+      case 56: prepare_bp_all<56>(sm); break;
+      case 72: prepare_bp_all<72>(sm); break;
+      case 104: prepare_bp_all<104>(sm); break;
+      case 136: prepare_bp_all<136>(sm); break;
+      default: break;
+    }
+  }
   const size_t smem = sizeof(ViewParams) * (size_t)std::min(p->n_views, kMaxViewsSmem);
   ensure_smem_attr((const void*)bp_kernel<kStore, false>, smem);
   ensure_smem_attr((const void*)bp_kernel<kStore, true>, smem);

@@ -74,21 +74,27 @@ struct GridConst {
   float invN;
 };
 
-// Box configuration of the TMA slab forward projector for one dominant axis.
+// Box of the TMA slab forward projector, in the view's frame (e, d, z):
+// e = in-plane cross axis (memory x), d = slab axis (memory y), z.
 struct SlabBox {
   int bx, by, bz;         // TMA box (elements) in memory order x, y, z
   int valid;
 };
 
 // Forward projector tiling (compile-time): CTA = TU x TV rays of one view,
-// slabs of TS voxels along the dominant axis, NSTAGE-deep TMA pipeline.
+// slabs of TS voxels along the view's dominant in-plane axis, NSTAGE-deep
+// TMA pipeline.  The box holds TS+1 rows of the slab axis padded to kBoxY so
+// that neighbouring rows and planes fall in different shared-memory banks.
 constexpr int kTU = 16;
 constexpr int kTV = 16;
-constexpr int kTS = 16;
+constexpr int kTS = 8;
+constexpr int kBoxY = 10;
 constexpr int kNStage = 2;
-constexpr int kSlabBase = -4;      // slab m covers texel rows [kSlabBase + m*kTS, +kTS)
-constexpr int kMaxSlabs = 160;
+constexpr int kSlabBase = -1;      // slab m covers texel rows [kSlabBase + m*kTS, +kTS)
+constexpr int kMaxSlabs = 260;
 constexpr int kSmemBudget = 200 * 1024;
+// Box widths (memory x) the slab kernel is compiled for; each is 8 mod 16.
+constexpr int kBoxWidths[] = {40, 56, 72, 104, 136};
 
 }  // namespace cbct
 
@@ -106,8 +112,14 @@ struct cbct_plan {
 
   // forward variant: 0 = gather (global loads), 1 = TMA slab
   int fwd_variant = 0;
-  cbct::SlabBox slab[2]{};  // [0] x-dominant views, [1] y-dominant views
-  size_t slab_smem = 0;     // dynamic shared memory of the slab kernel (bytes)
+  cbct::SlabBox slab{};     // box in the view frame for fp32 storage (x starts aligned to 4)
+  cbct::SlabBox slab16{};   // box for 16-bit storage (x starts aligned to 8)
+  size_t slab_smem = 0;     // dynamic shared memory of the fp32 slab kernel (bytes)
+  std::vector<int> subset_has_xdom;  // per subset (and all-views entry): any x-dominant view
+  void* d_volT = nullptr;   // x/y-transposed volume for x-dominant views (fp32 capacity)
+  int bp_variant = 0;       // 0 = global loads, 1 = TMA-staged detector boxes
+  cbct::SlabBox bp_box{};   // detector box (bx = u width, by = v rows)
+  int bp_max_views = 0;     // views per launch the TMA back-projector holds
 
   // scratch owned by the plan (allocated at creation or first use, reused)
   float* d_proj_scratch = nullptr;  // weighted copies of projections (mult_MH with offset weight)
@@ -146,6 +158,7 @@ void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* 
                     double* norm2_out, cudaStream_t st);
 void forward_choose_variant(cbct_plan* p);
 // backproject.cu
+void backproject_choose_variant(cbct_plan* p);
 void backproject_prepare(cbct_plan* p);
 void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int fdk_weight,
                         int accumulate, float out_scale, cudaStream_t st);

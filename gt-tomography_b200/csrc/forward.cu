@@ -8,18 +8,20 @@
 //
 // Two variants:
 //  * fwd_slab_kernel (default): a CTA marches a 16x16 tile of rays of one view
-//    through the volume in slabs of kTS voxels along the view's dominant axis.
-//    Each slab's footprint (the box around the tile's ray pyramid) is staged
-//    into shared memory by a 3-D TMA load; out-of-volume texels arrive as zeros
-//    (the border rule for free).  Samples are taken in ray order, so each ray's
-//    sum has the same order as the reference.
-//  * fwd_gather_kernel: the same arithmetic with bounds-checked global loads.
-//    Used when the plan's geometry does not fit the slab box budget or the
-//    volume pitch is not TMA-aligned.
+//    through the volume in slabs of kTS voxels along the view's dominant
+//    in-plane axis.  Each slab's footprint (the box around the tile's ray
+//    pyramid) is staged into shared memory by a 3-D TMA load; out-of-volume
+//    texels arrive as zeros (the border rule for free).  Views whose rays run
+//    mostly along x read an x/y-transposed copy of the volume, so every slab is
+//    a range of memory rows and the box is never padded along its slab axis.
+//    Samples are taken in ray order, so each ray's sum has the reference's
+//    summation order.  Pairs of lerps run as packed FP32 (FFMA2).
+//  * fwd_gather_kernel: the same arithmetic with bounds-checked global loads,
+//    used when the geometry does not fit the slab boxes or the volume pitch is
+//    not TMA-aligned.
 #include <climits>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "device_common.cuh"
 
@@ -138,28 +140,27 @@ __global__ void __launch_bounds__(256) fwd_gather_kernel(const V* __restrict__ v
   fwd_epilogue(o, gc, vp, p, u, v, active, val, sh_red, tid);
 }
 
-// ------------------------------------------------------------------ slab/TMA
-template <class V, bool CHECK>
-__device__ __forceinline__ float tri_box(const V* __restrict__ s, int BX, int BXY, int mx, int my,
-                                         int mz, float lx, float ly, float lz, int& bad) {
-  const float fx = floorf(lx), fy = floorf(ly), fz = floorf(lz);
-  const float ax = lx - fx, ay = ly - fy, az = lz - fz;
-  int ix = int(fx), iy = int(fy), iz = int(fz);
-  if (CHECK) bad |= (ix < 0) | (ix > mx) | (iy < 0) | (iy > my) | (iz < 0) | (iz > mz);
-  ix = min(max(ix, 0), mx);
-  iy = min(max(iy, 0), my);
-  iz = min(max(iz, 0), mz);
-  const V* q = s + ix + iy * BX + iz * BXY;
-  const float v000 = sm_f(q[0]), v100 = sm_f(q[1]);
-  const float v010 = sm_f(q[BX]), v110 = sm_f(q[BX + 1]);
-  const float v001 = sm_f(q[BXY]), v101 = sm_f(q[BXY + 1]);
-  const float v011 = sm_f(q[BXY + BX]), v111 = sm_f(q[BXY + BX + 1]);
-  const float c00 = fmaf(ax, v100 - v000, v000), c10 = fmaf(ax, v110 - v010, v010);
-  const float c01 = fmaf(ax, v101 - v001, v001), c11 = fmaf(ax, v111 - v011, v011);
-  const float c0 = fmaf(ay, c10 - c00, c00), c1 = fmaf(ay, c11 - c01, c01);
-  return fmaf(az, c1 - c0, c0);
+// ------------------------------------------------------------------ transpose
+// volT[k][i][j] = vol[k][j][i]: the volume seen with x and y exchanged.
+template <class V>
+__global__ void transpose_xy_kernel(const V* __restrict__ in, V* __restrict__ out, int nx, int ny) {
+  __shared__ V tile[32][33];
+  const size_t plane = (size_t)nx * ny;
+  const V* src = in + blockIdx.z * plane;
+  V* dst = out + blockIdx.z * plane;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int x = x0 + threadIdx.x, y = y0 + j;
+    if (x < nx && y < ny) tile[j][threadIdx.x] = src[(size_t)y * nx + x];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int y = y0 + threadIdx.x, x = x0 + j;
+    if (x < nx && y < ny) dst[(size_t)x * ny + y] = tile[threadIdx.x][j];
+  }
 }
 
+// ------------------------------------------------------------------ slab/TMA
 struct SlabShared {
   uint64_t bars[kNStage];
   int mlo, mhi, abort_flag;
@@ -167,12 +168,93 @@ struct SlabShared {
   double red[8];
 };
 
-// DOM = 1: rays mostly along y (slabs are y ranges, the in-plane cross axis is x);
-// DOM = 0: rays mostly along x.
-template <class V, int DOM, bool CHECK>
-__device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, const ViewParams& vp,
-                         const GridConst& gc, const SlabBox& box, const FwdOut& o, int* flags,
-                         unsigned char* smem_raw, SlabShared& sh) {
+// Packed lerp of two pairs: a + t (b - a) as (a - t a) + t b.
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
+  const float2 nt = make_float2(-t.x, -t.y);
+  return __ffma2_rn(t, b, __ffma2_rn(nt, a, a));
+}
+
+// Samples of one ray inside one slab.  (ce, cd, cz) are frame texel
+// coordinates; the box origin is (oe, od, oz); BX and kBoxY are the box
+// strides.  Consumes samples while floor(cd) stays inside the slab.
+template <class V, int BX>
+struct SlabSample {
+  static constexpr int BXY = BX * kBoxY;
+  // Trilinear value of one sample whose frame coordinates are (ced.x, ced.y, cz)
+  // and whose floors are (fe, fd, fz).
+  static __device__ __forceinline__ float eval(const V* __restrict__ s, float2 ced, float cz, float fe, float fd,
+                                               float fz, float orgf, unsigned maxidx, int& bad, bool check) {
+    const float2 aed = __fadd2_rn(ced, make_float2(-fe, -fd));
+    const float az = cz - fz;
+    const float idxf = fmaf(fz, float(BXY), fmaf(fd, float(BX), fe)) - orgf;
+    const int idx0 = int(idxf);
+    if (check) bad |= (unsigned)idx0 > maxidx;
+    const unsigned idx = min((unsigned)idx0, maxidx);
+    const V* q = s + idx;
+    const float2 a0 = make_float2(sm_f(q[0]), sm_f(q[BX]));              // (e0,d0,z0) (e0,d1,z0)
+    const float2 b0 = make_float2(sm_f(q[1]), sm_f(q[BX + 1]));          // (e1,d0,z0) (e1,d1,z0)
+    const float2 a1 = make_float2(sm_f(q[BXY]), sm_f(q[BXY + BX]));      // z1
+    const float2 b1 = make_float2(sm_f(q[BXY + 1]), sm_f(q[BXY + BX + 1]));
+    const float2 te = make_float2(aed.x, aed.x);
+    const float2 e0 = lerp2(a0, b0, te);   // z0: (d0, d1)
+    const float2 e1 = lerp2(a1, b1, te);   // z1: (d0, d1)
+    const float2 dz = lerp2(make_float2(e0.x, e1.x), make_float2(e0.y, e1.y), make_float2(aed.y, aed.y));
+    return fmaf(az, dz.y - dz.x, dz.x);
+  }
+};
+
+// Samples of one ray inside one slab, two per iteration (independent chains
+// for the scheduler).  (ce, cd, cz) are frame texel coordinates; samples are
+// consumed while floor(cd) stays inside the slab, in ray order.
+template <class V, int BX, int SGN, bool CHECK>
+__device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
+                                             float cz0, float dce, float dcd, float dcz, float lo, float hi,
+                                             float orgf, unsigned maxidx, float& acc, int& bad) {
+  using SS = SlabSample<V, BX>;
+  const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
+  auto outside = [&](float fd) { return SGN > 0 ? (fd >= hi) : (fd < lo); };
+  while (kf + 1.f < Nf) {
+    const float2 pa = __ffma2_rn(make_float2(kf, kf), dc, c0);
+    const float2 pb = __ffma2_rn(make_float2(kf + 1.f, kf + 1.f), dc, c0);
+    const float fda = floorf(pa.y), fdb = floorf(pb.y);
+    if (outside(fda)) return;
+    const float cza = fmaf(kf, dcz, cz0), czb = fmaf(kf + 1.f, dcz, cz0);
+    const float va = SS::eval(s, pa, cza, floorf(pa.x), fda, floorf(cza), orgf, maxidx, bad, CHECK);
+    if (outside(fdb)) {
+      acc += va;
+      kf += 1.f;
+      return;
+    }
+    const float vb = SS::eval(s, pb, czb, floorf(pb.x), fdb, floorf(czb), orgf, maxidx, bad, CHECK);
+    acc += va;
+    acc += vb;
+    kf += 2.f;
+  }
+  if (kf < Nf) {
+    const float2 pa = __ffma2_rn(make_float2(kf, kf), dc, c0);
+    const float fda = floorf(pa.y);
+    if (outside(fda)) return;
+    const float cza = fmaf(kf, dcz, cz0);
+    acc += SS::eval(s, pa, cza, floorf(pa.x), fda, floorf(cza), orgf, maxidx, bad, CHECK);
+    kf += 1.f;
+  }
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
+                                                       const __grid_constant__ CUtensorMap map_t,
+                                                       const V* __restrict__ vol,
+                                                       const ViewParams* __restrict__ views, GridConst gc,
+                                                       int BZ, FwdOut o, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ SlabShared sh;
+  // TMA destinations are 128-byte aligned (128 extra bytes are requested).
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  constexpr int BXY = BX * kBoxY;
+  const ViewParams vp = views[blockIdx.z];
+  const int dom = vp.dom;
+  const CUtensorMap* map = dom ? &map_v : &map_t;
   const int tid = threadIdx.x;
   const int p = blockIdx.z;
   const int u0 = blockIdx.x * kTU, v0 = blockIdx.y * kTV;
@@ -180,9 +262,12 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
   const bool active = (u < gc.W) && (v < gc.H);
   const Ray r = make_ray(vp, gc, min(u, gc.W - 1), min(v, gc.H - 1));
   const bool hit = active && (r.a2 > r.a1);
-  const float c0d = DOM ? r.c0y : r.c0x, dcd = DOM ? r.dcy : r.dcx;
-  const int Nd = DOM ? gc.ny : gc.nx;
-  (void)Nd;
+  // Frame coordinates: e = cross axis, d = slab axis (y for dom = 1, x for dom = 0).
+  const float ce0 = dom ? r.c0x : r.c0y, dce = dom ? r.dcx : r.dcy;
+  const float cd0 = dom ? r.c0y : r.c0x, dcd = dom ? r.dcy : r.dcx;
+  const float ke = dom ? gc.kx : gc.ky, be = dom ? gc.bx : gc.by;
+  const float kd = dom ? gc.ky : gc.kx, bd = dom ? gc.by : gc.bx;
+  const float Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
 
   if (tid == 0) {
     sh.mlo = INT_MAX;
@@ -193,8 +278,8 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
   }
   __syncthreads();
   if (hit) {
-    const int f0 = int(floorf(c0d));
-    const int f1 = int(floorf(fmaf(float(gc.N - 1), dcd, c0d)));
+    const int f0 = int(floorf(cd0));
+    const int f1 = int(floorf(fmaf(float(gc.N - 1), dcd, cd0)));
     const int m0 = (max(f0, kSlabBase) - kSlabBase) / kTS;
     const int m1 = (max(f1, kSlabBase) - kSlabBase) / kTS;
     atomicMin(&sh.mlo, min(m0, m1));
@@ -225,21 +310,13 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
     const float dx = fmaf(float(uc), vp.Eux, vp.D0x);
     const float dy = fmaf(float(uc), vp.Euy, vp.D0y);
     const float dz = fmaf(float(vc), vp.Evz, vp.D0z);
-    float ce, cz;
-    if (DOM) {
-      const float wy = (plane - gc.by) / gc.ky;
-      const float t = (wy - vp.Sy) / dy;
-      ce = fmaf(vp.Sx + t * dx, gc.kx, gc.bx);
-      cz = fmaf(t * dz, gc.kz, gc.bz);
-    } else {
-      const float wx = (plane - gc.bx) / gc.kx;
-      const float t = (wx - vp.Sx) / dx;
-      ce = fmaf(vp.Sy + t * dy, gc.ky, gc.by);
-      cz = fmaf(t * dz, gc.kz, gc.bz);
-    }
+    const float de = dom ? dx : dy, dd = dom ? dy : dx;
+    const float t = ((plane - bd) / kd - Sd) / dd;
+    float ce = fmaf(fmaf(t, de, Se), ke, be);
+    float cz = fmaf(t * dz, gc.kz, gc.bz);
     // Clamp before the int conversion so that far-away planes stay finite.
-    ce = fminf(fmaxf(ce, -1.0e6f), 1.0e6f);
-    cz = fminf(fmaxf(cz, -1.0e6f), 1.0e6f);
+    ce = fminf(fmaxf(ce, -1.0e5f), 1.0e5f);
+    cz = fminf(fmaxf(cz, -1.0e5f), 1.0e5f);
     atomicMin(&sh.emin[i], int(floorf(ce)));
     atomicMax(&sh.emax[i], int(floorf(ce)));
     atomicMin(&sh.zmin[i], int(floorf(cz)));
@@ -247,35 +324,33 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
   }
   __syncthreads();
 
-  const int BX = box.bx, BY = box.by, BZ = box.bz, BXY = BX * BY;
-  const uint32_t box_bytes = uint32_t(BX * BY * BZ * sizeof(V));
+  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
   const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
-  // Box origin of slab i, in memory order (x, y, z).
-  auto origin = [&](int i, int& ox, int& oy, int& oz) {
-    const int m = (vp.dsgn > 0) ? mlo + i : mhi - i;
-    const int sm = kSlabBase + m * kTS;
+  const unsigned maxidx = unsigned(BXY * (BZ - 1) - BX - 2);
+  // Box origin of slab i (visiting order), frame/memory order (e, d, z).
+  auto origin = [&](int i, int& oe, int& od, int& oz, int& m) {
+    m = (vp.dsgn > 0) ? mlo + i : mhi - i;
     const int ii = m - mlo;
-    const int e0 = sh.emin[ii] - 1;
+    oe = (sh.emin[ii] - 1) & ~(int(16 / sizeof(V)) - 1);   // 16-byte aligned x start
+    od = kSlabBase + m * kTS;
     oz = sh.zmin[ii] - 1;
-    // x (innermost) coordinates of a TMA box start on a 16-byte boundary.
-    if (DOM) { ox = e0 & ~7; oy = sm; }
-    else { ox = sm & ~7; oy = e0; }
   };
   auto issue = [&](int i) {
-    int ox, oy, oz;
-    origin(i, ox, oy, oz);
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
     uint64_t* bar = &sh.bars[i % kNStage];
     mbar_arrive_expect_tx(bar, box_bytes);
-    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, ox, oy, oz, bar);
+    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, oe, od, oz, bar);
   };
   if (tid == 0) {
     for (int i = 0; i < min(kNStage, nslab); ++i) issue(i);
   }
 
   float acc = 0.f;
-  int k = 0;
+  float kf = 0.f;
+  const float Nf = float(gc.N);
   int bad = 0;
-  int done = 0;  // slabs whose barrier completed
+  int done = 0;
   for (int i = 0; i < nslab; ++i) {
     const int slot = i % kNStage;
     const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
@@ -284,31 +359,21 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
       break;
     }
     done = i + 1;
-    int ox, oy, oz;
-    origin(i, ox, oy, oz);
-    const int m = (vp.dsgn > 0) ? mlo + i : mhi - i;
-    const int ii = m - mlo;
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
     if (CHECK && tid == 0) {
-      // The footprint must fit the box: emax + 2 (footprint + margin) inside.
-      const int eext = DOM ? (sh.emax[ii] + 2 - ox) : (sh.emax[ii] + 2 - oy);
-      const int zext = sh.zmax[ii] + 2 - oz;
-      if (eext >= (DOM ? BX : BY) || zext >= BZ) atomicAdd(&flags[0], 1);
+      // The footprint (max + 1) plus a one-voxel margin must fit in the box.
+      const int ii = m - mlo;
+      if (sh.emax[ii] + 2 - oe >= BX || sh.zmax[ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
     }
     if (hit) {
       const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
-      const float lo = float(kSlabBase + m * kTS), hi = lo + float(kTS);
-      const float fox = float(ox), foy = float(oy), foz = float(oz);
-      while (k < gc.N) {
-        const float kf = float(k);
-        const float cd = fmaf(kf, dcd, c0d);
-        const float fd = floorf(cd);
-        if (vp.dsgn > 0 ? (fd >= hi) : (fd < lo)) break;
-        const float cx = DOM ? fmaf(kf, r.dcx, r.c0x) : cd;
-        const float cy = DOM ? cd : fmaf(kf, r.dcy, r.c0y);
-        const float cz = fmaf(kf, r.dcz, r.c0z);
-        acc += tri_box<V, CHECK>(s, BX, BXY, BX - 2, BY - 2, BZ - 2, cx - fox, cy - foy, cz - foz, bad);
-        ++k;
-      }
+      const float lo = float(od), hi = lo + float(kTS);
+      const float orgf = float(oe + od * BX + oz * BXY);
+      if (vp.dsgn > 0)
+        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+      else
+        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
     }
     __syncthreads();
     if (tid == 0 && i + kNStage < nslab) {
@@ -322,7 +387,7 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
       (void)mbar_wait_bounded(&sh.bars[i % kNStage], (i / kNStage) & 1, kWaitLimit);
   }
   if (CHECK) {
-    if (hit && k != gc.N) bad = 1;  // every sample of a hit ray must be consumed
+    if (hit && kf != Nf) bad = 1;  // every sample of a hit ray must be consumed
     if (bad) atomicAdd(&flags[0], 1);
   }
 
@@ -336,25 +401,6 @@ __device__ void slab_body(const CUtensorMap* map, const V* __restrict__ vol, con
   fwd_epilogue(o, gc, vp, p, u, v, active, val, sh.red, tid);
 }
 
-template <class V, bool CHECK>
-__global__ void __launch_bounds__(256) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_x,
-                                                       const __grid_constant__ CUtensorMap map_y,
-                                                       const V* __restrict__ vol,
-                                                       const ViewParams* __restrict__ views,
-                                                       GridConst gc, SlabBox box_x, SlabBox box_y,
-                                                       FwdOut o, int* flags) {
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ SlabShared sh;
-  // TMA destinations are 128-byte aligned (128 extra bytes are requested).
-  unsigned char* smem_raw =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
-  const ViewParams vp = views[blockIdx.z];
-  if (vp.dom)
-    slab_body<V, 1, CHECK>(&map_y, vol, vp, gc, box_y, o, flags, smem_raw, sh);
-  else
-    slab_body<V, 0, CHECK>(&map_x, vol, vp, gc, box_x, o, flags, smem_raw, sh);
-}
-
 // ------------------------------------------------------------------ host
 size_t dtype_size(cbct_dtype dt) { return dt == CBCT_F32 ? 4 : 2; }
 
@@ -366,87 +412,134 @@ CUtensorMapDataType tma_dtype(cbct_dtype dt) {
   }
 }
 
-CUtensorMap make_map(const cbct_plan* p, cbct_dtype dt, const void* vol, const SlabBox& b) {
+CUtensorMap make_map(cbct_dtype dt, const void* vol, int n0, int n1, int n2, const SlabBox& b) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
   const size_t es = dtype_size(dt);
-  cuuint64_t dims[3] = {(cuuint64_t)p->g.nx, (cuuint64_t)p->g.ny, (cuuint64_t)p->g.nz};
-  cuuint64_t strides[2] = {(cuuint64_t)p->g.nx * es, (cuuint64_t)p->g.nx * p->g.ny * es};
+  cuuint64_t dims[3] = {(cuuint64_t)n0, (cuuint64_t)n1, (cuuint64_t)n2};
+  cuuint64_t strides[2] = {(cuuint64_t)n0 * es, (cuuint64_t)n0 * n1 * es};
   cuuint32_t box[3] = {(cuuint32_t)b.bx, (cuuint32_t)b.by, (cuuint32_t)b.bz};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult res = tensor_map_encoder()(&m, tma_dtype(dt), 3, const_cast<void*>(vol), dims, strides, box,
-                                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult res = tensor_map_encoder()(&m, tma_dtype(dt), 3, const_cast<void*>(vol), dims, strides, box, estr,
+                                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (res != CUDA_SUCCESS)
     throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)res));
   return m;
 }
 
 template <class V>
-void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaStream_t st,
-                  cbct_dtype dt, bool use_slab) {
+const SlabBox& box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->slab : p->slab16; }
+
+template <class V, int BX>
+void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim3 grid, int first,
+                 cudaStream_t st, cbct_dtype dt) {
+  const SlabBox& b = box_for<V>(p);
+  const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
+  const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
+                                  volT ? p->g.nx : p->g.ny, p->g.nz, b);
+  const size_t smem = kNStage * ((b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127)) + 128;
+  if (p->debug_checks) {
+    auto k = fwd_slab_kernel<V, BX, true>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, 256, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+  } else {
+    auto k = fwd_slab_kernel<V, BX, false>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, 256, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+  }
+  check_launch("fwd_slab_kernel");
+}
+
+template <class V>
+void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaStream_t st, cbct_dtype dt,
+                  bool use_slab) {
   const V* vol = static_cast<const V*>(vol_v);
   const int first = p->first[s], cnt = p->count[s];
   dim3 grid((p->g.width + kTU - 1) / kTU, (p->g.height + kTV - 1) / kTV, cnt);
-  if (use_slab) {
-    const CUtensorMap mx = make_map(p, dt, vol, p->slab[0]);
-    const CUtensorMap my = make_map(p, dt, vol, p->slab[1]);
-    const size_t es = sizeof(V);
-    auto stage_bytes = [&](const SlabBox& b) { return ((b.bx * b.by * b.bz * es) + 127) & ~size_t(127); };
-    const size_t smem = kNStage * std::max(stage_bytes(p->slab[0]), stage_bytes(p->slab[1])) + 128;
-    if (p->debug_checks) {
-      auto k = fwd_slab_kernel<V, true>;
-      ensure_smem_attr((const void*)k, smem);
-      k<<<grid, 256, smem, st>>>(mx, my, vol, p->d_views + first, p->gc, p->slab[0], p->slab[1], o,
-                                 p->d_flags);
-    } else {
-      auto k = fwd_slab_kernel<V, false>;
-      ensure_smem_attr((const void*)k, smem);
-      k<<<grid, 256, smem, st>>>(mx, my, vol, p->d_views + first, p->gc, p->slab[0], p->slab[1], o,
-                                 p->d_flags);
-    }
-    check_launch("fwd_slab_kernel");
-  } else {
+  if (!use_slab) {
     fwd_gather_kernel<V><<<grid, 256, 0, st>>>(vol, p->d_views + first, p->gc, o);
     check_launch("fwd_gather_kernel");
+    return;
+  }
+  const V* volT = nullptr;
+  if (p->subset_has_xdom[s]) {
+    V* t = static_cast<V*>(p->d_volT);
+    dim3 tg((p->g.nx + 31) / 32, (p->g.ny + 31) / 32, p->g.nz);
+    transpose_xy_kernel<V><<<tg, dim3(32, 8), 0, st>>>(vol, t, p->g.nx, p->g.ny);
+    check_launch("transpose_xy_kernel");
+    volT = t;
+  }
+  switch (box_for<V>(p).bx) {
+    case 40: launch_slab<V, 40>(p, vol, volT, o, grid, first, st, dt); break;
+    case 56: launch_slab<V, 56>(p, vol, volT, o, grid, first, st, dt); break;
+    case 72: launch_slab<V, 72>(p, vol, volT, o, grid, first, st, dt); break;
+    case 104: launch_slab<V, 104>(p, vol, volT, o, grid, first, st, dt); break;
+    case 136: launch_slab<V, 136>(p, vol, volT, o, grid, first, st, dt); break;
+    default: throw Error(CBCT_ERR_INTERNAL, "unsupported slab box width");
+  }
+}
+
+template <class V, int BX>
+void prepare_width(size_t smem) {
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, false>, smem);
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, true>, smem);
+}
+
+template <class V>
+void prepare_typed(const cbct_plan* p) {
+  const SlabBox& b = box_for<V>(p);
+  const size_t smem = kNStage * ((b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127)) + 128;
+  switch (b.bx) {
+    case 40: prepare_width<V, 40>(smem); break;
+    case 56: prepare_width<V, 56>(smem); break;
+    case 72: prepare_width<V, 72>(smem); break;
+    case 104: prepare_width<V, 104>(smem); break;
+    case 136: prepare_width<V, 136>(smem); break;
+    default: break;
   }
 }
 
 }  // namespace
 
-// Chooses the slab variant and its TMA box sizes from the plan geometry: for
-// every view and tile, the footprint of every slab (corner-ray bounding box,
-// computed in FP64) sets the maximum box extent, plus a safety margin.
+// Chooses the slab variant and its TMA box from the plan geometry: for every
+// view and tile, the footprint of every slab (corner-ray bounding box in the
+// view's frame, computed in FP64) sets the largest box extent, plus margins.
 void forward_choose_variant(cbct_plan* p) {
   const cbct_geometry& g = p->g;
   p->fwd_variant = 0;
-  p->slab[0] = p->slab[1] = SlabBox{0, 0, 0, 0};
+  p->slab = SlabBox{0, 0, 0, 0};
+  p->subset_has_xdom.assign(p->n_subsets + 1, 0);
+  for (int s = 0; s <= p->n_subsets; ++s)
+    for (int i = p->first[s]; i < p->first[s] + p->count[s]; ++i)
+      if (p->hviews[i].dom == 0) p->subset_has_xdom[s] = 1;
   if (p->force_gather) return;
   const double kx = g.nx / (double)g.lx, ky = g.ny / (double)g.ly, kz = g.nz / (double)g.lz;
   const double bx = g.nx / 2.0 - 0.5, by = g.ny / 2.0 - 0.5, bz = g.nz / 2.0 - 0.5;
-  int ext_e[2] = {0, 0}, ext_z[2] = {0, 0};
+  int ext_e = 0, ext_z = 0;
   bool ok = true;
   const int tiles_u = (g.width + kTU - 1) / kTU, tiles_v = (g.height + kTV - 1) / kTV;
   for (int iv = 0; iv < p->n_views && ok; ++iv) {
     const ViewParams& vp = p->hviews[iv];
     const int dom = vp.dom;
     const int Nd = dom ? g.ny : g.nx;
+    const double ke = dom ? kx : ky, be = dom ? bx : by, kd = dom ? ky : kx, bd = dom ? by : bx;
+    const double Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
     const int nsl = (Nd + 1 - kSlabBase + kTS - 1) / kTS + 1;
     if (nsl > kMaxSlabs) { ok = false; break; }
-    // Direction sign must be uniform over the view (checked at all corners).
-    for (int tu = 0; tu < tiles_u; ++tu) {
+    for (int tu = 0; tu < tiles_u && ok; ++tu) {
       const int u0 = tu * kTU, ue = std::min(u0 + kTU, g.width) - 1;
       for (int tv = 0; tv < tiles_v; ++tv) {
         const int v0 = tv * kTV, ve = std::min(v0 + kTV, g.height) - 1;
-        double cd[4][3];
+        double cd[4][3];  // corner directions in frame order (e, d, z)
         for (int c = 0; c < 4; ++c) {
           const int uc = (c & 1) ? ue : u0, vc = (c & 2) ? ve : v0;
-          cd[c][0] = vp.D0x + uc * (double)vp.Eux;
-          cd[c][1] = vp.D0y + uc * (double)vp.Euy;
+          const double dx = vp.D0x + uc * (double)vp.Eux, dy = vp.D0y + uc * (double)vp.Euy;
+          cd[c][0] = dom ? dx : dy;
+          cd[c][1] = dom ? dy : dx;
           cd[c][2] = vp.D0z + vc * (double)vp.Evz;
-          const double dd = cd[c][dom], de = cd[c][1 - dom];
-          if (dd * vp.dsgn < 0.25 * std::fabs(de) || dd * vp.dsgn <= 0) ok = false;
+          // The slab axis must dominate every ray of the view with a uniform sign.
+          if (cd[c][1] * vp.dsgn <= 0 || cd[c][1] * vp.dsgn < 0.25 * std::fabs(cd[c][0])) ok = false;
         }
         if (!ok) break;
         for (int m = 0; m < nsl; ++m) {
@@ -454,58 +547,53 @@ void forward_choose_variant(cbct_plan* p) {
           for (int c = 0; c < 8; ++c) {
             const double plane = kSlabBase + m * kTS + ((c & 4) ? kTS : 0);
             const double* d = cd[c & 3];
-            double ce, cz;
-            if (dom) {
-              const double t = ((plane - by) / ky - vp.Sy) / d[1];
-              ce = (vp.Sx + t * d[0]) * kx + bx;
-              cz = t * d[2] * kz + bz;
-            } else {
-              const double t = ((plane - bx) / kx - vp.Sx) / d[0];
-              ce = (vp.Sy + t * d[1]) * ky + by;
-              cz = t * d[2] * kz + bz;
-            }
+            const double t = ((plane - bd) / kd - Sd) / d[1];
+            const double ce = (Se + t * d[0]) * ke + be;
+            const double cz = t * d[2] * kz + bz;
             emn = std::min(emn, ce); emx = std::max(emx, ce);
             zmn = std::min(zmn, cz); zmx = std::max(zmx, cz);
           }
           // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin
           const int ee = (int)(std::floor(emx) - std::floor(emn)) + 3 + 2;
           const int ez = (int)(std::floor(zmx) - std::floor(zmn)) + 3 + 2;
-          ext_e[dom] = std::max(ext_e[dom], ee);
-          ext_z[dom] = std::max(ext_z[dom], std::min(ez, g.nz + 4));
+          ext_e = std::max(ext_e, ee);
+          ext_z = std::max(ext_z, std::min(ez, g.nz + 4));
         }
       }
-      if (!ok) break;
     }
   }
   if (!ok) return;
-  // Box x starts are rounded down to a multiple of 8 elements (16 bytes for
-  // 16-bit storage, 32 for fp32), which widens the x extent by up to 7.
-  auto rup = [](int v, int a) { return (v + a - 1) / a * a; };
-  SlabBox bxd{rup(kTS + 1 + 7, 8), ext_e[0], ext_z[0], 1};   // x-dominant: x is the slab axis
-  SlabBox byd{rup(ext_e[1] + 7, 8), kTS + 1, ext_z[1], 1};
-  for (SlabBox* b : {&bxd, &byd}) {
-    if (b->by < 2) b->by = 2;
-    if (b->bz < 2) b->bz = 2;
-    if (b->bx > 256 || b->by > 256 || b->bz > 256) ok = false;
-  }
-  const size_t stage = std::max((size_t)bxd.bx * bxd.by * bxd.bz, (size_t)byd.bx * byd.by * byd.bz) * 4;
-  const size_t smem = kNStage * ((stage + 127) & ~size_t(127)) + 128;
-  if (!ok || smem > (size_t)kSmemBudget) return;
-  p->slab[0] = bxd;
-  p->slab[1] = byd;
-  p->slab_smem = smem;
+  // The x start of a box is rounded down to a 16-byte boundary (4 fp32 or 8
+  // 16-bit elements), which widens the box by up to 3 or 7 elements.
+  auto width = [&](int slack) {
+    for (int w : kBoxWidths)
+      if (w >= ext_e + slack) return w;
+    return 0;
+  };
+  const int w32 = width(3), w16 = width(7);
+  if (w32 == 0 || w16 == 0) return;
+  const int boxz = std::max(ext_z, 2);
+  if (boxz > 256) return;
+  SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+  auto smem_of = [](const SlabBox& b, size_t es) {
+    return kNStage * ((b.bx * b.by * b.bz * es + 127) & ~size_t(127)) + 128;
+  };
+  if (smem_of(b32, 4) > (size_t)kSmemBudget || smem_of(b16, 2) > (size_t)kSmemBudget) return;
+  p->slab = b32;
+  p->slab16 = b16;
+  p->slab_smem = smem_of(b32, 4);
   p->fwd_variant = 1;
 }
 
 void forward_prepare(cbct_plan* p) {
   if (p->fwd_variant != 1) return;
-  const size_t smem32 = p->slab_smem;
-  ensure_smem_attr((const void*)fwd_slab_kernel<float, false>, smem32);
-  ensure_smem_attr((const void*)fwd_slab_kernel<float, true>, smem32);
-  ensure_smem_attr((const void*)fwd_slab_kernel<__half, false>, smem32);
-  ensure_smem_attr((const void*)fwd_slab_kernel<__half, true>, smem32);
-  ensure_smem_attr((const void*)fwd_slab_kernel<__nv_bfloat16, false>, smem32);
-  ensure_smem_attr((const void*)fwd_slab_kernel<__nv_bfloat16, true>, smem32);
+  prepare_typed<float>(p);
+  prepare_typed<__half>(p);
+  prepare_typed<__nv_bfloat16>(p);
+  bool any_x = false;
+  for (int s = 0; s <= p->n_subsets; ++s) any_x = any_x || p->subset_has_xdom[s];
+  if (any_x && !p->d_volT)
+    CBCT_CUDA(cudaMalloc(&p->d_volT, (size_t)p->g.nx * p->g.ny * p->g.nz * sizeof(float)));
 }
 
 void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
@@ -534,8 +622,9 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
     o.partials = p->d_partials;
   }
   const size_t es = dtype_size(dt);
-  bool use_slab = p->fwd_variant == 1 && ((p->g.nx * es) % 16 == 0) &&
-                  (reinterpret_cast<uintptr_t>(vol) % 16 == 0);
+  const bool use_slab = p->fwd_variant == 1 && ((size_t)p->g.nx * es) % 16 == 0 &&
+                        ((size_t)p->g.ny * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
+                        (!p->subset_has_xdom[s] || p->d_volT != nullptr);
   switch (dt) {
     case CBCT_F32: launch_typed<float>(p, s, vol, o, st, dt, use_slab); break;
     case CBCT_F16: launch_typed<__half>(p, s, vol, o, st, dt, use_slab); break;

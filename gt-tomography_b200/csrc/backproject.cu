@@ -138,12 +138,14 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__
 }
 
 // ------------------------------------------------------------------ TMA-staged
-// A CTA owns a 32 x 4 x kZT voxel block.  For each view the block's footprint
+// A CTA owns a kTX x kTY x kZT voxel block; each warp holds an 8 x 4 patch of
+// columns so that its lanes read a narrow range of detector words.  For each view the block's footprint
 // on the detector (the bounding box of its eight projected corners, a convex
 // image of a convex block) is staged into shared memory by a 3-D TMA load
 // whose out-of-detector texels arrive as zeros, so the bilinear taps need no
 // bounds checks.  Views are pipelined over two stages.
 constexpr int kZT = 16;
+constexpr int kTX = 16, kTY = 8;     // columns per CTA of the TMA back-projector
 constexpr uint32_t kBpWaitLimit = 1u << 22;
 
 struct BpView {
@@ -151,7 +153,7 @@ struct BpView {
 };
 
 template <int EPI, bool FDK, int BU>
-__global__ void __launch_bounds__(kBX * kBY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
                                                            const ViewParams* __restrict__ views, int n_views,
                                                            GridConst gc, BpEpi e, int BV, int* flags) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -165,9 +167,9 @@ __global__ void __launch_bounds__(kBX * kBY) bp_tma_kernel(const __grid_constant
   BpView* tv = reinterpret_cast<BpView*>(base_ptr + 2 * stage_stride);
   int2* org = reinterpret_cast<int2*>(tv + n_views);     // per view: (u origin, v origin)
   int2* ext = org + n_views;                             // per view: (max u, max v) for checks
-  const int tid = threadIdx.y * kBX + threadIdx.x;
-  const int nthr = kBX * kBY;
-  const int i0 = blockIdx.x * kBX, j0 = blockIdx.y * kBY, k0 = blockIdx.z * kZT;
+  const int tid = threadIdx.x;
+  const int nthr = kTX * kTY;
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY, k0 = blockIdx.z * kZT;
 
   for (int q = tid; q < n_views; q += nthr) {
     const ViewParams& vp = views[q];
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kBX * kBY) bp_tma_kernel(const __grid_constant
   }
   __syncthreads();
   // Footprints: 8 corners of the block (voxel centres) per view.
-  const int ie = min(i0 + kBX, gc.nx) - 1, je = min(j0 + kBY, gc.ny) - 1, ke = min(k0 + kZT, gc.nz) - 1;
+  const int ie = min(i0 + kTX, gc.nx) - 1, je = min(j0 + kTY, gc.ny) - 1, ke = min(k0 + kZT, gc.nz) - 1;
   for (int q = tid; q < n_views * 8; q += nthr) {
     const int pv = q >> 3, c = q & 7;
     const BpView w = tv[pv];
@@ -220,7 +222,8 @@ __global__ void __launch_bounds__(kBX * kBY) bp_tma_kernel(const __grid_constant
     for (int pv = 0; pv < min(2, n_views); ++pv) issue(pv);
   }
 
-  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int i = i0 + (warp & 1) * 8 + (lane & 7), j = j0 + (warp >> 1) * 4 + (lane >> 3);
   const float x = fmaf(float(min(i, gc.nx - 1)) + 0.5f, gc.vx, -gc.hx);
   const float y = fmaf(float(min(j, gc.ny - 1)) + 0.5f, gc.vy, -gc.hy);
   const float z0 = fmaf(float(k0) + 0.5f, gc.vz, -gc.hz);
@@ -306,8 +309,8 @@ void launch_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const Bp
                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (res != CUDA_SUCCESS) throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled (projections) failed");
-  dim3 block(kBX, kBY);
-  dim3 grid((p->g.nx + kBX - 1) / kBX, (p->g.ny + kBY - 1) / kBY, (p->g.nz + kZT - 1) / kZT);
+  dim3 block(kTX * kTY);
+  dim3 grid((p->g.nx + kTX - 1) / kTX, (p->g.ny + kTY - 1) / kTY, (p->g.nz + kZT - 1) / kZT);
   const size_t smem = bp_tma_smem(p, cnt);
   auto k = bp_tma_kernel<EPI, FDK, BU>;
   ensure_smem_attr((const void*)k, smem);
@@ -360,7 +363,7 @@ void launch_bp(cbct_plan* p, int s, const float* proj, const BpEpi& e, cudaStrea
 }  // namespace
 
 // Chooses the TMA-staged back-projector and its detector box: the largest
-// footprint of any 32 x 4 x kZT block in any view (FP64, corner projections),
+// footprint of any kTX x kTY x kZT block in any view (FP64, corner projections),
 // plus margins.
 void backproject_choose_variant(cbct_plan* p) {
   const cbct_geometry& g = p->g;
@@ -372,15 +375,15 @@ void backproject_choose_variant(cbct_plan* p) {
   const double ku = g.width / double(g.fov_u), kv = g.height / double(g.fov_v);
   const double bu = g.width / 2.0 - 0.5, bv = g.height / 2.0 - 0.5;
   int eu = 0, ev = 0;
-  const int bxn = (g.nx + kBX - 1) / kBX, byn = (g.ny + kBY - 1) / kBY, bzn = (g.nz + kZT - 1) / kZT;
+  const int bxn = (g.nx + kTX - 1) / kTX, byn = (g.ny + kTY - 1) / kTY, bzn = (g.nz + kZT - 1) / kZT;
   for (int iv = 0; iv < p->n_views; ++iv) {
     const double th = double(p->angles[iv]) * (3.14159265358979323846 / 180.0);
     const double cs = std::cos(th), sn = std::sin(th);
     const double ox = p->offsets[2 * iv], oy = p->offsets[2 * iv + 1];
     for (int bi = 0; bi < bxn; ++bi)
       for (int bj = 0; bj < byn; ++bj) {
-        const int i0 = bi * kBX, ie = std::min(i0 + kBX, g.nx) - 1;
-        const int j0 = bj * kBY, je = std::min(j0 + kBY, g.ny) - 1;
+        const int i0 = bi * kTX, ie = std::min(i0 + kTX, g.nx) - 1;
+        const int j0 = bj * kTY, je = std::min(j0 + kTY, g.ny) - 1;
         double umn = 1e30, umx = -1e30, imn = 1e30, imx = -1e30;
         for (int c = 0; c < 4; ++c) {
           const double x = (((c & 1) ? ie : i0) + 0.5) * vx - g.lx / 2.0;

@@ -29,7 +29,8 @@ EXPORTED = [
     "cbct_offset_override", "cbct_plan_create", "cbct_plan_destroy", "cbct_plan_subset",
     "cbct_plan_forward_variant", "cbct_plan_set_option", "cbct_plan_read_flags", "cbct_forward",
     "cbct_backproject", "cbct_offset_correct", "cbct_fdk_filter", "cbct_fdk",
-    "cbct_forward_residual", "cbct_osmom_update", "cbct_reduce_f64", "cbct_osmom_solve",
+    "cbct_forward_residual", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
+    "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
 ]
 
@@ -88,6 +89,7 @@ _SIGS = {
     "cbct_forward_residual": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _vp, _f, _i32, _vp, _vp]),
     "cbct_osmom_update": (C.c_int, [_vp, _vp, _vp, _vp, _sz, _f, _f, _i32, _vp]),
     "cbct_reduce_f64": (C.c_int, [_i32, _vp, _vp, _sz, _vp, _vp]),
+    "cbct_reduce_f64_noalloc": (C.c_int, [_i32, _vp, _vp, _sz, _vp, _vp]),
     "cbct_osmom_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
     "cbct_ossart_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
     "cbct_phantom_voxelize": (C.c_int, [_gp, _vp, _i32, _i32, _vp, _vp]),

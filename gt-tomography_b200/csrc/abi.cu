@@ -485,6 +485,15 @@ cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t
   });
 }
 
+cbct_status cbct_reduce_f64_noalloc(int32_t kind, const float* a, const float* b, size_t n, double* out_dev,
+                                    void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(kind >= 0 && kind <= 2, "kind must be 0, 1 or 2");
+    CBCT_REQUIRE(a && out_dev && (kind != 0 || b), "NULL array");
+    reduce_noalloc_launch(kind, a, b, n, out_dev, S(stream));
+  });
+}
+
 static cbct_solver_params solver_defaults(const cbct_solver_params* p) {
   cbct_solver_params d{};
   d.iterations = 10;

@@ -171,6 +171,7 @@ void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const f
 void reduce_launch(int kind, const float* a, const float* b, size_t n, double* partials,
                    size_t n_partials, double* out, cudaStream_t st);
 void finalize_partials(const double* partials, int n, double* out, cudaStream_t st);
+void reduce_noalloc_launch(int kind, const float* a, const float* b, size_t n, double* out, cudaStream_t st);
 void osmom_update_launch(float* z, float* xold, const float* precon, const float* g, size_t n,
                          float step, float mom, int nonneg, cudaStream_t st);
 

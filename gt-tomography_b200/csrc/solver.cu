@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "device_common.cuh"
@@ -112,6 +114,47 @@ void reduce_launch(int kind, const float* a, const float* b, size_t n, double* p
 void finalize_partials(const double* partials, int n, double* out, cudaStream_t st) {
   finalize_kernel<<<1, kRedThreads, 0, st>>>(partials, n, out);
   check_launch("finalize_kernel");
+}
+
+// ------------------------------------------------------------------ allocation-free reduction
+// Scratch of cbct_reduce_f64_noalloc: the per-block partial sums of the
+// reduction live in this file-scope device array instead of device memory
+// obtained from cudaMalloc.  It holds kNoAllocMaxPartials doubles (8 KiB), and
+// every GPU that loads the library keeps it until the process exits.  All calls
+// share it: a call writes every partial it later reads, so contents left by an
+// earlier call never reach a result, but two calls that overlap on the GPU
+// (different streams, no ordering between them) race on it.
+constexpr int kNoAllocMaxPartials = 1024;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxPartials];
+
+// The array's name is only a host-side stand-in in host code; its device
+// address is looked up once per device, with that device current, by the first
+// call made on that device.
+static double* noalloc_partials_address() {
+  static std::mutex mu;
+  static std::vector<double*> by_device;
+  int dev = 0;
+  CBCT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)by_device.size() <= dev) by_device.resize(dev + 1, nullptr);
+  if (by_device[dev] == nullptr) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
+    if (e != cudaSuccess)
+      throw Error(CBCT_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_partials): ") + cudaGetErrorString(e));
+    by_device[dev] = static_cast<double*>(ptr);
+  }
+  return by_device[dev];
+}
+
+void reduce_noalloc_launch(int kind, const float* a, const float* b, size_t n, double* out, cudaStream_t st) {
+  // Same launch shape as reduce_launch: one partial per block.
+  const size_t needed = std::min<size_t>(kRedBlocks, std::max<size_t>((n + kRedThreads - 1) / kRedThreads, 1));
+  if (needed > (size_t)kNoAllocMaxPartials)
+    throw Error(CBCT_ERR_INVALID_ARGUMENT, "cbct_reduce_f64_noalloc: the reduction needs " + std::to_string(needed) +
+                                               " partial sums but its static scratch holds " +
+                                               std::to_string(kNoAllocMaxPartials));
+  reduce_launch(kind, a, b, n, noalloc_partials_address(), (size_t)kNoAllocMaxPartials, out, st);
 }
 
 void osmom_update_launch(float* z, float* xold, const float* precon, const float* g, size_t n, float step,

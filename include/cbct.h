@@ -222,6 +222,26 @@ CBCT_API cbct_status cbct_osmom_update(float* z, float* xold, const float* preco
 CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t n,
                             double* out_dev, void* stream);
 
+/* The same FP64 reduction for callers that cannot allocate device memory.
+ * No counterpart in the reference: it exists for code that must not call
+ * cudaMalloc while it runs, such as a caller that records its work into a CUDA
+ * graph (allocation is not allowed during stream capture) or a host whose
+ * device memory is owned by another allocator (a framework's caching
+ * allocator) that forbids side allocations.  cbct_reduce_f64 allocates its
+ * partial-sum buffer on its first call on each host thread; this entry point
+ * allocates nothing and calls no allocating routine.
+ * Scratch: the per-block partial sums live in a static device array of 1024
+ * doubles (8 KiB) that every GPU which loads the library holds until the
+ * process exits.  A call needs min(592, ceil(n/256)) of them; a call that
+ * would need more than 1024 is rejected with CBCT_ERR_INVALID_ARGUMENT.
+ * Set-up: the first call on each device looks up the array's device address
+ * (with that device current); make that first call before any stream capture.
+ * All calls share the array: each call writes every partial it reads, so an
+ * earlier call's leftovers never reach a result, but calls that overlap on the
+ * GPU (different streams with no ordering between them) race on it. */
+CBCT_API cbct_status cbct_reduce_f64_noalloc(int32_t kind, const float* a, const float* b, size_t n,
+                                             double* out_dev, void* stream);
+
 /* ----------------------------------------------------------------------------
  * Solvers (device-resident loops)
  * ------------------------------------------------------------------------- */

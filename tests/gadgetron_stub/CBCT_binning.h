@@ -1,0 +1,2 @@
+#pragma once
+#include "gadgetron_stub.h"

@@ -205,31 +205,41 @@ def flush_l2(buf):
     buf.fill_(1.0)
 
 
-def dist_setup(n_gpus: int):
+def dist_setup(backend: str = "nccl", timeout_s: float = 600.0):
+    """Rank, world size and local rank from the torchrun environment; joins the
+    process group when there is more than one rank (replicas: the group only
+    carries the barrier and the max-over-ranks reduction of the step time)."""
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and not torch.distributed.is_initialized():
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return rank, world, local
 
 
-def max_over_ranks(v: float, world: int):
+def max_over_ranks(v: float, world: int, device: str = "cuda") -> float:
     import torch
     if world == 1:
         return v
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(world):
+def whole_job_rate(units_per_rank: float, world: int, ms_max: float) -> float:
+    """Units processed by all ranks (replicas do equal work) per second of the
+    slowest rank, in billions."""
+    return units_per_rank * world / (ms_max * 1e-3) / 1e9
+
+
+def barrier(world, sync_cuda: bool = True):
     import torch
     if world > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
+    if sync_cuda:
+        torch.cuda.synchronize()
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -290,7 +300,7 @@ def reference_arm(args, wl: Workload):
 # ------------------------------------------------------------------ our arm
 def ours(args, wl: Workload):
     import torch
-    rank, world, local = dist_setup(args.gpus)
+    rank, world, local = dist_setup("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     gtb = _package()
@@ -335,7 +345,7 @@ def ours(args, wl: Workload):
     clk = clocks.stop()
     ms = max_over_ranks(sum(times) / len(times), world)
     fs, bv = wl.updates_per_step()
-    gups = (fs + bv) * world / (ms * 1e-3) / 1e9
+    gups = whole_job_rate(fs + bv, world, ms)
 
     # ---- end-to-end through the public API with host buffers
     b_host = b.cpu().pin_memory()
@@ -365,7 +375,7 @@ def ours(args, wl: Workload):
         e2e_times.append(e0.elapsed_time(e1))
     barrier(world)
     ms_e2e = max_over_ranks(sum(e2e_times) / len(e2e_times), world)
-    gups_e2e = (fs + bv) * world / (ms_e2e * 1e-3) / 1e9
+    gups_e2e = whole_job_rate(fs + bv, world, ms_e2e)
 
     # ---- dominant kernel: forward residual of one subset, timed alone
     s0 = 0

@@ -418,6 +418,38 @@ def ours(args, wl: Workload):
         "forward_variant": plan.forward_variant(),
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and wl.name == "c2" and not args.no_plain:
+        # The plain FP32 one-scan-at-a-time path (reference structure, texture
+        # filtering) on the same inputs: one warm-up and one timed reconstruction.
+        import ctypes as C
+        L = gtb._lib
+        g = wl.geometry(gtb)
+        aa = np.ascontiguousarray(a, np.float32)
+        oo = np.ascontiguousarray(o, np.float32)
+        sz = np.ascontiguousarray(sizes, np.int32)
+        ocv = np.ascontiguousarray(oc, np.int32)
+        zp = torch.empty_like(z)
+
+        def plain_step():
+            L.call("cbct_plain_osmom_solve", C.byref(g), aa.ctypes.data, oo.ctypes.data, aa.size, sz.ctypes.data,
+                   len(sz), ocv.ctypes.data, b.data_ptr(), zp.data_ptr(), wl.iters, 1, None)
+
+        plain_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plain_step()
+        e1.record(stream)
+        e1.synchronize()
+        ms_plain = e0.elapsed_time(e1)
+        plan.osmom(b, z, None, wl.iters, nonneg=True, use_graph=True, resid=resid)
+        torch.cuda.synchronize()
+        diff = float((z.double() - zp.double()).norm() / zp.double().norm())
+        line["plain_path"] = {"ms_per_step": round(ms_plain, 1), "value": round(whole_job_rate(fs + bv, 1, ms_plain), 3),
+                              "unit": "GUPS", "speedup_of_value": round(ms_plain / ms, 3),
+                              "rel_l2_ours_vs_plain": diff,
+                              "what": "reference structure re-hosted on B200: texture filtering, per-call "
+                                      "cudaArray copies and uploads, element-wise passes, host-synced norms"}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             O, g, vol, ang, off, k, threads, run = cpu_sample(wl, budget_s=8.0)
@@ -487,6 +519,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison leg")
     ap.add_argument("--only", choices=["forward", "backproject"], default=None,
                     help="time one kernel of the workload (profiling)")
     args = ap.parse_args()

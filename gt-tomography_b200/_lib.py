@@ -33,6 +33,8 @@ EXPORTED = [
     "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
 ]
+# The plain reference-replica path (include/cbct_plain.h), a measurement baseline.
+EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve"]
 
 
 class CbctGeometry(C.Structure):
@@ -95,6 +97,9 @@ _SIGS = {
     "cbct_phantom_voxelize": (C.c_int, [_gp, _vp, _i32, _i32, _vp, _vp]),
     "cbct_phantom_project": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp]),
     "cbct_convert": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp]),
+    "cbct_plain_forward": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32]),
+    "cbct_plain_backproject": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32, _i32]),
+    "cbct_plain_osmom_solve": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp]),
 }
 
 

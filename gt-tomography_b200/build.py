@@ -56,8 +56,12 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_mtime):
             jobs.append((s, o))
     if jobs:
+        # The plain reference-replica path is compiled with --use_fast_math, as the
+        # reference itself is (its CMakeLists.txt:52); the product kernels are not.
+        def flags(src):
+            return extra + (["--use_fast_math"] if os.path.basename(src).startswith("plain_") else [])
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
-            for msg in ex.map(lambda j: _compile(j[0], j[1], extra), jobs):
+            for msg in ex.map(lambda j: _compile(j[0], j[1], flags(j[0])), jobs):
                 if verbose and msg:
                     print(msg, file=sys.stderr)
     if force or jobs or not os.path.exists(LIB):

@@ -1,0 +1,386 @@
+// plain_replica.cu -- the plain FP32 one-scan-at-a-time GPU path (baseline).
+//
+// Built with --use_fast_math (see build.py), like the reference
+// (CMakeLists.txt:52).  The kernels restate xray/conebeam_projection.cu with
+// texture objects in place of the texture references CUDA 12 removed:
+//   forward  :412-528 (tex3D, normalised coords, linear filter, border 0)
+//   backward :922-1037 (tex2DLayered)
+//   offset   :233-262 (sin^2 weight)
+// and the host functions keep the reference's per-call structure: a cudaArray
+// of the whole volume / subset is allocated and filled on every call, angles
+// and offsets are uploaded on every call (thrust device_vector at :600-601,
+// :1225-1226), the grid is 1-D with 256 threads (setup_grid :48-75).  The
+// OS-MOM loop restates osMOMSolverD.h:82-196 with one pass per Gadgetron array
+// operation, a fresh device image per subset step (:153) and in denoise (:209),
+// and host-synchronised norms (:147-149, :206).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/cbct_plain.h"
+#include "cbct_internal.h"
+
+namespace cbct {
+namespace plain {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(CBCT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// setup_grid (conebeam_projection.cu:48-75): 256 threads, 1-D grid, 2-D when too long.
+void setup_grid(size_t n, dim3* block, dim3* grid) {
+  *block = dim3(256);
+  size_t gx = (n + 255) / 256;
+  unsigned gy = 1;
+  if (gx > 65535) {
+    gx = (unsigned)std::floor(std::sqrt(double(n) / 256.0));
+    const size_t per = 256 * gx;
+    gy = (unsigned)((n + per - 1) / per);
+  }
+  *grid = dim3((unsigned)gx, gy);
+}
+
+__device__ __forceinline__ size_t gidx() {
+  return (size_t)blockIdx.y * gridDim.x * blockDim.x + (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+}
+
+__global__ void fwd_kernel(float* __restrict__ projections, const float* __restrict__ angles,
+                           const float2* __restrict__ offsets, float3 L, int W, int H, float2 ps_mm, int P,
+                           float SDD, float SAD, int N, bool accumulate, cudaTextureObject_t tex) {
+  const size_t idx = gidx();
+  if (idx >= (size_t)W * H * P) return;
+  const int u = int(idx % W), v = int((idx / W) % H), p = int(idx / ((size_t)W * H));
+  float s, c;
+  sincosf(angles[p] * (CUDART_PI_F / 180.0f), &s, &c);
+  // start = R (0,-SAD,0); rows of R are (c,-s,0), (s,c,0), (0,0,1)
+  float3 sp = make_float3(s * SAD, -c * SAD, 0.f);
+  const float pcx = ((u + 0.5f) / float(W) - 0.5f) * ps_mm.x + offsets[p].x;
+  const float pcy = ((v + 0.5f) / float(H) - 0.5f) * ps_mm.y + offsets[p].y;
+  const float ADD = SDD - SAD;
+  const float3 ep = make_float3(c * pcx - s * ADD, s * pcx + c * ADD, pcy);
+  float3 dir = make_float3(ep.x - sp.x, ep.y - sp.y, ep.z - sp.z);
+  const float vx = (L.x / 2 - sp.x) / dir.x, vy = (L.y / 2 - sp.y) / dir.y, vz = (L.z / 2 - sp.z) / dir.z;
+  const float wx = (-L.x / 2 - sp.x) / dir.x, wy = (-L.y / 2 - sp.y) / dir.y, wz = (-L.z / 2 - sp.z) / dir.z;
+  const float a1 = fmaxf(fmaxf(fmaxf(fminf(wx, vx), fminf(wy, vy)), fminf(wz, vz)), 0.0f);
+  const float aend = fminf(fminf(fminf(fmaxf(wx, vx), fmaxf(wy, vy)), fmaxf(wz, vz)), 1.0f);
+  sp.x += a1 * dir.x; sp.y += a1 * dir.y; sp.z += a1 * dir.z;
+  const float dx = (aend - a1) * dir.x, dy = (aend - a1) * dir.y, dz = (aend - a1) * dir.z;
+  const float sampling_distance = sqrtf(dx * dx + dy * dy + dz * dz) / N;
+  sp.x = sp.x / L.x + 0.5f; sp.y = sp.y / L.y + 0.5f; sp.z = sp.z / L.z + 0.5f;
+  const float f = (aend - a1) / float(N);
+  dir.x = dir.x / L.x * f; dir.y = dir.y / L.y * f; dir.z = dir.z / L.z * f;
+  float result = 0.0f;
+  for (int k = 0; k < N; ++k)
+    result += tex3D<float>(tex, sp.x + dir.x * float(k), sp.y + dir.y * float(k), sp.z + dir.z * float(k));
+  projections[idx] = accumulate ? projections[idx] + result * sampling_distance : result * sampling_distance;
+}
+
+__global__ void bp_kernel(float* __restrict__ image, const float* __restrict__ angles,
+                          const float2* __restrict__ offsets, int nx, int ny, int nz, float3 L, float2 ps_mm, int P,
+                          float SDD, float SAD, bool accumulate, cudaTextureObject_t tex) {
+  const size_t idx = gidx();
+  if (idx >= (size_t)nx * ny * nz) return;
+  const int i = int(idx % nx), j = int((idx / nx) % ny), k = int(idx / ((size_t)nx * ny));
+  const float px = ((i + 0.5f) / nx - 0.5f) * L.x;
+  const float py = ((j + 0.5f) / ny - 0.5f) * L.y;
+  const float pz = ((k + 0.5f) / nz - 0.5f) * L.z;
+  const float incoming = accumulate ? image[idx] : 0.0f;
+  float result = 0.0f;
+  for (int p = 0; p < P; ++p) {
+    float s, c;
+    sincosf(-(angles[p] * (CUDART_PI_F / 180.0f)), &s, &c);
+    const float qx = c * px - s * py, qy = s * px + c * py;   // R(-angle) pos
+    float3 d = make_float3(qx, qy + SAD, pz);
+    d.x /= d.y; d.z /= d.y; d.y = 1.0f;
+    const float ex = SDD * d.x - offsets[p].x, ez = SDD * d.z - offsets[p].y;
+    const float uu = ex / ps_mm.x + 0.5f, vv = ez / ps_mm.y + 0.5f;
+    result += tex2DLayered<float>(tex, uu, vv, p);
+  }
+  image[idx] = incoming + result;
+}
+
+__global__ void offset_kernel(float* __restrict__ projections, const float2* __restrict__ offsets, int W, int H,
+                              int P, float2 ps_mm) {
+  const size_t idx = gidx();
+  if (idx >= (size_t)W * H * P) return;
+  const int u = int(idx % W), p = int(idx / ((size_t)W * H));
+  const float o = offsets[p].x;
+  const float t = (ps_mm.x * (float(u) / float(W) - 0.5f) + o) * o / fabsf(o);
+  const float omega = ps_mm.x / 2.0f - fabsf(o);
+  if (fabsf(t) <= omega) {
+    const float sw = sinf(CUDART_PI_F * (t + omega) / (4.0f * omega));
+    projections[idx] *= sw * sw;
+  }
+  if (t < -omega) projections[idx] *= 0;
+}
+
+// Gadgetron array operations, one pass each.
+__global__ void ew_sub(float* a, const float* b, size_t n) { size_t i = gidx(); if (i < n) a[i] -= b[i]; }
+__global__ void ew_mul(float* a, const float* b, size_t n) { size_t i = gidx(); if (i < n) a[i] *= b[i]; }
+__global__ void ew_scale(float* a, float s, size_t n) { size_t i = gidx(); if (i < n) a[i] *= s; }
+__global__ void ew_axpy(float a, const float* x, float* y, size_t n) { size_t i = gidx(); if (i < n) y[i] += a * x[i]; }
+__global__ void ew_fill(float* a, float v, size_t n) { size_t i = gidx(); if (i < n) a[i] = v; }
+__global__ void ew_clamp_min(float* a, float v, size_t n) { size_t i = gidx(); if (i < n) a[i] = fmaxf(a[i], v); }
+__global__ void ew_reciprocal(float* a, size_t n) { size_t i = gidx(); if (i < n) a[i] = 1.0f / a[i]; }
+__global__ void red_sq(const float* a, size_t n, double* out) {
+  __shared__ double sh[256];
+  double acc = 0;
+  for (size_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += (size_t)gridDim.x * 256) acc += double(a[i]) * a[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+__global__ void red_abs(const float* a, size_t n, double* out) {
+  __shared__ double sh[256];
+  double acc = 0;
+  for (size_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += (size_t)gridDim.x * 256) acc += fabs(double(a[i]));
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+template <class K, class... A>
+void launch_ew(K k, size_t n, A... a) {
+  dim3 b, g;
+  setup_grid(n, &b, &g);
+  k<<<g, b>>>(a...);
+  check(cudaGetLastError(), "plain element-wise kernel");
+}
+
+// Host-synchronised reduction (the value comes back to the host, as cuBLAS nrm2/asum do).
+double reduce_host(bool squares, const float* a, size_t n) {
+  const int blocks = 592;
+  double* d = nullptr;
+  check(cudaMalloc(&d, blocks * sizeof(double)), "cudaMalloc");
+  if (squares) red_sq<<<blocks, 256>>>(a, n, d);
+  else red_abs<<<blocks, 256>>>(a, n, d);
+  std::vector<double> h(blocks);
+  check(cudaMemcpy(h.data(), d, blocks * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+  cudaFree(d);
+  double s = 0;
+  for (double v : h) s += v;
+  return s;
+}
+
+struct Uploads {
+  float* angles = nullptr;
+  float2* offsets = nullptr;
+  Uploads(const float* a, const float* o, int n) {
+    check(cudaMalloc(&angles, sizeof(float) * n), "cudaMalloc");
+    check(cudaMalloc(&offsets, sizeof(float2) * n), "cudaMalloc");
+    check(cudaMemcpy(angles, a, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+    check(cudaMemcpy(offsets, o, sizeof(float2) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+  }
+  ~Uploads() {
+    cudaFree(angles);
+    cudaFree(offsets);
+  }
+};
+
+void forward(const cbct_geometry& g, const float* angles, const float* offsets, int P, const float* vol,
+             float* proj, bool accumulate) {
+  if (P == 0) return;
+  cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+  cudaExtent ext = make_cudaExtent(g.nx, g.ny, g.nz);
+  cudaArray_t arr = nullptr;
+  check(cudaMalloc3DArray(&arr, &ch, ext), "cudaMalloc3DArray");
+  cudaMemcpy3DParms cp = {};
+  cp.srcPtr = make_cudaPitchedPtr((void*)vol, g.nx * sizeof(float), g.nx, g.ny);
+  cp.dstArray = arr;
+  cp.extent = ext;
+  cp.kind = cudaMemcpyDeviceToDevice;
+  check(cudaMemcpy3D(&cp), "cudaMemcpy3D");
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = arr;
+  cudaTextureDesc td = {};
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 1;
+  cudaTextureObject_t tex = 0;
+  check(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+  {
+    Uploads up(angles, offsets, P);
+    dim3 b, gr;
+    setup_grid((size_t)g.width * g.height * P, &b, &gr);
+    const int N = (int)(g.samples_per_pixel * float(g.nx));
+    fwd_kernel<<<gr, b>>>(proj, up.angles, up.offsets, make_float3(g.lx, g.ly, g.lz), g.width, g.height,
+                          make_float2(g.fov_u, g.fov_v), P, g.SDD, g.SAD, N, accumulate, tex);
+    check(cudaGetLastError(), "plain fwd_kernel");
+    check(cudaDeviceSynchronize(), "plain fwd_kernel");
+  }
+  cudaDestroyTextureObject(tex);
+  cudaFreeArray(arr);
+}
+
+void backproject(const cbct_geometry& g, const float* angles, const float* offsets, int P, const float* proj,
+                 float* vol, bool offset_correction, bool accumulate) {
+  if (P == 0) return;
+  Uploads up(angles, offsets, P);
+  const size_t np = (size_t)g.width * g.height * P;
+  const float* src = proj;
+  float* copy = nullptr;
+  if (offset_correction) {
+    check(cudaMalloc(&copy, np * sizeof(float)), "cudaMalloc");
+    check(cudaMemcpy(copy, proj, np * sizeof(float), cudaMemcpyDeviceToDevice), "cudaMemcpy");
+    launch_ew(offset_kernel, np, copy, (const float2*)up.offsets, g.width, g.height, P,
+              make_float2(g.fov_u, g.fov_v));
+    src = copy;
+  }
+  cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+  cudaExtent ext = make_cudaExtent(g.width, g.height, P);
+  cudaArray_t arr = nullptr;
+  check(cudaMalloc3DArray(&arr, &ch, ext, cudaArrayLayered), "cudaMalloc3DArray(layered)");
+  cudaMemcpy3DParms cp = {};
+  cp.srcPtr = make_cudaPitchedPtr((void*)src, g.width * sizeof(float), g.width, g.height);
+  cp.dstArray = arr;
+  cp.extent = ext;
+  cp.kind = cudaMemcpyDeviceToDevice;
+  check(cudaMemcpy3D(&cp), "cudaMemcpy3D");
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = arr;
+  cudaTextureDesc td = {};
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 1;
+  cudaTextureObject_t tex = 0;
+  check(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+  dim3 b, gr;
+  setup_grid((size_t)g.nx * g.ny * g.nz, &b, &gr);
+  bp_kernel<<<gr, b>>>(vol, up.angles, up.offsets, g.nx, g.ny, g.nz, make_float3(g.lx, g.ly, g.lz),
+                       make_float2(g.fov_u, g.fov_v), P, g.SDD, g.SAD, accumulate, tex);
+  check(cudaGetLastError(), "plain bp_kernel");
+  check(cudaDeviceSynchronize(), "plain bp_kernel");
+  cudaDestroyTextureObject(tex);
+  cudaFreeArray(arr);
+  if (copy) cudaFree(copy);
+}
+
+void osmom(const cbct_geometry& g, const float* angles, const float* offsets, int P, const int* sizes, int S,
+           const int* offcorr, const float* b, float* z_out, int iters, bool nonneg, double* resid) {
+  const size_t nv = (size_t)g.nx * g.ny * g.nz, plane = (size_t)g.width * g.height, np = plane * P;
+  std::vector<int> first(S, 0);
+  for (int s = 1; s < S; ++s) first[s] = first[s - 1] + sizes[s - 1];
+  auto M = [&](int s, const float* x, float* out) {
+    forward(g, angles + first[s], offsets + 2 * first[s], sizes[s], x, out, false);
+  };
+  auto MH = [&](int s, const float* in, float* x, bool acc) {
+    backproject(g, angles + first[s], offsets + 2 * first[s], sizes[s], in, x, offcorr[s] != 0, acc);
+  };
+  float *z = nullptr, *x = nullptr, *xold = nullptr, *precon = nullptr, *tmp_proj = nullptr;
+  check(cudaMalloc(&z, nv * 4), "cudaMalloc");
+  check(cudaMalloc(&x, nv * 4), "cudaMalloc");
+  check(cudaMalloc(&xold, nv * 4), "cudaMalloc");
+  check(cudaMalloc(&precon, nv * 4), "cudaMalloc");
+  check(cudaMalloc(&tmp_proj, np * 4), "cudaMalloc");
+  check(cudaMemset(z, 0, nv * 4), "cudaMemset");                               // clear(z) (:100-104)
+  check(cudaMemcpy(x, z, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");       // x = z
+  check(cudaMemcpy(xold, z, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");    // xold = z
+  // precon: fill(1), mult_M (all subsets), mult_MH (all subsets), clamp_min, reciprocal (:115-120)
+  launch_ew(ew_fill, nv, precon, 1.0f, nv);
+  for (int s = 0; s < S; ++s) M(s, precon, tmp_proj + plane * first[s]);
+  for (int s = 0; s < S; ++s) MH(s, tmp_proj + plane * first[s], precon, s > 0);
+  launch_ew(ew_clamp_min, nv, precon, 1e-6f, nv);
+  launch_ew(ew_reciprocal, nv, precon, nv);
+  float t = 1, told = 1;
+  int step = 0;
+  for (int it = 0; it < iters; ++it) {
+    for (int s = 0; s < S; ++s, ++step) {
+      t = 0.5f * (1 + std::sqrt(1 + 4 * t * t));
+      float* ts = tmp_proj + plane * first[s];
+      const size_t ns = plane * sizes[s];
+      M(s, x, ts);
+      launch_ew(ew_sub, ns, ts, b + plane * first[s], ns);                     // -= subsets[s]
+      const double n2 = reduce_host(true, ts, ns);                             // VERBOSE nrm2 (:147-149)
+      if (resid) resid[step] = n2;
+      float* tmp_image = nullptr;                                              // ARRAY_TYPE tmp_image (:153)
+      check(cudaMalloc(&tmp_image, nv * 4), "cudaMalloc");
+      MH(s, ts, tmp_image, false);
+      launch_ew(ew_mul, nv, tmp_image, (const float*)precon, nv);
+      launch_ew(ew_axpy, nv, -1.0f * S, (const float*)tmp_image, z, nv);
+      cudaFree(tmp_image);
+      // denoise (:205-213): asum(precon) on the host path, a fresh g, then x = z
+      (void)reduce_host(false, precon, nv);
+      float* gbuf = nullptr;
+      check(cudaMalloc(&gbuf, nv * 4), "cudaMalloc");
+      cudaFree(gbuf);
+      check(cudaMemcpy(x, z, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");
+      if (nonneg) launch_ew(ew_clamp_min, nv, x, 0.0f, nv);
+      check(cudaMemcpy(z, x, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");  // *z = *x
+      launch_ew(ew_scale, nv, z, 1 + (told - 1) / t, nv);
+      launch_ew(ew_axpy, nv, -(told - 1) / t, (const float*)xold, z, nv);
+      std::swap(x, xold);
+      check(cudaMemcpy(x, z, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");  // *x = *z
+      told = t;
+    }
+  }
+  check(cudaMemcpy(z_out, z, nv * 4, cudaMemcpyDeviceToDevice), "cudaMemcpy");
+  check(cudaDeviceSynchronize(), "plain osmom");
+  cudaFree(z);
+  cudaFree(x);
+  cudaFree(xold);
+  cudaFree(precon);
+  cudaFree(tmp_proj);
+}
+
+template <class F>
+cbct_status guard(F&& f) {
+  try {
+    f();
+    return CBCT_OK;
+  } catch (const Error& e) {
+    return e.status;
+  } catch (...) {
+    return CBCT_ERR_INTERNAL;
+  }
+}
+
+}  // namespace plain
+}  // namespace cbct
+
+using namespace cbct::plain;
+
+extern "C" {
+
+cbct_status cbct_plain_forward(const cbct_geometry* g, const float* angles, const float* offsets, int32_t n,
+                               const float* vol, float* proj, int32_t accumulate) {
+  return guard([&] {
+    if (!g || !angles || !offsets || !vol || !proj || n < 0) throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
+    forward(*g, angles, offsets, n, vol, proj, accumulate != 0);
+  });
+}
+
+cbct_status cbct_plain_backproject(const cbct_geometry* g, const float* angles, const float* offsets, int32_t n,
+                                   const float* proj, float* vol, int32_t offset_correction, int32_t accumulate) {
+  return guard([&] {
+    if (!g || !angles || !offsets || !vol || !proj || n < 0) throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
+    backproject(*g, angles, offsets, n, proj, vol, offset_correction != 0, accumulate != 0);
+  });
+}
+
+cbct_status cbct_plain_osmom_solve(const cbct_geometry* g, const float* angles, const float* offsets, int32_t n,
+                                   const int32_t* sizes, int32_t S, const int32_t* offcorr, const float* b,
+                                   float* z_out, int32_t iterations, int32_t nonneg, double* resid) {
+  return guard([&] {
+    if (!g || !angles || !offsets || !sizes || !offcorr || !b || !z_out || S < 1)
+      throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
+    osmom(*g, angles, offsets, n, sizes, S, offcorr, b, z_out, iterations, nonneg != 0, resid);
+  });
+}
+
+}  // extern "C"

@@ -14,8 +14,8 @@ from cases import make
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _declared():
-    txt = open(os.path.join(ROOT, "include", "cbct.h")).read()
+def _declared(header="cbct.h"):
+    txt = open(os.path.join(ROOT, "include", header)).read()
     return sorted(set(re.findall(r"CBCT_API\s+[\w\s\*]*?\b(cbct_\w+)\s*\(", txt)))
 
 
@@ -29,6 +29,8 @@ def test_header_symbols_exported(gtb):
     exported = set(re.findall(r" T (cbct_\w+)", out))
     assert set(names) <= exported
     assert set(gtb._lib.EXPORTED) == set(names)
+    plain = _declared("cbct_plain.h")
+    assert set(plain) == set(gtb._lib.EXPORTED_PLAIN) and set(plain) <= exported
 
 
 def test_status_strings(gtb):

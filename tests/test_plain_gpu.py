@@ -1,0 +1,116 @@
+"""The plain reference-replica GPU path (include/cbct_plain.h).
+
+It restates the reference's CUDA kernels with hardware texture filtering, so
+it stands in for "the reference's CUDA projector outputs": it must agree with
+the oracle's texture-emulating mode closely and with the exact FP64 oracle to
+within the texture unit's 9-bit interpolation weights.  The product's FP32
+path is compared against it on identical geometry and the difference is
+bounded by the same texture-weight error."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cases import make
+
+pytestmark = pytest.mark.gpu
+
+
+def _plain_forward(gtb, case, vol):
+    import torch
+    L = gtb._lib
+    g = case.cgeom(gtb)
+    v = torch.from_numpy(vol.astype(np.float32)).cuda()
+    out = torch.zeros((case.angles.size, case.H, case.W), dtype=torch.float32, device="cuda")
+    a = np.ascontiguousarray(case.angles, np.float32)
+    o = np.ascontiguousarray(case.offsets, np.float32)
+    L.call("cbct_plain_forward", C.byref(g), a.ctypes.data, o.ctypes.data, a.size, v.data_ptr(), out.data_ptr(), 0)
+    return out.cpu().numpy()
+
+
+def _plain_bp(gtb, case, proj, offcorr=0):
+    import torch
+    L = gtb._lib
+    g = case.cgeom(gtb)
+    p = torch.from_numpy(proj.astype(np.float32)).cuda()
+    out = torch.zeros((case.nz, case.ny, case.nx), dtype=torch.float32, device="cuda")
+    a = np.ascontiguousarray(case.angles, np.float32)
+    o = np.ascontiguousarray(case.offsets, np.float32)
+    L.call("cbct_plain_backproject", C.byref(g), a.ctypes.data, o.ctypes.data, a.size, p.data_ptr(), out.data_ptr(),
+           offcorr, 0)
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["cube", "aniso", "offset"])
+def test_plain_forward_vs_oracle_modes(gtb, O, cuda, name):
+    case = make(name)
+    ell = gtb.phantom.ellipsoids(3, (case.lx, case.ly, case.lz), n=6).astype(np.float64)
+    g = case.oracle_geom(O)
+    vol = O.phantom_voxelize(g, ell, ss=2)
+    plain = _plain_forward(gtb, case, vol)
+    tex = O.forward(g, vol, case.angles, case.offsets, mode=1)
+    exact = O.forward(g, vol, case.angles, case.offsets, mode=0)
+    e_tex, e_exact = O.rel_l2(plain, tex), O.rel_l2(plain, exact)
+    print(f"{name}: plain vs texture-emulating oracle {e_tex:.2e}, vs exact FP64 {e_exact:.2e}")
+    assert e_tex < 2e-3 and e_exact < 5e-3
+
+
+def test_plain_backproject_vs_oracle(gtb, O, cuda):
+    case = make("offset")
+    rng = np.random.default_rng(0)
+    p = rng.uniform(0, 1, (case.angles.size, case.H, case.W))
+    g = case.oracle_geom(O)
+    plain = _plain_bp(gtb, case, p, offcorr=1)
+    pw = O.offset_weight(g, p, case.offsets, 0)
+    tex = O.backproject(g, pw, case.angles, case.offsets, mode=1)
+    exact = O.backproject(g, pw, case.angles, case.offsets, mode=0)
+    e_tex, e_exact = O.rel_l2(plain, tex), O.rel_l2(plain, exact)
+    print(f"plain BP vs texture-emulating oracle {e_tex:.2e}, vs exact FP64 {e_exact:.2e}")
+    assert e_tex < 2e-3 and e_exact < 5e-3
+
+
+def test_product_path_vs_plain_path(gtb, O, cuda):
+    """The product's FP32 software interpolation against the reference-style
+    texture path on identical geometry: they differ by the texture unit's
+    weight quantisation, while the product tracks the FP64 oracle to ~1e-6."""
+    import torch
+    case = make("c1small")
+    ell = gtb.phantom.ellipsoids(5, (case.lx, case.ly, case.lz), n=8).astype(np.float64)
+    g = case.oracle_geom(O)
+    vol = O.phantom_voxelize(g, ell, ss=2)
+    plain = _plain_forward(gtb, case, vol)
+    plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets)
+    out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
+    plan.forward(torch.from_numpy(vol.astype(np.float32)).to(cuda), out)
+    ours = out.cpu().numpy()
+    exact = O.forward(g, vol, case.angles, case.offsets)
+    d_plain, d_ours = O.rel_l2(ours, plain), O.rel_l2(ours, exact)
+    print(f"product vs plain texture path {d_plain:.2e}; product vs FP64 {d_ours:.2e}; "
+          f"plain vs FP64 {O.rel_l2(plain, exact):.2e}")
+    assert d_ours < 1e-4 and d_plain < 5e-3
+
+
+def test_plain_osmom_vs_oracle(gtb, O, cuda):
+    import torch
+    case = make("cube")
+    g = case.oracle_geom(O)
+    ell = gtb.phantom.ellipsoids(13, (case.lx, case.ly, case.lz), n=5).astype(np.float64)
+    b = O.phantom_project(g, ell, case.angles, case.offsets)
+    S = 3
+    order, sizes = O.subset_partition(case.angles.size, S)
+    a, o, bp = case.angles[order], case.offsets[order], b[order]
+    zr, rr = O.osmom(g, bp, a, o, sizes, np.zeros(S, np.int32), iters=2, nonneg=True)
+    L = gtb._lib
+    cg = case.cgeom(gtb)
+    bt = torch.from_numpy(bp.astype(np.float32)).to(cuda)
+    z = torch.empty((case.nz, case.ny, case.nx), dtype=torch.float32, device=cuda)
+    resid = np.zeros(2 * S)
+    sz = np.ascontiguousarray(sizes, np.int32)
+    oc = np.zeros(S, np.int32)
+    aa, oo = np.ascontiguousarray(a, np.float32), np.ascontiguousarray(o, np.float32)
+    L.call("cbct_plain_osmom_solve", C.byref(cg), aa.ctypes.data, oo.ctypes.data, aa.size, sz.ctypes.data, S,
+           oc.ctypes.data, bt.data_ptr(), z.data_ptr(), 2, 1, resid.ctypes.data)
+    e = O.rel_l2(z.cpu().numpy(), zr)
+    print(f"plain OS-MOM vs FP64 oracle {e:.2e}")
+    assert e < 1e-2
+    assert np.allclose(resid, rr, rtol=2e-2)

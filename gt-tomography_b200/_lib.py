@@ -31,7 +31,7 @@ EXPORTED = [
     "cbct_backproject", "cbct_offset_correct", "cbct_fdk_filter", "cbct_fdk",
     "cbct_forward_residual", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
     "cbct_osmom_solve",
-    "cbct_ossart_solve", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
+    "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
 ]
 # The plain reference-replica path (include/cbct_plain.h), a measurement baseline.
 EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve"]
@@ -49,6 +49,11 @@ class CbctSolverParams(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("beta", C.c_float), ("gamma", C.c_float),
                 ("non_negativity", C.c_int32), ("use_graph", C.c_int32), ("storage", C.c_int32),
                 ("refine_every", C.c_int32)]
+
+
+class CbctBatchItem(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("b", C.c_void_p), ("x0", C.c_void_p), ("z_out", C.c_void_p),
+                ("params", CbctSolverParams), ("resid_norm2_out", C.c_void_p)]
 
 
 class CbctError(RuntimeError):
@@ -94,6 +99,7 @@ _SIGS = {
     "cbct_reduce_f64_noalloc": (C.c_int, [_i32, _vp, _vp, _sz, _vp, _vp]),
     "cbct_osmom_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
     "cbct_ossart_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
+    "cbct_batch_osmom": (C.c_int, [C.POINTER(CbctBatchItem), _i32, _i32]),
     "cbct_phantom_voxelize": (C.c_int, [_gp, _vp, _i32, _i32, _vp, _vp]),
     "cbct_phantom_project": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp]),
     "cbct_convert": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp]),

@@ -29,6 +29,7 @@ void fdk_run(cbct_plan* p, const float* proj, float* vol, const float* filter, u
              cudaStream_t st);
 void phantom_voxelize_launch(const GridConst& gc, const float* ell, int K, int ss, float* vol, cudaStream_t st);
 void phantom_project_launch(cbct_plan* p, int s, const float* ell, int K, float* proj, cudaStream_t st);
+void batch_osmom(const cbct_batch_item* items, int n, int n_streams);
 
 static thread_local std::string g_last_error;
 
@@ -524,6 +525,10 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
     CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
   });
+}
+
+cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams) {
+  return guard([&] { batch_osmom(items, n, n_streams); });
 }
 
 cbct_status cbct_phantom_voxelize(const cbct_geometry* g, const float* ell, int32_t n, int32_t ss, float* vol,

@@ -374,40 +374,49 @@ void backproject_choose_variant(cbct_plan* p) {
   const double vx = double(g.lx) / g.nx, vy = double(g.ly) / g.ny, vz = double(g.lz) / g.nz;
   const double ku = g.width / double(g.fov_u), kv = g.height / double(g.fov_v);
   const double bu = g.width / 2.0 - 0.5, bv = g.height / 2.0 - 0.5;
-  int eu = 0, ev = 0;
   const int bxn = (g.nx + kTX - 1) / kTX, byn = (g.ny + kTY - 1) / kTY, bzn = (g.nz + kZT - 1) / kZT;
-  for (int iv = 0; iv < p->n_views; ++iv) {
-    const double th = double(p->angles[iv]) * (3.14159265358979323846 / 180.0);
-    const double cs = std::cos(th), sn = std::sin(th);
-    const double ox = p->offsets[2 * iv], oy = p->offsets[2 * iv + 1];
-    for (int bi = 0; bi < bxn; ++bi)
-      for (int bj = 0; bj < byn; ++bj) {
-        const int i0 = bi * kTX, ie = std::min(i0 + kTX, g.nx) - 1;
-        const int j0 = bj * kTY, je = std::min(j0 + kTY, g.ny) - 1;
-        double umn = 1e30, umx = -1e30, imn = 1e30, imx = -1e30;
-        for (int c = 0; c < 4; ++c) {
-          const double x = (((c & 1) ? ie : i0) + 0.5) * vx - g.lx / 2.0;
-          const double y = (((c & 2) ? je : j0) + 0.5) * vy - g.ly / 2.0;
-          const double xr = cs * x + sn * y, yr = -sn * x + cs * y;
-          const double inv = 1.0 / (yr + g.SAD);
-          const double u = (g.SDD * xr * inv - ox) * ku + bu;
-          umn = std::min(umn, u); umx = std::max(umx, u);
-          imn = std::min(imn, inv); imx = std::max(imx, inv);
+  std::vector<std::pair<int, int>> acc(host_threads(), {0, 0});
+  parallel_for(p->n_views, [&](int lo, int hi, int tid) {
+    int& eu = acc[tid].first;
+    int& ev = acc[tid].second;
+    for (int iv = lo; iv < hi; ++iv) {
+      const double th = double(p->angles[iv]) * (3.14159265358979323846 / 180.0);
+      const double cs = std::cos(th), sn = std::sin(th);
+      const double ox = p->offsets[2 * iv], oy = p->offsets[2 * iv + 1];
+      for (int bi = 0; bi < bxn; ++bi)
+        for (int bj = 0; bj < byn; ++bj) {
+          const int i0 = bi * kTX, ie = std::min(i0 + kTX, g.nx) - 1;
+          const int j0 = bj * kTY, je = std::min(j0 + kTY, g.ny) - 1;
+          double umn = 1e30, umx = -1e30, imn = 1e30, imx = -1e30;
+          for (int c = 0; c < 4; ++c) {
+            const double x = (((c & 1) ? ie : i0) + 0.5) * vx - g.lx / 2.0;
+            const double y = (((c & 2) ? je : j0) + 0.5) * vy - g.ly / 2.0;
+            const double xr = cs * x + sn * y, yr = -sn * x + cs * y;
+            const double inv = 1.0 / (yr + g.SAD);
+            const double u = (g.SDD * xr * inv - ox) * ku + bu;
+            umn = std::min(umn, u); umx = std::max(umx, u);
+            imn = std::min(imn, inv); imx = std::max(imx, inv);
+          }
+          eu = std::max(eu, (int)(std::floor(umx) - std::floor(umn)) + 3 + 2);
+          // rows: z spans of every z block, at the nearest and farthest magnification
+          for (int bk = 0; bk < bzn; ++bk) {
+            const int k0 = bk * kZT, ke = std::min(k0 + kZT, g.nz) - 1;
+            const double z0 = (k0 + 0.5) * vz - g.lz / 2.0, z1 = (ke + 0.5) * vz - g.lz / 2.0;
+            double vmn = 1e30, vmx = -1e30;
+            for (double inv : {imn, imx})
+              for (double z : {z0, z1}) {
+                const double v = (g.SDD * z * inv - oy) * kv + bv;
+                vmn = std::min(vmn, v); vmx = std::max(vmx, v);
+              }
+            ev = std::max(ev, (int)(std::floor(vmx) - std::floor(vmn)) + 3 + 2);
+          }
         }
-        eu = std::max(eu, (int)(std::floor(umx) - std::floor(umn)) + 3 + 2);
-        // rows: z spans of every z block, at the nearest and farthest magnification
-        for (int bk = 0; bk < bzn; ++bk) {
-          const int k0 = bk * kZT, ke = std::min(k0 + kZT, g.nz) - 1;
-          const double z0 = (k0 + 0.5) * vz - g.lz / 2.0, z1 = (ke + 0.5) * vz - g.lz / 2.0;
-          double vmn = 1e30, vmx = -1e30;
-          for (double inv : {imn, imx})
-            for (double z : {z0, z1}) {
-              const double v = (g.SDD * z * inv - oy) * kv + bv;
-              vmn = std::min(vmn, v); vmx = std::max(vmx, v);
-            }
-          ev = std::max(ev, (int)(std::floor(vmx) - std::floor(vmn)) + 3 + 2);
-        }
-      }
+    }
+  });
+  int eu = 0, ev = 0;
+  for (auto& a : acc) {
+    eu = std::max(eu, a.first);
+    ev = std::max(ev, a.second);
   }
   int w = 0;
   for (int c : kBoxWidths)

@@ -3,9 +3,11 @@
 
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cbct.h"
@@ -33,6 +35,27 @@ struct Error : std::runtime_error {
   do {                                                                                  \
     if (!(cond)) throw ::cbct::Error(CBCT_ERR_INVALID_ARGUMENT, msg);                   \
   } while (0)
+
+// Host threads used for plan set-up loops.
+inline int host_threads() {
+  const unsigned hc = std::thread::hardware_concurrency();
+  return (int)std::min(32u, std::max(1u, hc));
+}
+
+// Runs f(begin, end, thread_index) over [0, n) split into contiguous chunks on
+// host_threads() threads (the calling thread takes the first chunk).
+template <class F>
+void parallel_for(int n, F&& f) {
+  const int T = std::max(1, std::min(host_threads(), n));
+  std::vector<std::thread> th;
+  const int chunk = (n + T - 1) / T;
+  for (int t = 1; t < T; ++t) {
+    const int lo = t * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi) th.emplace_back([&f, lo, hi, t] { f(lo, hi, t); });
+  }
+  f(0, std::min(n, chunk), 0);
+  for (auto& x : th) x.join();
+}
 
 inline void check_launch(const char* what) {
   cudaError_t e = cudaGetLastError();

@@ -516,51 +516,68 @@ void forward_choose_variant(cbct_plan* p) {
   if (p->force_gather) return;
   const double kx = g.nx / (double)g.lx, ky = g.ny / (double)g.ly, kz = g.nz / (double)g.lz;
   const double bx = g.nx / 2.0 - 0.5, by = g.ny / 2.0 - 0.5, bz = g.nz / 2.0 - 0.5;
-  int ext_e = 0, ext_z = 0;
-  bool ok = true;
   const int tiles_u = (g.width + kTU - 1) / kTU, tiles_v = (g.height + kTV - 1) / kTV;
-  for (int iv = 0; iv < p->n_views && ok; ++iv) {
-    const ViewParams& vp = p->hviews[iv];
-    const int dom = vp.dom;
-    const int Nd = dom ? g.ny : g.nx;
-    const double ke = dom ? kx : ky, be = dom ? bx : by, kd = dom ? ky : kx, bd = dom ? by : bx;
-    const double Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
-    const int nsl = (Nd + 1 - kSlabBase + kTS - 1) / kTS + 1;
-    if (nsl > kMaxSlabs) { ok = false; break; }
-    for (int tu = 0; tu < tiles_u && ok; ++tu) {
-      const int u0 = tu * kTU, ue = std::min(u0 + kTU, g.width) - 1;
+  // Per thread: largest e extent, largest z extent, and whether every view fits.
+  struct Acc { int e = 0, z = 0, ok = 1; };
+  std::vector<Acc> acc(host_threads());
+  // The in-plane coordinate of a ray does not depend on the detector row, so the
+  // e extent is a function of (view, tile column, slab); the z extent comes from
+  // the products t * dz at the extreme path parameters and rows of each tile.
+  parallel_for(p->n_views, [&](int lo, int hi, int tid) {
+    Acc& a = acc[tid];
+    std::vector<double> dz0(tiles_v), dz1(tiles_v);
+    for (int iv = lo; iv < hi && a.ok; ++iv) {
+      const ViewParams& vp = p->hviews[iv];
+      const int dom = vp.dom;
+      const int Nd = dom ? g.ny : g.nx;
+      const double ke = dom ? kx : ky, be = dom ? bx : by, kd = dom ? ky : kx, bd = dom ? by : bx;
+      const double Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
+      const int nsl = (Nd + 1 - kSlabBase + kTS - 1) / kTS + 1;
+      if (nsl > kMaxSlabs) { a.ok = 0; break; }
       for (int tv = 0; tv < tiles_v; ++tv) {
         const int v0 = tv * kTV, ve = std::min(v0 + kTV, g.height) - 1;
-        double cd[4][3];  // corner directions in frame order (e, d, z)
-        for (int c = 0; c < 4; ++c) {
-          const int uc = (c & 1) ? ue : u0, vc = (c & 2) ? ve : v0;
-          const double dx = vp.D0x + uc * (double)vp.Eux, dy = vp.D0y + uc * (double)vp.Euy;
-          cd[c][0] = dom ? dx : dy;
-          cd[c][1] = dom ? dy : dx;
-          cd[c][2] = vp.D0z + vc * (double)vp.Evz;
+        dz0[tv] = vp.D0z + v0 * (double)vp.Evz;
+        dz1[tv] = vp.D0z + ve * (double)vp.Evz;
+      }
+      for (int tu = 0; tu < tiles_u && a.ok; ++tu) {
+        const int uc[2] = {tu * kTU, std::min(tu * kTU + kTU, g.width) - 1};
+        double de[2], dd[2];
+        for (int c = 0; c < 2; ++c) {
+          const double dx = vp.D0x + uc[c] * (double)vp.Eux, dy = vp.D0y + uc[c] * (double)vp.Euy;
+          de[c] = dom ? dx : dy;
+          dd[c] = dom ? dy : dx;
           // The slab axis must dominate every ray of the view with a uniform sign.
-          if (cd[c][1] * vp.dsgn <= 0 || cd[c][1] * vp.dsgn < 0.25 * std::fabs(cd[c][0])) ok = false;
+          if (dd[c] * vp.dsgn <= 0 || dd[c] * vp.dsgn < 0.25 * std::fabs(de[c])) a.ok = 0;
         }
-        if (!ok) break;
+        if (!a.ok) break;
         for (int m = 0; m < nsl; ++m) {
-          double emn = 1e30, emx = -1e30, zmn = 1e30, zmx = -1e30;
-          for (int c = 0; c < 8; ++c) {
-            const double plane = kSlabBase + m * kTS + ((c & 4) ? kTS : 0);
-            const double* d = cd[c & 3];
-            const double t = ((plane - bd) / kd - Sd) / d[1];
-            const double ce = (Se + t * d[0]) * ke + be;
-            const double cz = t * d[2] * kz + bz;
+          double emn = 1e30, emx = -1e30, tmn = 1e30, tmx = -1e30;
+          for (int c = 0; c < 4; ++c) {
+            const double plane = kSlabBase + m * kTS + ((c & 2) ? kTS : 0);
+            const double t = ((plane - bd) / kd - Sd) / dd[c & 1];
+            const double ce = (Se + t * de[c & 1]) * ke + be;
             emn = std::min(emn, ce); emx = std::max(emx, ce);
-            zmn = std::min(zmn, cz); zmx = std::max(zmx, cz);
+            tmn = std::min(tmn, t); tmx = std::max(tmx, t);
           }
           // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin
-          const int ee = (int)(std::floor(emx) - std::floor(emn)) + 3 + 2;
-          const int ez = (int)(std::floor(zmx) - std::floor(zmn)) + 3 + 2;
-          ext_e = std::max(ext_e, ee);
-          ext_z = std::max(ext_z, std::min(ez, g.nz + 4));
+          a.e = std::max(a.e, (int)(std::floor(emx) - std::floor(emn)) + 3 + 2);
+          for (int tv = 0; tv < tiles_v; ++tv) {
+            const double z00 = tmn * dz0[tv], z01 = tmn * dz1[tv], z10 = tmx * dz0[tv], z11 = tmx * dz1[tv];
+            const double zmn = std::min(std::min(z00, z01), std::min(z10, z11)) * kz + bz;
+            const double zmx = std::max(std::max(z00, z01), std::max(z10, z11)) * kz + bz;
+            const int ez = (int)(std::floor(zmx) - std::floor(zmn)) + 3 + 2;
+            a.z = std::max(a.z, std::min(ez, g.nz + 4));
+          }
         }
       }
     }
+  });
+  int ext_e = 0, ext_z = 0;
+  bool ok = true;
+  for (const Acc& a : acc) {
+    ext_e = std::max(ext_e, a.e);
+    ext_z = std::max(ext_z, a.z);
+    ok = ok && a.ok;
   }
   if (!ok) return;
   // The x start of a box is rounded down to a 16-byte boundary (4 fp32 or 8

@@ -329,6 +329,22 @@ def osmom_update(z, xold, precon, g, step, mom, nonneg=False, stream=None):
            int(nonneg), _stream(stream))
 
 
+def batch_osmom(jobs, n_streams=8):
+    """Solves independent OS-MOM problems concurrently (cbct_batch_osmom).
+
+    jobs: sequence of dicts with keys plan, b, z (outputs) and optionally x0,
+    iterations, beta, gamma, nonneg, storage, refine_every, resid.  Each result
+    is bitwise identical to solving that job alone.  Synchronises the device."""
+    items = (L.CbctBatchItem * len(jobs))()
+    for i, j in enumerate(jobs):
+        prm = L.CbctSolverParams(int(j.get("iterations", 10)), float(j.get("beta", 1.0)), float(j.get("gamma", 0.0)),
+                                 int(j.get("nonneg", False)), 1, int(j.get("storage", L.CBCT_F32)),
+                                 int(j.get("refine_every", 0)))
+        items[i] = L.CbctBatchItem(j["plan"].handle.value, _ptr(j["b"]), _ptr(j.get("x0")), _ptr(j["z"]), prm,
+                                   _ptr(j.get("resid")))
+    L.call("cbct_batch_osmom", items, len(jobs), int(n_streams))
+
+
 def convert(src, dst, dtype, stream=None):
     L.call("cbct_convert", _ptr(src), _ptr(dst), src.numel(), dtype, _stream(stream))
     return dst

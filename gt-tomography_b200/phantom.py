@@ -44,3 +44,50 @@ def poisson_log(line_integrals, I0: float, seed: int):
     lam = I0 * torch.exp(-line_integrals.double())
     counts = torch.poisson(lam, generator=gen)
     return (-torch.log(torch.clamp(counts, min=1.0) / I0)).float()
+
+
+def uneven_scans(n: int = 64, seed0: int = 1000, vol_range=(96, 320), z_range=(64, 320), view_range=(90, 720),
+                 width_range=(256, 768), step: int = 8):
+    """Scan shapes of the batched workload: volume x/y uniform in vol_range, z in
+    z_range, views in view_range, detector width in width_range with a 4:3
+    aspect; 1 mm voxels; pixel pitch 1.2*1.5*max(nx,ny)/W mm so that the
+    detector covers the volume.  Sizes are multiples of `step` (8), as CT grids
+    and detectors usually are.  Scan i uses seed seed0 + i."""
+    out = []
+    for i in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed0 + i))
+        q = lambda lo, hi: int(rng.integers(lo // step, hi // step + 1)) * step
+        nx, ny, nz = q(*vol_range), q(*vol_range), q(*z_range)
+        P = int(rng.integers(view_range[0], view_range[1] + 1))
+        W = q(*width_range)
+        H = (3 * W) // 4
+        pitch = 1.2 * 1.5 * max(nx, ny) / W
+        out.append(dict(seed=seed0 + i, n=(nx, ny, nz), P=P, W=W, H=H, pitch=pitch))
+    return out
+
+
+def make_osmom_scan(spec: dict, subsets: int, I0: float, device, offset_mm: float = 0.0, SAD: float = 1000.0,
+                    SDD: float = 1500.0, n_ellipsoids: int = 10):
+    """Device-resident OS-MOM problem for one scan shape (from uneven_scans):
+    views over 360 degrees in subset order, a seeded ellipsoid phantom, its exact
+    line integrals with Poisson noise (I0 > 0) and the log transform.
+    Returns (plan, b, (angles, offsets, subset_sizes, offset_correction))."""
+    import torch
+    from . import _lib as L
+    from .operators import Plan, offset_override, subset_partition
+    nx, ny, nz = spec["n"]
+    P, W, H, pitch = spec["P"], spec["W"], spec["H"], spec["pitch"]
+    lengths = (float(nx), float(ny), float(nz))
+    g = L.CbctGeometry(SAD, SDD, W * pitch, H * pitch, W, H, nx, ny, nz, *lengths, 1.5)
+    ang = circular_orbit(P)
+    off = np.tile(np.array([[offset_mm, 0.0]], np.float32), (P, 1))
+    order, sizes = subset_partition(P, subsets)
+    a, o = ang[order] - ang.min(), off[order]
+    first = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(int)
+    oc = [int(offset_override(g, o[f:f + n])) if n else 0 for f, n in zip(first, sizes)]
+    plan = Plan(g, a, o, sizes, oc)
+    ell = torch.from_numpy(ellipsoids(spec["seed"], lengths, n=n_ellipsoids).reshape(-1)).to(device)
+    exact = torch.empty(plan.proj_shape(), dtype=torch.float32, device=device)
+    plan.phantom_project(ell, exact)
+    b = poisson_log(exact, I0, spec["seed"] + 1) if I0 else exact
+    return plan, b.contiguous(), (a, o, sizes, oc)

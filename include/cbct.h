@@ -273,6 +273,28 @@ CBCT_API cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const fl
                               const cbct_solver_params* params, double* cost_out, void* stream);
 
 /* ----------------------------------------------------------------------------
+ * Batched reconstruction of many independent scans
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+  cbct_plan* plan;              /* the scan's geometry and subsets */
+  const float* b;               /* measured projections (subset-contiguous), device */
+  const float* x0;              /* initial image or NULL */
+  float* z_out;                 /* result, device */
+  cbct_solver_params params;    /* use_graph is forced on */
+  double* resid_norm2_out;      /* NULL or device array of iterations*n_subsets doubles */
+} cbct_batch_item;
+
+/* Runs n independent osMOMSolverD reconstructions (cbct_osmom_solve semantics)
+ * concurrently on up to n_streams streams.  Items are ordered largest first and
+ * each goes to the least-loaded stream; each item replays its own plan's
+ * captured CUDA graph.  Items must not share plans or output buffers.  Every
+ * kernel of an item reads only that item's buffers, so each result is bitwise
+ * identical to the item solved alone.  Synchronises the device.
+ * No counterpart in the reference (its drivers reconstruct one scan per process). */
+CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams);
+
+/* ----------------------------------------------------------------------------
  * Synthetic phantoms (seeded ellipsoids; used by the benchmarks and tests)
  * Ellipsoid record (10 floats): cx cy cz ax ay az phi theta psi density,
  * rotation R = Rz(phi) Ry(theta) Rx(psi).

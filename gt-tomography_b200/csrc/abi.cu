@@ -29,7 +29,7 @@ void fdk_run(cbct_plan* p, const float* proj, float* vol, const float* filter, u
              cudaStream_t st);
 void phantom_voxelize_launch(const GridConst& gc, const float* ell, int K, int ss, float* vol, cudaStream_t st);
 void phantom_project_launch(cbct_plan* p, int s, const float* ell, int K, float* proj, cudaStream_t st);
-void batch_osmom(const cbct_batch_item* items, int n, int n_streams);
+void batch_osmom(const cbct_batch_item* items, int n, int n_streams, cudaStream_t caller);
 
 static thread_local std::string g_last_error;
 
@@ -452,6 +452,31 @@ cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float
   });
 }
 
+cbct_status cbct_spacecarver(cbct_plan* plan, int32_t s, const float* proj, float limit, uint8_t* mask,
+                             int32_t combine, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    CBCT_REQUIRE(proj && mask, "NULL array");
+    spacecarver_launch(plan, i, proj, limit, mask, combine, S(stream));
+  });
+}
+
+cbct_status cbct_apply_mask(float* vol, const uint8_t* mask, size_t n, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(vol && mask, "NULL array");
+    apply_mask_launch(vol, mask, n, S(stream));
+  });
+}
+
+cbct_status cbct_plan_set_mask(cbct_plan* plan, const uint8_t* mask) {
+  return guard([&] {
+    CBCT_REQUIRE(plan, "plan is NULL");
+    plan->d_mask = mask;
+    // A captured solver graph holds the old mask pointer; drop it.
+    graph_cache_free(plan);
+  });
+}
+
 cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol, const float* b,
                                   float* r, float scale, int32_t apply_offset, double* norm2_out, void* stream) {
   return guard([&] {
@@ -527,8 +552,8 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
   });
 }
 
-cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams) {
-  return guard([&] { batch_osmom(items, n, n_streams); });
+cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream) {
+  return guard([&] { batch_osmom(items, n, n_streams, S(stream)); });
 }
 
 cbct_status cbct_phantom_voxelize(const cbct_geometry* g, const float* ell, int32_t n, int32_t ss, float* vol,

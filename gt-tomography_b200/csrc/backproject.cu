@@ -35,6 +35,7 @@ constexpr int kMaxViewsSmem = 1024;
 enum { kStore = 0, kRecip = 1, kMom = 2, kSart = 3 };
 
 struct BpEpi {
+  const unsigned char* mask;  // voxel mask applied to the back-projection (nullable)
   float* vol;            // kStore / kRecip output, kSart: x (in/out), kMom: z (in/out)
   float* xold;           // kMom
   const float* aux;      // kMom: precon D; kSart: V_s
@@ -44,10 +45,18 @@ struct BpEpi {
   int accumulate;
 };
 
+// With a mask, the operator's output is multiplied by it (apply_mask after
+// mult_MH, cuConebeamProjectionOperator.cpp:113-114), so the masked value of an
+// accumulating call is mask * (incoming + sum).
 template <int EPI>
 __device__ __forceinline__ void bp_store(const BpEpi& e, size_t idx, float g) {
+  const float m = e.mask ? float(e.mask[idx]) : 1.f;
   if (EPI == kStore) {
-    e.vol[idx] = e.scale * ((e.accumulate ? e.vol[idx] : 0.f) + g);
+    e.vol[idx] = e.scale * (((e.accumulate ? e.vol[idx] : 0.f) + g) * m);
+    return;
+  }
+  g *= m;
+  if (EPI == kStore) {
   } else if (EPI == kRecip) {
     e.vol[idx] = 1.f / fmaxf(g, 1e-6f);
   } else if (EPI == kMom) {
@@ -452,6 +461,7 @@ void backproject_prepare(cbct_plan* p) {
 void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int fdk_weight,
                         int accumulate, float out_scale, cudaStream_t st) {
   BpEpi e{};
+  e.mask = fdk_weight ? nullptr : p->d_mask;
   e.vol = vol;
   e.scale = out_scale;
   e.accumulate = accumulate;
@@ -461,6 +471,7 @@ void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int 
 
 void backproject_recip_launch(cbct_plan* p, int s, const float* proj, float* out, cudaStream_t st) {
   BpEpi e{};
+  e.mask = p->d_mask;
   e.vol = out;
   launch_bp<kRecip, false>(p, s, proj, e, st);
 }
@@ -468,6 +479,7 @@ void backproject_recip_launch(cbct_plan* p, int s, const float* proj, float* out
 void backproject_mom_launch(cbct_plan* p, int s, const float* proj, float* z, float* xold,
                             const float* precon, float step, float mom, int nonneg, cudaStream_t st) {
   BpEpi e{};
+  e.mask = p->d_mask;
   e.vol = z;
   e.xold = xold;
   e.aux = precon;
@@ -480,6 +492,7 @@ void backproject_mom_launch(cbct_plan* p, int s, const float* proj, float* z, fl
 void backproject_sart_launch(cbct_plan* p, int s, const float* proj, float* x, const float* V,
                              float step, int nonneg, cudaStream_t st) {
   BpEpi e{};
+  e.mask = p->d_mask;
   e.vol = x;
   e.aux = V;
   e.scale = step;

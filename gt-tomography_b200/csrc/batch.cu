@@ -49,7 +49,7 @@ double work_of(const cbct_batch_item& it) {
 
 }  // namespace
 
-void batch_osmom(const cbct_batch_item* items, int n, int n_streams) {
+void batch_osmom(const cbct_batch_item* items, int n, int n_streams, cudaStream_t caller) {
   if (n <= 0) return;
   CBCT_REQUIRE(items != nullptr, "items is NULL");
   CBCT_REQUIRE(n_streams >= 1, "n_streams must be >= 1");
@@ -65,6 +65,12 @@ void batch_osmom(const cbct_batch_item* items, int n, int n_streams) {
   for (int i = 0; i < n; ++i) work[i] = work_of(items[i]);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
   std::vector<double> load(S, 0.0);
+  // The pool streams are non-blocking: order them after the caller's stream.
+  cudaEvent_t ready;
+  CBCT_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  CBCT_CUDA(cudaEventRecord(ready, caller));
+  for (int s = 0; s < S; ++s) CBCT_CUDA(cudaStreamWaitEvent(pool[s], ready, 0));
+  CBCT_CUDA(cudaEventDestroy(ready));
   // Plans record their graphs on first use (host-side capture); the replays
   // then run asynchronously on the pool's streams.
   for (int i : order) {

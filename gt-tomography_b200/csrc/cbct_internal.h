@@ -161,6 +161,7 @@ struct cbct_plan {
 
   int debug_checks = 0;
   int force_gather = 0;
+  const unsigned char* d_mask = nullptr;  // voxel mask applied after back-projection (caller-owned)
 };
 
 namespace cbct {
@@ -197,6 +198,11 @@ void finalize_partials(const double* partials, int n, double* out, cudaStream_t 
 void reduce_noalloc_launch(int kind, const float* a, const float* b, size_t n, double* out, cudaStream_t st);
 void osmom_update_launch(float* z, float* xold, const float* precon, const float* g, size_t n,
                          float step, float mom, int nonneg, cudaStream_t st);
+
+// mask.cu
+void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,
+                        cudaStream_t st);
+void apply_mask_launch(float* vol, const unsigned char* mask, size_t n, cudaStream_t st);
 
 // host helpers (abi.cu)
 void default_filter(int W, float* out);

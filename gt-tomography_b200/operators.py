@@ -286,6 +286,18 @@ class Plan:
                int(apply_offset), _ptr(norm2), _stream(stream))
         return r
 
+    def spacecarver(self, proj, limit, mask, s=-1, combine=False, stream=None):
+        """conebeam_spacecarver over subset s: uint8 mask, 1 = keep."""
+        _need_cuda_f32(proj, self.proj_shape(s), "projections")
+        L.call("cbct_spacecarver", self._h, s, _ptr(proj), float(limit), _ptr(mask), int(combine), _stream(stream))
+        return mask
+
+    def set_mask(self, mask):
+        """Mask applied to the output of every back-projection (None clears it).
+        The plan keeps a reference so the mask stays alive while it is used."""
+        self._mask = mask
+        L.call("cbct_plan_set_mask", self._h, _ptr(mask))
+
     def phantom_project(self, ell_dev, out, s=-1, stream=None):
         _need_cuda_f32(out, self.proj_shape(s), "projections")
         n = ell_dev.numel() // 10
@@ -329,12 +341,13 @@ def osmom_update(z, xold, precon, g, step, mom, nonneg=False, stream=None):
            int(nonneg), _stream(stream))
 
 
-def batch_osmom(jobs, n_streams=8):
+def batch_osmom(jobs, n_streams=8, stream=None):
     """Solves independent OS-MOM problems concurrently (cbct_batch_osmom).
 
     jobs: sequence of dicts with keys plan, b, z (outputs) and optionally x0,
     iterations, beta, gamma, nonneg, storage, refine_every, resid.  Each result
-    is bitwise identical to solving that job alone.  Synchronises the device."""
+    is bitwise identical to solving that job alone.  Starts after the work on
+    the current stream and returns when every job has finished."""
     items = (L.CbctBatchItem * len(jobs))()
     for i, j in enumerate(jobs):
         prm = L.CbctSolverParams(int(j.get("iterations", 10)), float(j.get("beta", 1.0)), float(j.get("gamma", 0.0)),
@@ -342,7 +355,13 @@ def batch_osmom(jobs, n_streams=8):
                                  int(j.get("refine_every", 0)))
         items[i] = L.CbctBatchItem(j["plan"].handle.value, _ptr(j["b"]), _ptr(j.get("x0")), _ptr(j["z"]), prm,
                                    _ptr(j.get("resid")))
-    L.call("cbct_batch_osmom", items, len(jobs), int(n_streams))
+    L.call("cbct_batch_osmom", items, len(jobs), int(n_streams), _stream(stream))
+
+
+def apply_mask(vol, mask, stream=None):
+    """apply_mask (conebeam_projection.cu:1651-1657): vol *= mask."""
+    L.call("cbct_apply_mask", _ptr(vol), _ptr(mask), vol.numel(), _stream(stream))
+    return vol
 
 
 def convert(src, dst, dtype, stream=None):
@@ -423,7 +442,23 @@ class cuConebeamProjectionOperator:
         return self.use_offset_correction
 
     def set_mask(self, mask):
-        raise NotImplementedError("voxel masks (apply_mask) are not implemented in this build")
+        """cuConebeamProjectionOperator::set_mask: mult_MH applies it (.cpp:113-114)."""
+        self.mask = mask
+        for pl in self.plans:
+            if pl is not None:
+                pl.set_mask(mask if mask is None or mask.dim() == 3 else None)
+
+    def calculate_mask(self, projections, limit: float):
+        """cuConebeamProjectionOperator::calculate_mask (.cpp:118-147): one space
+        carve per bin; returns a uint8 mask of the domain's shape."""
+        T = torch()
+        masks = []
+        for pl, p in zip(self.plans, self._views(projections, True, False)):
+            m = T.ones(pl.vol_shape, dtype=T.uint8, device=projections.device)
+            if pl is not None:
+                pl.spacecarver(p, limit, m)
+            masks.append(m)
+        return masks[0] if len(masks) == 1 else T.stack(masks)
 
     def _views(self, arr, per_bin, is_volume):
         out, off = [], 0
@@ -555,6 +590,19 @@ class CBSubsetOperator:
         tmp = T.empty(self.plan.proj_shape(subset), dtype=T.float32, device=x.device)
         self.mult_M(x, tmp, subset, False)
         return self.mult_MH(tmp, out, subset, accumulate)
+
+    def calculate_mask(self, projections, limit: float):
+        """CBSubsetOperator::calculate_mask (.cpp:179-190): the AND of every
+        subset's space-carved mask."""
+        T = torch()
+        mask = T.ones(self.plan.vol_shape, dtype=T.uint8, device=projections.device)
+        for s, p in enumerate(self.projection_subsets(projections)):
+            self.plan.spacecarver(p, limit, mask, s, combine=True)
+        return mask
+
+    def set_mask(self, mask):
+        """CBSubsetOperator::set_mask: every subset's mult_MH applies the mask."""
+        self.plan.set_mask(mask)
 
     def offset_correct(self, projections):
         """CBSubsetOperator::offset_correct (.cpp:44-50): sqrt weight on subsets with correction."""

@@ -198,6 +198,28 @@ CBCT_API cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, co
                      uint32_t flags, float* work, void* stream);
 
 /* ----------------------------------------------------------------------------
+ * Voxel masks
+ * Masks are uint8 arrays of nx*ny*nz voxels (1 = keep), the layout of the
+ * reference's cuNDArray<bool>.
+ * ------------------------------------------------------------------------- */
+
+/* Space carver over the views of subset s (s = -1: all views):
+ * conebeam_spacecarver (conebeam_projection.cu:1043-1167, kernel :822-921).
+ * combine = 0 writes the mask; combine = 1 ANDs it into `mask`, as
+ * CBSubsetOperator::calculate_mask combines its subsets (CBSubsetOperator.cpp:179-190). */
+CBCT_API cbct_status cbct_spacecarver(cbct_plan* plan, int32_t s, const float* proj, float limit, uint8_t* mask,
+                                      int32_t combine, void* stream);
+
+/* vol *= mask (apply_mask, conebeam_projection.cu:1651-1657). */
+CBCT_API cbct_status cbct_apply_mask(float* vol, const uint8_t* mask, size_t n, void* stream);
+
+/* Sets (or clears, with NULL) the mask the plan's back-projections apply to
+ * their output (cuConebeamProjectionOperator::set_mask and the apply_mask at
+ * .cpp:113-114).  The caller keeps the mask alive while the plan uses it.
+ * Applies to cbct_backproject without CBCT_BP_FDK_WEIGHT and to the solvers. */
+CBCT_API cbct_status cbct_plan_set_mask(cbct_plan* plan, const uint8_t* mask);
+
+/* ----------------------------------------------------------------------------
  * Solver building blocks
  * ------------------------------------------------------------------------- */
 
@@ -286,13 +308,15 @@ typedef struct {
 } cbct_batch_item;
 
 /* Runs n independent osMOMSolverD reconstructions (cbct_osmom_solve semantics)
- * concurrently on up to n_streams streams.  Items are ordered largest first and
- * each goes to the least-loaded stream; each item replays its own plan's
- * captured CUDA graph.  Items must not share plans or output buffers.  Every
- * kernel of an item reads only that item's buffers, so each result is bitwise
- * identical to the item solved alone.  Synchronises the device.
+ * concurrently on up to n_streams internal streams.  Items are ordered largest
+ * first and each goes to the least-loaded stream; each item replays its own
+ * plan's captured CUDA graph.  Items must not share plans or output buffers.
+ * Every kernel of an item reads only that item's buffers, so each result is
+ * bitwise identical to the item solved alone.  The work starts after all work
+ * already enqueued on `stream` and the call returns once every item has
+ * finished (later work on `stream` is ordered after it).
  * No counterpart in the reference (its drivers reconstruct one scan per process). */
-CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams);
+CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream);
 
 /* ----------------------------------------------------------------------------
  * Synthetic phantoms (seeded ellipsoids; used by the benchmarks and tests)

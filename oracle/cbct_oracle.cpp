@@ -494,6 +494,7 @@ struct SubsetOp {
   int S;
   double spp;
   int mode;
+  const unsigned char* mask = nullptr;  // apply_mask after mult_MH (cuConebeamProjectionOperator.cpp:113-114)
   size_t npx() const { return (size_t)g->W * g->H; }
   int first(int s) const { int f = 0; for (int i = 0; i < s; ++i) f += sizes[i]; return f; }
   void M(int s, const double* x, double* out) const {
@@ -509,6 +510,10 @@ struct SubsetOp {
     } else {
       backproject<double, double>(*g, angles + f, offs + 2 * f, sizes[s], 0, mode, in, x, acc);
     }
+    if (mask) {
+      const size_t nv = (size_t)g->nx * g->ny * g->nz;
+      for (size_t i = 0; i < nv; ++i) x[i] *= double(mask[i]);
+    }
   }
 };
 
@@ -516,11 +521,17 @@ struct SubsetOp {
 // b holds the projections in subset-contiguous order.  resid_norm2 (optional,
 // iters*S entries) receives ||A_s x - b_s||^2 for each subset step (the
 // VERBOSE print of :147-149).  Returns z, the momentum point (:195).
+static const unsigned char* g_solver_mask = nullptr;
+
+// Mask used by the next oracle_osmom / oracle_ossart call (NULL = none).
+void oracle_set_solver_mask(const unsigned char* mask) { g_solver_mask = mask; }
+
 int oracle_osmom(const Geom* g, const float* angles, const float* offs, const int* sizes,
                  const int* offcorr, int S, double spp, int iters, double beta, double gamma,
                  int nonneg, const double* x0, const double* b, double* z_out,
                  double* resid_norm2) {
   SubsetOp A{g, angles, offs, sizes, offcorr, S, spp, 0};
+  A.mask = g_solver_mask;
   const size_t nv = (size_t)g->nx * g->ny * g->nz;
   int P = 0;
   for (int s = 0; s < S; ++s) P += sizes[s];
@@ -568,6 +579,7 @@ int oracle_ossart(const Geom* g, const float* angles, const float* offs, const i
                   const int* offcorr, int S, double spp, int iters, double beta, double gamma,
                   int nonneg, const double* x0, const double* b, double* x_out, double* cost_out) {
   SubsetOp A{g, angles, offs, sizes, offcorr, S, spp, 0};
+  A.mask = g_solver_mask;
   const size_t nv = (size_t)g->nx * g->ny * g->nz;
   int P = 0;
   for (int s = 0; s < S; ++s) P += sizes[s];
@@ -701,6 +713,37 @@ void oracle_phantom_project(const double* ell, int K, const Geom* g, const float
         proj[((size_t)p * g->H + v) * g->W + u] = acc;
       }
     }
+}
+
+// Space carver, conebeam_spacecarver_kernel (conebeam_projection.cu:822-921):
+// the voxel centre (with z negated, :852) is projected into every view and the
+// projection is point-sampled (texel floor(u*W), border 0, projections_mask_tex
+// at :41-42); views where the sample is nonzero and below `limit` are counted,
+// and the mask is 1 where fewer than 3 views were counted.
+void oracle_spacecarver(const Geom* g, const float* angles, const float* offs, int P, const double* proj,
+                        double limit, unsigned char* mask) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < g->nz; ++k)
+    for (int j = 0; j < g->ny; ++j)
+      for (int i = 0; i < g->nx; ++i) {
+        const double x = ((i + 0.5) / g->nx - 0.5) * g->lx;
+        const double y = ((j + 0.5) / g->ny - 0.5) * g->ly;
+        const double z = -((k + 0.5) / g->nz - 0.5) * g->lz;
+        int count = 0;
+        for (int p = 0; p < P; ++p) {
+          const double th = double(angles[p]) * (kPi / 180.0);
+          const double c = std::cos(th), s = std::sin(th);
+          const double xr = c * x + s * y, yr = -s * x + c * y;
+          const double dy = yr + g->SAD;
+          const double ex = g->SDD * (xr / dy) - offs[2 * p], ez = g->SDD * (z / dy) - offs[2 * p + 1];
+          const double un = ex / g->fov_u + 0.5, vn = ez / g->fov_v + 0.5;
+          const long iu = (long)std::floor(un * g->W), iv = (long)std::floor(vn * g->H);
+          double t = 0.0;
+          if (iu >= 0 && iu < g->W && iv >= 0 && iv < g->H) t = proj[((size_t)p * g->H + iv) * g->W + iu];
+          if (t < limit && t != 0.0) ++count;
+        }
+        mask[((size_t)k * g->ny + j) * g->nx + i] = count < 3 ? 1 : 0;
+      }
 }
 
 int oracle_num_threads() { return omp_get_max_threads(); }

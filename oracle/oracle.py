@@ -86,6 +86,9 @@ def _declare(L):
     L.oracle_phantom_voxelize.argtypes = [_f64, C.c_int, _GP, C.c_int, _f64]
     L.oracle_phantom_project.argtypes = [_f64, C.c_int, _GP, _f32, _f32, C.c_int, _f64]
     L.oracle_set_num_threads.argtypes = [C.c_int]
+    L.oracle_set_solver_mask.argtypes = [C.c_void_p]
+    L.oracle_spacecarver.argtypes = [_GP, _f32, _f32, C.c_int, _f64, C.c_double,
+                                     _P(dtype=np.uint8, flags="C_CONTIGUOUS")]
 
 
 def _views(angles, offsets):
@@ -199,10 +202,16 @@ def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonne
 
 
 def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
-          x0=None, spp=1.5):
-    """osMOMSolverD::solve (no regulariser); returns (z, per-step ||r||^2)."""
-    return _solver(lib().oracle_osmom, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
-                   nonneg, x0, spp, iters * len(sizes))
+          x0=None, spp=1.5, mask=None):
+    """osMOMSolverD::solve (no regulariser); returns (z, per-step ||r||^2).
+    mask: optional uint8 voxel mask applied after every mult_MH."""
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    lib().oracle_set_solver_mask(None if m is None else m.ctypes.data)
+    try:
+        return _solver(lib().oracle_osmom, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
+                       nonneg, x0, spp, iters * len(sizes))
+    finally:
+        lib().oracle_set_solver_mask(None)
 
 
 def ossart(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
@@ -224,6 +233,16 @@ def phantom_project(g: Geometry, ell, angles, offsets):
     a, o = _views(angles, offsets)
     out = np.zeros((a.size, g.H, g.W), dtype=np.float64)
     lib().oracle_phantom_project(e.reshape(-1), e.shape[0], C.byref(g.c()), a, o, a.size, out)
+    return out
+
+
+def spacecarver(g: Geometry, proj, angles, offsets, limit: float):
+    """conebeam_spacecarver: uint8 mask (nz, ny, nx), 1 where fewer than 3 views
+    see a nonzero value below `limit`."""
+    a, o = _views(angles, offsets)
+    p = np.ascontiguousarray(proj, dtype=np.float64)
+    out = np.zeros((g.nz, g.ny, g.nx), dtype=np.uint8)
+    lib().oracle_spacecarver(C.byref(g.c()), a, o, a.size, p, float(limit), out)
     return out
 
 

@@ -18,7 +18,8 @@ The directory name contains a hyphen, so it is imported by path:
 from . import _lib  # noqa: F401
 from ._lib import CBCT_BF16, CBCT_F16, CBCT_F32, CbctError, lib  # noqa: F401
 from .operators import (  # noqa: F401
-    CBCT_acquisition, CBCT_binning, CBCT_geometry, CBSubsetOperator, Plan, batch_osmom, cuConebeamProjectionOperator,
+    CBCT_acquisition, CBCT_binning, CBCT_geometry, CBSubsetOperator, CBSubsetWeightOperator, Plan, batch_osmom,
+    cuConebeamProjectionOperator,
     default_frequency_filter, fdk_reconstruct_3d, hann_ramp_filter, hoCuConebeamProjectionOperator,
     osMOMSolverD, osSARTSolver, phantom_voxelize, reduce_f64, subset_partition)
 from . import phantom  # noqa: F401

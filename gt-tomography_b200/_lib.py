@@ -32,7 +32,7 @@ EXPORTED = [
     "cbct_forward_residual", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
     "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
-    "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask",
+    "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
 ]
 # The plain reference-replica path (include/cbct_plain.h), a measurement baseline.
 EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve"]
@@ -107,6 +107,7 @@ _SIGS = {
     "cbct_spacecarver": (C.c_int, [_vp, _i32, _vp, _f, _vp, _i32, _vp]),
     "cbct_apply_mask": (C.c_int, [_vp, _vp, _sz, _vp]),
     "cbct_plan_set_mask": (C.c_int, [_vp, _vp]),
+    "cbct_plan_set_projection_weights": (C.c_int, [_vp, _vp]),
     "cbct_plain_forward": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "cbct_plain_backproject": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32, _i32]),
     "cbct_plain_osmom_solve": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp]),

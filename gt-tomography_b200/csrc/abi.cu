@@ -400,29 +400,46 @@ cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, floa
     CBCT_REQUIRE(vol && proj, "NULL array");
     CBCT_REQUIRE((flags & ~(CBCT_BP_OFFSET_WEIGHT | CBCT_BP_FDK_WEIGHT)) == 0, "unknown flags");
     const size_t plane = (size_t)plan->g.width * plan->g.height;
-    // Which views get the weight: every view of the call with the explicit flag,
-    // else the subsets whose offset correction is on (all subsets when s = -1).
-    bool any = (flags & CBCT_BP_OFFSET_WEIGHT) != 0;
+    // Which views get the Wang weight: every view of the call with the explicit
+    // flag, else the subsets whose offset correction is on (all subsets, s = -1).
+    auto weighted = [&](int k) {
+      return (flags & CBCT_BP_OFFSET_WEIGHT) != 0 || (use_plan_offset && plan->offcorr[k] != 0);
+    };
+    bool any = plan->d_pweights != nullptr || (flags & CBCT_BP_OFFSET_WEIGHT) != 0;
     if (!any && use_plan_offset) {
-      if (i < plan->n_subsets) any = plan->offcorr[i] != 0;
-      else for (int k = 0; k < plan->n_subsets; ++k) any = any || plan->offcorr[k] != 0;
+      if (i < plan->n_subsets) any = weighted(i);
+      else for (int k = 0; k < plan->n_subsets; ++k) any = any || weighted(k);
     }
     const float* in = proj;
     if (any) {
-      // mult_MH copies the input and weights the copy (cuConebeamProjectionOperator.cpp:101-102).
+      // mult_MH works on a weighted copy of its input (CBSubsetWeightOperator.h:44-49,
+      // cuConebeamProjectionOperator.cpp:101-102); the input itself is not modified.
       float* w = proj_scratch(plan, plane * plan->count[i]);
-      if ((flags & CBCT_BP_OFFSET_WEIGHT) || i < plan->n_subsets) {
-        offset_weight_launch(plan, i, proj, w, 0, S(stream));
-      } else {
-        for (int k = 0; k < plan->n_subsets; ++k) {
-          const size_t o = plane * plan->first[k], n = plane * plan->count[k];
-          if (plan->offcorr[k]) offset_weight_launch(plan, k, proj + o, w + o, 0, S(stream));
-          else if (n) CBCT_CUDA(cudaMemcpyAsync(w + o, proj + o, n * sizeof(float), cudaMemcpyDeviceToDevice, S(stream)));
+      const int k0 = i < plan->n_subsets ? i : 0, k1 = i < plan->n_subsets ? i + 1 : plan->n_subsets;
+      for (int k = k0; k < k1; ++k) {
+        const size_t o = i < plan->n_subsets ? 0 : plane * plan->first[k];
+        const size_t n = plane * plan->count[k];
+        if (n == 0) continue;
+        const float* src = proj + o;
+        if (plan->d_pweights) {
+          mul_launch(w + o, src, plan->d_pweights + plane * plan->first[k], n, S(stream));
+          src = w + o;
         }
+        const bool off = i < plan->n_subsets ? weighted(i) : weighted(k);
+        if (off) offset_weight_launch(plan, k, src, w + o, 0, S(stream));
+        else if (src != w + o) CBCT_CUDA(cudaMemcpyAsync(w + o, src, n * sizeof(float), cudaMemcpyDeviceToDevice, S(stream)));
       }
       in = w;
     }
     backproject_launch(plan, i, in, vol, (flags & CBCT_BP_FDK_WEIGHT) ? 1 : 0, accumulate, 1.f, S(stream));
+  });
+}
+
+cbct_status cbct_plan_set_projection_weights(cbct_plan* plan, const float* weights) {
+  return guard([&] {
+    CBCT_REQUIRE(plan, "plan is NULL");
+    plan->d_pweights = weights;
+    graph_cache_free(plan);   // captured solver graphs hold the old pointer
   });
 }
 

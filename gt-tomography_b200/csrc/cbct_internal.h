@@ -162,6 +162,7 @@ struct cbct_plan {
   int debug_checks = 0;
   int force_gather = 0;
   const unsigned char* d_mask = nullptr;  // voxel mask applied after back-projection (caller-owned)
+  const float* d_pweights = nullptr;      // projection weights, all views in subset order (caller-owned)
 };
 
 namespace cbct {
@@ -203,6 +204,7 @@ void osmom_update_launch(float* z, float* xold, const float* precon, const float
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,
                         cudaStream_t st);
 void apply_mask_launch(float* vol, const unsigned char* mask, size_t n, cudaStream_t st);
+void mul_launch(float* out, const float* in, const float* w, size_t n, cudaStream_t st);
 
 // host helpers (abi.cu)
 void default_filter(int W, float* out);

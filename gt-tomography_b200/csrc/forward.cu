@@ -40,6 +40,7 @@ struct FwdOut {
   int apply_offset;      // residual mode: multiply by the sin^2 Wang weight
   int accumulate;        // store mode: out += result
   double* partials;      // residual mode: per-block sum of squares (nullable)
+  const float* wproj;    // projection weights of the subset (CBSubsetWeightOperator; nullable)
 };
 
 constexpr uint32_t kWaitLimit = 1u << 22;
@@ -89,6 +90,10 @@ __device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& g
   double sq = 0.0;
   if (active) {
     const size_t idx = ((size_t)p * gc.H + v) * gc.W + u;
+    // CBSubsetWeightOperator: mult_M multiplies the projection by w, and mult_MH
+    // of the residual weights its input by w again (CBSubsetWeightOperator.h:32-49).
+    const float wp = o.wproj ? o.wproj[idx] : 1.f;
+    val *= wp;
     if (o.mode == kModeStore) {
       o.out[idx] = o.accumulate ? o.out[idx] + val : val;
     } else if (o.mode == kModeRecip) {
@@ -96,7 +101,7 @@ __device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& g
     } else {
       const float d = o.b ? val - o.b[idx] : val;
       sq = double(d) * double(d);
-      float w = o.scale;
+      float w = o.scale * wp;
       if (o.pw) w *= o.pw[idx];
       if (o.apply_offset) w *= offset_weight_full(gc.fov_u, gc.W, u, vp.ox);
       o.out[idx] = d * w;
@@ -633,6 +638,7 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
   o.partials = nullptr;
   const int cnt = p->count[s];
   if (cnt == 0) return;
+  o.wproj = p->d_pweights ? p->d_pweights + (size_t)p->g.width * p->g.height * p->first[s] : nullptr;
   const size_t nblocks = (size_t)((p->g.width + kTU - 1) / kTU) * ((p->g.height + kTV - 1) / kTV) * cnt;
   if (norm2_out) {
     if (nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");

@@ -46,7 +46,19 @@ __global__ void apply_mask_kernel(float* __restrict__ vol, const unsigned char* 
     vol[i] = vol[i] * float(mask[i]);
 }
 
+__global__ void mul_kernel(float* out, const float* in, const float* __restrict__ w, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i] * w[i];
+}
+
 }  // namespace
+
+void mul_launch(float* out, const float* in, const float* w, size_t n, cudaStream_t st) {
+  if (n == 0) return;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  mul_kernel<<<blocks, 256, 0, st>>>(out, in, w, n);
+  check_launch("mul_kernel");
+}
 
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,
                         cudaStream_t st) {

@@ -253,6 +253,8 @@ static void run_ossart(cbct_plan* p, const float* b, const float* x0, float* x, 
   fill_launch(r, proj_elems(p), 1.f, st);
   for (int s = 0; s < S; ++s) {
     float* rs = r + plane_elems(p) * p->first[s];
+    if (p->d_pweights)  // mult_MH of CBSubsetWeightOperator weights its input
+      mul_launch(rs, rs, p->d_pweights + plane_elems(p) * p->first[s], plane_elems(p) * p->count[s], st);
     if (p->offcorr[s]) offset_weight_launch(p, s, rs, rs, 0, st);
     backproject_recip_launch(p, s, rs, V + nv * s, st);
   }

@@ -292,6 +292,14 @@ class Plan:
         L.call("cbct_spacecarver", self._h, s, _ptr(proj), float(limit), _ptr(mask), int(combine), _stream(stream))
         return mask
 
+    def set_projection_weights(self, weights):
+        """Projection weights of CBSubsetWeightOperator (device tensor of the
+        plan's projection shape, subset order; None clears)."""
+        if weights is not None:
+            _need_cuda_f32(weights, self.proj_shape(), "weights")
+        self._pweights = weights
+        L.call("cbct_plan_set_projection_weights", self._h, _ptr(weights))
+
     def set_mask(self, mask):
         """Mask applied to the output of every back-projection (None clears it).
         The plan keeps a reference so the mask stays alive while it is used."""
@@ -610,6 +618,28 @@ class CBSubsetOperator:
             if self.offcorr[s]:
                 self.plan.offset_correct(p, s, 1)
         return projections
+
+
+class CBSubsetWeightOperator(CBSubsetOperator):
+    """CBSubsetOperator with per-pixel projection weights
+    (xray/CBSubsetWeightOperator.h:11-63): setup multiplies the acquisition's
+    projections by the weights, mult_M returns w * (A x) and mult_MH
+    back-projects w * input."""
+
+    def setup(self, acq: CBCT_acquisition, binning: Optional[CBCT_binning] = None, is_dims_in_mm=None,
+              projection_weights=None, is_dims=None):
+        w = np.ascontiguousarray(projection_weights, np.float32)
+        if acq.projections is not None:
+            acq.set_projections(np.ascontiguousarray(acq.projections * w))
+        self._host_weights = w
+        super().setup(acq, binning, is_dims_in_mm, is_dims=None)
+        self.weights = torch().from_numpy(np.ascontiguousarray(w[self.permutation])).cuda()
+        if is_dims is not None:
+            self.set_domain_dimensions(is_dims)
+
+    def _make_plan(self):
+        super()._make_plan()
+        self.plan.set_projection_weights(self.weights)
 
 
 class hoCuConebeamProjectionOperator:

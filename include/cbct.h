@@ -219,6 +219,13 @@ CBCT_API cbct_status cbct_apply_mask(float* vol, const uint8_t* mask, size_t n, 
  * Applies to cbct_backproject without CBCT_BP_FDK_WEIGHT and to the solvers. */
 CBCT_API cbct_status cbct_plan_set_mask(cbct_plan* plan, const uint8_t* mask);
 
+/* Projection weights of CBSubsetWeightOperator (xray/CBSubsetWeightOperator.h:11-63):
+ * a device array of W*H*n_views floats in subset-contiguous order (NULL clears).
+ * With weights set, cbct_forward returns w * (A x), cbct_backproject back-projects
+ * w * input, and the fused residual and the solvers weight the same way.  The
+ * caller keeps the array alive while the plan uses it. */
+CBCT_API cbct_status cbct_plan_set_projection_weights(cbct_plan* plan, const float* weights);
+
 /* ----------------------------------------------------------------------------
  * Solver building blocks
  * ------------------------------------------------------------------------- */

@@ -495,14 +495,26 @@ struct SubsetOp {
   double spp;
   int mode;
   const unsigned char* mask = nullptr;  // apply_mask after mult_MH (cuConebeamProjectionOperator.cpp:113-114)
+  const double* weights = nullptr;      // CBSubsetWeightOperator projection weights (all views, subset order)
   size_t npx() const { return (size_t)g->W * g->H; }
   int first(int s) const { int f = 0; for (int i = 0; i < s; ++i) f += sizes[i]; return f; }
+  // CBSubsetWeightOperator::mult_M (CBSubsetWeightOperator.h:32-43): out = w * (A x).
   void M(int s, const double* x, double* out) const {
     int f = first(s);
     forward<double, double>(*g, angles + f, offs + 2 * f, sizes[s], spp, mode, x, out, 0);
+    if (weights)
+      for (size_t i = 0; i < npx() * sizes[s]; ++i) out[i] *= weights[npx() * f + i];
   }
-  void MH(int s, const double* in, double* x, int acc) const {
+  // CBSubsetWeightOperator::mult_MH (.h:44-49): the input times w goes into mult_MH.
+  void MH(int s, const double* in_raw, double* x, int acc) const {
     int f = first(s);
+    std::vector<double> wtmp;
+    const double* in = in_raw;
+    if (weights) {
+      wtmp.assign(in_raw, in_raw + npx() * sizes[s]);
+      for (size_t i = 0; i < wtmp.size(); ++i) wtmp[i] *= weights[npx() * f + i];
+      in = wtmp.data();
+    }
     if (offcorr[s]) {
       std::vector<double> tmp(in, in + npx() * sizes[s]);
       offset_weight<double>(*g, offs + 2 * f, sizes[s], 0, tmp.data());
@@ -522,9 +534,11 @@ struct SubsetOp {
 // iters*S entries) receives ||A_s x - b_s||^2 for each subset step (the
 // VERBOSE print of :147-149).  Returns z, the momentum point (:195).
 static const unsigned char* g_solver_mask = nullptr;
+static const double* g_solver_weights = nullptr;
 
-// Mask used by the next oracle_osmom / oracle_ossart call (NULL = none).
+// Mask and projection weights used by the next oracle_osmom / oracle_ossart call (NULL = none).
 void oracle_set_solver_mask(const unsigned char* mask) { g_solver_mask = mask; }
+void oracle_set_solver_weights(const double* w) { g_solver_weights = w; }
 
 int oracle_osmom(const Geom* g, const float* angles, const float* offs, const int* sizes,
                  const int* offcorr, int S, double spp, int iters, double beta, double gamma,
@@ -532,6 +546,7 @@ int oracle_osmom(const Geom* g, const float* angles, const float* offs, const in
                  double* resid_norm2) {
   SubsetOp A{g, angles, offs, sizes, offcorr, S, spp, 0};
   A.mask = g_solver_mask;
+  A.weights = g_solver_weights;
   const size_t nv = (size_t)g->nx * g->ny * g->nz;
   int P = 0;
   for (int s = 0; s < S; ++s) P += sizes[s];
@@ -580,6 +595,7 @@ int oracle_ossart(const Geom* g, const float* angles, const float* offs, const i
                   int nonneg, const double* x0, const double* b, double* x_out, double* cost_out) {
   SubsetOp A{g, angles, offs, sizes, offcorr, S, spp, 0};
   A.mask = g_solver_mask;
+  A.weights = g_solver_weights;
   const size_t nv = (size_t)g->nx * g->ny * g->nz;
   int P = 0;
   for (int s = 0; s < S; ++s) P += sizes[s];

@@ -87,6 +87,7 @@ def _declare(L):
     L.oracle_phantom_project.argtypes = [_f64, C.c_int, _GP, _f32, _f32, C.c_int, _f64]
     L.oracle_set_num_threads.argtypes = [C.c_int]
     L.oracle_set_solver_mask.argtypes = [C.c_void_p]
+    L.oracle_set_solver_weights.argtypes = [C.c_void_p]
     L.oracle_spacecarver.argtypes = [_GP, _f32, _f32, C.c_int, _f64, C.c_double,
                                      _P(dtype=np.uint8, flags="C_CONTIGUOUS")]
 
@@ -202,23 +203,32 @@ def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonne
 
 
 def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
-          x0=None, spp=1.5, mask=None):
+          x0=None, spp=1.5, mask=None, weights=None):
     """osMOMSolverD::solve (no regulariser); returns (z, per-step ||r||^2).
-    mask: optional uint8 voxel mask applied after every mult_MH."""
+    mask: optional uint8 voxel mask applied after every mult_MH; weights:
+    optional projection weights of CBSubsetWeightOperator (subset order)."""
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
     lib().oracle_set_solver_mask(None if m is None else m.ctypes.data)
+    lib().oracle_set_solver_weights(None if w is None else w.ctypes.data)
     try:
         return _solver(lib().oracle_osmom, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
                        nonneg, x0, spp, iters * len(sizes))
     finally:
         lib().oracle_set_solver_mask(None)
+        lib().oracle_set_solver_weights(None)
 
 
 def ossart(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
-           x0=None, spp=1.5):
+           x0=None, spp=1.5, weights=None):
     """osSARTSolver::solve; returns (x, per-iteration ||Ax-b||^2)."""
-    return _solver(lib().oracle_ossart, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
-                   nonneg, x0, spp, iters)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    lib().oracle_set_solver_weights(None if w is None else w.ctypes.data)
+    try:
+        return _solver(lib().oracle_ossart, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
+                       nonneg, x0, spp, iters)
+    finally:
+        lib().oracle_set_solver_weights(None)
 
 
 def phantom_voxelize(g: Geometry, ell, ss=4):

@@ -1,6 +1,6 @@
 """Benchmark of the cone-beam OS-MOM hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c4|c5]
 
 Workload (default, c2): OS-MOM reconstruction (osMOMSolverD semantics,
 positivity, no regulariser) of a 256^3 seeded ellipsoid phantom from 360
@@ -565,15 +565,176 @@ def batched(args):
     print(json.dumps(line), flush=True)
 
 
+def _scan_host(gtb, sp, dev, I0=1e5):
+    """One seeded scan of the batched shapes: geometry, acquisition-order
+    angles/offsets and noisy log projections (pinned float32 host tensor)."""
+    import torch
+    L = gtb._lib
+    nx, ny, nz = sp["n"]
+    P, W, H, pitch = sp["P"], sp["W"], sp["H"], sp["pitch"]
+    g = L.CbctGeometry(1000.0, 1500.0, W * pitch, H * pitch, W, H, nx, ny, nz, float(nx), float(ny), float(nz), 1.5)
+    ang = gtb.phantom.circular_orbit(P)
+    off = np.zeros((P, 2), np.float32)
+    plan = gtb.Plan(g, ang, off)
+    ell = torch.from_numpy(gtb.phantom.ellipsoids(sp["seed"], (nx, ny, nz)).reshape(-1)).to(dev)
+    exact = torch.empty(plan.proj_shape(), dtype=torch.float32, device=dev)
+    plan.phantom_project(ell, exact)
+    b = gtb.phantom.poisson_log(exact, I0, sp["seed"] + 1)
+    host = torch.empty(b.shape, dtype=torch.float32).pin_memory()
+    host.copy_(b)
+    plan.close()
+    return g, ang, off, host
+
+
+def served(args):
+    """Serving loop (the north star's fifth configuration): Poisson arrivals
+    at --rate requests/s of FDK (70 %, Hann-windowed ramp) and OS-MOM (30 %,
+    8 subsets x 10 iterations, positivity) reconstructions with the batched
+    configuration's scan shapes (seeds 2000+i), storage bfloat16 or float32
+    per request (seeded coin; bfloat16 OS-MOM refines in FP32 every 5
+    iterations), admitted against a --budget-gb HBM budget on --slots request
+    slots.  Inputs are made on the device beforehand and held in pinned host
+    memory; every request copies its projections in and its volume out.
+    Latency = completion - submission on the host clock (a request is
+    submitted at its arrival time).  The plain FP32 path then serves the same
+    requests one at a time (host arrays in and out); its latencies follow from
+    its measured service times and the same arrival times, first in first out."""
+    import ctypes as C
+    import torch
+    gtb = _package()
+    L = gtb._lib
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(args.seed))
+    n = args.requests
+    specs = gtb.phantom.uneven_scans(n, seed0=2000)
+    kinds = ["fdk" if u < 0.7 else "osmom" for u in rng.random(n)]
+    use_bf16 = rng.random(n) < 0.5
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    arrivals -= arrivals[0]
+
+    def make_request(i, proj, vol):
+        g, ang, off = inputs[i][:3]
+        if kinds[i] == "fdk":
+            return gtb.Server.fdk_request(g, ang, off, proj, vol, filt=gtb.hann_ramp_filter(g.width))
+        return gtb.Server.osmom_request(g, ang, off, proj, vol, 8, iterations=10, nonneg=True, use_graph=True,
+                                        refine_every=5 if proj.dtype == torch.bfloat16 else 0)
+
+    inputs, reqs, vols = [], [], []
+    for i, sp in enumerate(specs):
+        g, ang, off, p32 = _scan_host(gtb, sp, dev)
+        proj = p32.to(torch.bfloat16).pin_memory() if use_bf16[i] else p32
+        inputs.append((g, ang, off, proj))
+        vols.append(torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32).pin_memory())
+        reqs.append(make_request(i, proj, vols[i]))
+    h2d = sum(x[3].numel() * x[3].element_size() for x in inputs)
+    d2h = sum(v.numel() * 4 for v in vols)
+    torch.cuda.synchronize()
+    srv = gtb.Server(args.budget_gb * 1e9, args.slots)
+    # Warm-up (untimed): one request of each kind and storage loads every kernel.
+    for i in [kinds.index(k) for k in ("fdk", "osmom") if k in kinds]:
+        for dt in (torch.float32, torch.bfloat16):
+            p = inputs[i][3].to(dt).pin_memory()
+            srv.wait(srv.submit(make_request(i, p, torch.empty_like(vols[i]).pin_memory())))
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    tickets = []
+    for i in range(n):
+        delay = arrivals[i] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(srv.submit(reqs[i]))
+    recs = [srv.wait(t) for t in tickets]
+    clk = clocks.stop()
+    lat = np.array([r["t_done"] - r["t_submit"] for r in recs])
+    span = max(r["t_done"] for r in recs) - min(r["t_submit"] for r in recs)
+    peak_inflight = max(sum(1 for r in recs if r["t_admit"] <= q["t_admit"] < r["t_done"]) for q in recs)
+    # bfloat16 storage against float32 storage of the same requests
+    storage_effect = {}
+    for k in ("fdk", "osmom"):
+        i = next((j for j in range(n) if kinds[j] == k and use_bf16[j]), None)
+        if i is None:
+            continue
+        p32 = _scan_host(gtb, specs[i], dev)[3]
+        v32 = torch.empty_like(vols[i]).pin_memory()
+        srv.wait(srv.submit(make_request(i, p32, v32)))
+        storage_effect[k] = float((vols[i] - v32).double().norm() / v32.double().norm())
+    srv.close()
+    # The plain FP32 path, one request at a time, on the same requests.
+    service, plain_err = [], {}
+    n_plain = n if not args.no_plain else 0
+    for i in range(n_plain):
+        g, ang, off = inputs[i][:3]
+        p32 = _scan_host(gtb, specs[i], dev)[3]
+        out = torch.empty_like(vols[i]).pin_memory()
+        a = np.ascontiguousarray(ang - ang.min(), np.float32)
+        o = np.ascontiguousarray(off, np.float32)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        if kinds[i] == "fdk":
+            f = gtb.hann_ramp_filter(g.width).astype(np.float32)
+            oc = int(gtb.operators.offset_override(g, off))
+            L.call("cbct_plain_fdk", C.byref(g), a.ctypes.data, o.ctypes.data, a.size, p32.data_ptr(),
+                   out.data_ptr(), f.ctypes.data, oc, 20)
+        else:
+            order, sizes = gtb.subset_partition(a.size, 8)
+            ap, op = np.ascontiguousarray(a[order]), np.ascontiguousarray(o[order])
+            first = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+            oc = np.array([int(gtb.operators.offset_override(g, op[f:f + s])) if s else 0
+                           for f, s in zip(first, sizes)], np.int32)
+            b = p32[torch.from_numpy(order.astype(np.int64))].to(dev)
+            z = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device=dev)
+            L.call("cbct_plain_osmom_solve", C.byref(g), ap.ctypes.data, op.ctypes.data, a.size,
+                   sizes.astype(np.int32).ctypes.data, 8, oc.ctypes.data, b.data_ptr(), z.data_ptr(), 10, 1, None)
+            out.copy_(z)
+        torch.cuda.synchronize()
+        service.append(time.perf_counter() - t1)
+        if kinds[i] not in plain_err and not use_bf16[i]:
+            plain_err[kinds[i]] = float((vols[i] - out).double().norm() / out.double().norm())
+    line = {"metric": "served recon/s (Poisson arrivals, 70% FDK / 30% OS-MOM)", "value": round(n / span, 3),
+            "unit": "recon/s", "n_gpus": 1, "steps": 1, "warmup": 4, "ms_per_step": round(span * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/bf16 storage, f32 compute",
+            "data": "synthetic",
+            "config": {"workload": f"{n} requests at {args.rate}/s, sizes of the batched configuration (seeds 2000+i)",
+                       "fdk": int(sum(k == "fdk" for k in kinds)), "osmom": int(sum(k == "osmom" for k in kinds)),
+                       "bf16_requests": int(use_bf16.sum()), "slots": args.slots, "budget_gb": args.budget_gb,
+                       "osmom": "8 subsets x 10 iterations, positivity, CUDA graph; bf16 refines every 5",
+                       "fdk_filter": "Hann-windowed ramp", "latency": "host clock, completion - arrival"},
+            "latency_p50_s": round(float(np.percentile(lat, 50)), 3),
+            "latency_p99_s": round(float(np.percentile(lat, 99)), 3),
+            "peak_requests_in_flight": int(peak_inflight),
+            "e2e": {"value": round(n / span, 3), "unit": "recon/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "storage_bf16_vs_f32_rel_l2": {k: round(v, 6) for k, v in storage_effect.items()},
+            "clocks": clk}
+    if service:
+        done, plain_lat = 0.0, []
+        for arr, s in zip(arrivals, service):
+            done = max(arr, done) + s
+            plain_lat.append(done - arr)
+        line["plain_path"] = {"recon_per_s": round(n / (done - arrivals[0]), 3),
+                              "latency_p50_s": round(float(np.percentile(plain_lat, 50)), 3),
+                              "latency_p99_s": round(float(np.percentile(plain_lat, 99)), 3),
+                              "service_s_total": round(float(sum(service)), 2),
+                              "served_vs_plain_rel_l2": {k: round(v, 6) for k, v in plain_err.items()}}
+        line["speedup_vs_plain"] = round((n / span) / line["plain_path"]["recon_per_s"], 3)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c4"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c4", "c5"])
     ap.add_argument("--scans", type=int, default=64, help="c4: number of scans")
     ap.add_argument("--streams", type=int, default=8, help="c4: streams of the batch executor")
+    ap.add_argument("--requests", type=int, default=32, help="c5: requests in the arrival stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="c5: Poisson arrival rate, requests/s")
+    ap.add_argument("--slots", type=int, default=4, help="c5: request slots of the server")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="c5: HBM budget of the server")
+    ap.add_argument("--seed", type=int, default=5, help="c5: seed of kinds, storage and arrivals")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison leg")
     ap.add_argument("--only", choices=["forward", "backproject"], default=None,
@@ -581,6 +742,9 @@ def main():
     args = ap.parse_args()
     if args.config == "c4":
         batched(args)
+        return
+    if args.config == "c5":
+        served(args)
         return
     wl = Workload(args.config)
     if args.only:

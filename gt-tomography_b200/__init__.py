@@ -17,6 +17,8 @@ The directory name contains a hyphen, so it is imported by path:
 """
 from . import _lib  # noqa: F401
 from ._lib import CBCT_BF16, CBCT_F16, CBCT_F32, CbctError, lib  # noqa: F401
+from . import serving  # noqa: F401
+from .serving import Server  # noqa: F401
 from .operators import (  # noqa: F401
     CBCT_acquisition, CBCT_binning, CBCT_geometry, CBSubsetOperator, CBSubsetWeightOperator, Plan, batch_osmom,
     cuConebeamProjectionOperator,

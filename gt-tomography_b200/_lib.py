@@ -33,9 +33,12 @@ EXPORTED = [
     "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
     "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
+    "cbct_fdk_filter_ex", "cbct_fdk_ex",
+    "cbct_server_create", "cbct_server_request_bytes", "cbct_server_submit", "cbct_server_wait",
+    "cbct_server_now", "cbct_server_destroy",
 ]
 # The plain reference-replica path (include/cbct_plain.h), a measurement baseline.
-EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve"]
+EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve", "cbct_plain_fdk"]
 
 
 class CbctGeometry(C.Structure):
@@ -49,12 +52,33 @@ class CbctGeometry(C.Structure):
 class CbctSolverParams(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("beta", C.c_float), ("gamma", C.c_float),
                 ("non_negativity", C.c_int32), ("use_graph", C.c_int32), ("storage", C.c_int32),
-                ("refine_every", C.c_int32)]
+                ("refine_every", C.c_int32), ("proj_storage", C.c_int32)]
 
 
 class CbctBatchItem(C.Structure):
     _fields_ = [("plan", C.c_void_p), ("b", C.c_void_p), ("x0", C.c_void_p), ("z_out", C.c_void_p),
                 ("params", CbctSolverParams), ("resid_norm2_out", C.c_void_p)]
+
+
+CBCT_REQ_FDK, CBCT_REQ_OSMOM = 0, 1
+
+
+class CbctServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_inflight", C.c_int32), ("device", C.c_int32)]
+
+
+class CbctRequest(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("geometry", CbctGeometry), ("angles_deg", C.c_void_p),
+                ("offsets_xy", C.c_void_p), ("n_views", C.c_int32), ("n_subsets", C.c_int32),
+                ("storage", C.c_int32), ("proj_host", C.c_void_p), ("vol_host", C.c_void_p),
+                ("params", CbctSolverParams), ("filter", C.c_void_p), ("fdk_flags", C.c_uint32),
+                ("offset_correction", C.c_int32)]
+
+
+class CbctRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("slot", C.c_int32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("bytes_reserved", C.c_size_t), ("bytes_peak", C.c_size_t),
+                ("message", C.c_char * 256)]
 
 
 class CbctError(RuntimeError):
@@ -108,9 +132,18 @@ _SIGS = {
     "cbct_apply_mask": (C.c_int, [_vp, _vp, _sz, _vp]),
     "cbct_plan_set_mask": (C.c_int, [_vp, _vp]),
     "cbct_plan_set_projection_weights": (C.c_int, [_vp, _vp]),
+    "cbct_fdk_filter_ex": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _vp, _u32, _vp]),
+    "cbct_fdk_ex": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _u32, _vp, _vp]),
+    "cbct_server_create": (C.c_int, [C.POINTER(CbctServerConfig), C.POINTER(_vp)]),
+    "cbct_server_request_bytes": (C.c_int, [C.POINTER(CbctRequest), C.POINTER(_sz)]),
+    "cbct_server_submit": (C.c_int, [_vp, C.POINTER(CbctRequest), C.POINTER(C.c_uint64)]),
+    "cbct_server_wait": (C.c_int, [_vp, C.c_uint64, C.c_double, C.POINTER(CbctRequestInfo)]),
+    "cbct_server_now": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "cbct_server_destroy": (C.c_int, [_vp]),
     "cbct_plain_forward": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "cbct_plain_backproject": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32, _i32]),
     "cbct_plain_osmom_solve": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp]),
+    "cbct_plain_fdk": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _vp, _i32, _i32]),
 }
 
 

@@ -21,17 +21,20 @@ void graph_cache_free(cbct_plan* p);
 void fill_launch(float* x, size_t n, float v, cudaStream_t st);
 void convert_launch(const float* src, void* dst, size_t n, cbct_dtype dt, cudaStream_t st);
 void backproject_recip_launch(cbct_plan* p, int s, const float* proj, float* out, cudaStream_t st);
-void osmom_solve(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const cbct_solver_params& prm,
                  double* resid, cudaStream_t st);
 void ossart_solve(cbct_plan* p, const float* b, const float* x0, float* x, const cbct_solver_params& prm,
                   double* cost, cudaStream_t st);
-void fdk_run(cbct_plan* p, const float* proj, float* vol, const float* filter, uint32_t flags, float* work,
-             cudaStream_t st);
+void fdk_run(cbct_plan* p, const void* proj, float* vol, const float* filter, uint32_t flags, float* work,
+             cudaStream_t st, cbct_dtype proj_dtype);
 void phantom_voxelize_launch(const GridConst& gc, const float* ell, int K, int ss, float* vol, cudaStream_t st);
 void phantom_project_launch(cbct_plan* p, int s, const float* ell, int K, float* proj, cudaStream_t st);
 void batch_osmom(const cbct_batch_item* items, int n, int n_streams, cudaStream_t caller);
 
-static thread_local std::string g_last_error;
+std::string& last_error_slot() {
+  static thread_local std::string msg;
+  return msg;
+}
 
 void ensure_smem_attr(const void* func, size_t bytes) {
   static std::mutex mu;
@@ -44,6 +47,47 @@ void ensure_smem_attr(const void* func, size_t bytes) {
   if (cur >= bytes) return;
   CBCT_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   cur = bytes;
+}
+
+void* plan_alloc(cbct_plan* p, size_t bytes) {
+  if (bytes == 0) return nullptr;
+  void* ptr = nullptr;
+  if (p->pool) CBCT_CUDA(cudaMallocFromPoolAsync(&ptr, bytes, p->pool, p->pool_stream));
+  else CBCT_CUDA(cudaMalloc(&ptr, bytes));
+  p->allocs.emplace_back(ptr, bytes);
+  p->dev_bytes += bytes;
+  p->dev_bytes_peak = std::max(p->dev_bytes_peak, p->dev_bytes);
+  return ptr;
+}
+
+void plan_dealloc(cbct_plan* p, void* ptr) {
+  if (!ptr) return;
+  for (size_t i = 0; i < p->allocs.size(); ++i) {
+    if (p->allocs[i].first != ptr) continue;
+    p->dev_bytes -= p->allocs[i].second;
+    p->allocs.erase(p->allocs.begin() + i);
+    if (p->pool) cudaFreeAsync(ptr, p->pool_stream);
+    else cudaFree(ptr);
+    return;
+  }
+}
+
+void plan_upload(cbct_plan* p, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  if (p->pool) {
+    // Stream-ordered after the pool allocation; the host buffer may go away
+    // when this returns, so wait for the copy (plan set-up only).
+    CBCT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, p->pool_stream));
+    CBCT_CUDA(cudaStreamSynchronize(p->pool_stream));
+  } else {
+    CBCT_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  }
+}
+
+void plan_memset(cbct_plan* p, void* dst, int value, size_t bytes) {
+  if (bytes == 0) return;
+  if (p->pool) CBCT_CUDA(cudaMemsetAsync(dst, value, bytes, p->pool_stream));
+  else CBCT_CUDA(cudaMemset(dst, value, bytes));
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -96,7 +140,26 @@ void subset_partition(int n_views, const int* view_bin, int n_subsets, int* orde
   *n_out = n;
 }
 
-static void validate_geometry(const cbct_geometry* g) {
+// Short-scan test of cuConebeamProjectionOperator::setup (.cpp:166-174) and
+// hoCuConebeamProjectionOperator::setup (.h:57-66), in float as there: the
+// largest angle (angles start at 0) against pi + 3 delta.
+bool short_scan_rule(const cbct_geometry& g, const float* angles, int n) {
+  const float span = *std::max_element(angles, angles + n);
+  const float delta = std::atan(g.fov_u / (2.0f * g.SDD));
+  const float pi = 3.14159265358979f;
+  return !(span * pi / 180.0f > pi + 3.0f * delta);
+}
+
+// Offset-correction override (cuConebeamProjectionOperator.cpp:176-181,
+// hoCuConebeamProjectionOperator.h:72-76): |mean offset_x| > 0.1 fov_u.
+bool offset_override_rule(const cbct_geometry& g, const float* offsets, int n) {
+  float mx = 0.f;
+  for (int i = 0; i < n; ++i) mx += offsets[2 * i];
+  mx /= float(n);
+  return std::fabs(mx) > g.fov_u * 0.1f;
+}
+
+void validate_geometry(const cbct_geometry* g) {
   CBCT_REQUIRE(g != nullptr, "geometry is NULL");
   CBCT_REQUIRE(g->width > 0 && g->height > 0, "detector size must be positive");
   CBCT_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0, "volume size must be positive");
@@ -150,22 +213,17 @@ static ViewParams make_view(const cbct_geometry& g, double angle_deg, double ox,
   return v;
 }
 
-static void plan_free(cbct_plan* p) {
+void plan_free(cbct_plan* p) {
   if (!p) return;
   fdk_state_free(p);
   graph_cache_free(p);
-  cudaFree(p->d_views);
-  cudaFree(p->d_proj_scratch);
-  cudaFree(p->d_partials);
-  cudaFree(p->d_flags);
-  cudaFree(p->d_fdk_work);
-  cudaFree(p->d_volT);
-  cudaFree(p->ws);
+  while (!p->allocs.empty()) plan_dealloc(p, p->allocs.back().first);
   delete p;
 }
 
-static cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float* offsets, int n_views,
-                              const int* subset_sizes, int n_subsets, const int* offcorr) {
+cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float* offsets, int n_views,
+                       const int* subset_sizes, int n_subsets, const int* offcorr, cudaMemPool_t pool,
+                       cudaStream_t pool_stream, bool forward_buffers) {
   validate_geometry(g);
   CBCT_REQUIRE(n_views > 0, "n_views must be positive");
   CBCT_REQUIRE(angles && offsets, "angles/offsets are NULL");
@@ -199,15 +257,17 @@ static cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const
     p->hviews.push_back(make_view(*g, angles[i], offsets[2 * i], offsets[2 * i + 1]));
   }
   CBCT_CUDA(cudaGetDevice(&p->device));
-  CBCT_CUDA(cudaMalloc(&p->d_views, sizeof(ViewParams) * n_views));
-  CBCT_CUDA(cudaMemcpy(p->d_views, p->hviews.data(), sizeof(ViewParams) * n_views, cudaMemcpyHostToDevice));
+  p->pool = pool;
+  p->pool_stream = pool_stream;
+  p->d_views = plan_alloc_n<ViewParams>(p.get(), n_views);
+  plan_upload(p.get(), p->d_views, p->hviews.data(), sizeof(ViewParams) * n_views);
   const size_t tiles = (size_t)((g->width + kTU - 1) / kTU) * ((g->height + kTV - 1) / kTV);
   p->n_partials = std::max<size_t>(tiles * n_views, 148 * 4);
-  CBCT_CUDA(cudaMalloc(&p->d_partials, sizeof(double) * p->n_partials));
-  CBCT_CUDA(cudaMalloc(&p->d_flags, sizeof(int) * 4));
-  CBCT_CUDA(cudaMemset(p->d_flags, 0, sizeof(int) * 4));
+  p->d_partials = plan_alloc_n<double>(p.get(), p->n_partials);
+  p->d_flags = plan_alloc_n<int>(p.get(), 4);
+  plan_memset(p.get(), p->d_flags, 0, sizeof(int) * 4);
   forward_choose_variant(p.get());
-  forward_prepare(p.get());
+  if (forward_buffers) forward_prepare(p.get());
   backproject_choose_variant(p.get());
   backproject_prepare(p.get());
   return p.release();
@@ -221,34 +281,13 @@ static int subset_index(const cbct_plan* p, int s) {
 
 static float* proj_scratch(cbct_plan* p, size_t elems) {
   if (p->proj_scratch_elems < elems) {
-    cudaFree(p->d_proj_scratch);
+    plan_dealloc(p, p->d_proj_scratch);
     p->d_proj_scratch = nullptr;
     p->proj_scratch_elems = 0;
-    CBCT_CUDA(cudaMalloc(&p->d_proj_scratch, elems * sizeof(float)));
+    p->d_proj_scratch = plan_alloc_n<float>(p, elems);
     p->proj_scratch_elems = elems;
   }
   return p->d_proj_scratch;
-}
-
-template <class F>
-cbct_status guard(F&& f) {
-  try {
-    f();
-    g_last_error.clear();
-    return CBCT_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.status;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return CBCT_ERR_OUT_OF_MEMORY;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return CBCT_ERR_INTERNAL;
-  } catch (...) {
-    g_last_error = "unknown error";
-    return CBCT_ERR_INTERNAL;
-  }
 }
 
 static cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -275,7 +314,7 @@ const char* cbct_status_string(cbct_status s) {
   return "CBCT_ERR_UNKNOWN";
 }
 
-const char* cbct_last_error(void) { return g_last_error.c_str(); }
+const char* cbct_last_error(void) { return last_error_slot().c_str(); }
 const char* cbct_version(void) { return "gt-tomography_b200 0.1 (sm_100a)"; }
 
 cbct_status cbct_subset_partition(int32_t n_views, const int32_t* view_bin, int32_t n_subsets, int32_t* order_out,
@@ -311,20 +350,14 @@ cbct_status cbct_cosine_weights(const cbct_geometry* g, float* out) {
 cbct_status cbct_is_short_scan(const cbct_geometry* g, const float* angles, int32_t n, int32_t* out) {
   return guard([&] {
     CBCT_REQUIRE(g && angles && out && n > 0, "bad arguments");
-    const float span = *std::max_element(angles, angles + n);
-    const float delta = std::atan(g->fov_u / (2.0f * g->SDD));
-    const float pi = 3.14159265358979f;
-    *out = (span * pi / 180.0f > pi + 3.0f * delta) ? 0 : 1;
+    *out = short_scan_rule(*g, angles, n) ? 1 : 0;
   });
 }
 
 cbct_status cbct_offset_override(const cbct_geometry* g, const float* offsets, int32_t n, int32_t* out) {
   return guard([&] {
     CBCT_REQUIRE(g && offsets && out && n > 0, "bad arguments");
-    float mx = 0.f;
-    for (int i = 0; i < n; ++i) mx += offsets[2 * i];
-    mx /= float(n);
-    *out = std::fabs(mx) > g->fov_u * 0.1f ? 1 : 0;
+    *out = offset_override_rule(*g, offsets, n) ? 1 : 0;
   });
 }
 
@@ -334,7 +367,8 @@ cbct_status cbct_plan_create(const cbct_geometry* g, const float* angles_deg, co
   return guard([&] {
     CBCT_REQUIRE(plan_out, "plan_out is NULL");
     *plan_out = nullptr;
-    *plan_out = plan_create(g, angles_deg, offsets_xy, n_views, subset_sizes, n_subsets, offset_correction);
+    *plan_out = plan_create(g, angles_deg, offsets_xy, n_views, subset_sizes, n_subsets, offset_correction, nullptr,
+                            nullptr, true);
   });
 }
 
@@ -465,7 +499,33 @@ cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float
                      float* work, void* stream) {
   return guard([&] {
     CBCT_REQUIRE(plan && proj && vol, "NULL argument");
-    fdk_run(plan, proj, vol, filter, flags, work, S(stream));
+    fdk_run(plan, proj, vol, filter, flags, work, S(stream), CBCT_F32);
+  });
+}
+
+static void require_dtype(cbct_dtype dt) {
+  CBCT_REQUIRE(dt == CBCT_F32 || dt == CBCT_F16 || dt == CBCT_BF16, "unknown storage type");
+}
+
+cbct_status cbct_fdk_filter_ex(cbct_plan* plan, int32_t s, cbct_dtype proj_dtype, const void* proj_in,
+                               float* proj_out, const float* filter, uint32_t flags, void* stream) {
+  return guard([&] {
+    const int i = subset_index(plan, s);
+    require_dtype(proj_dtype);
+    CBCT_REQUIRE(proj_in && proj_out, "NULL array");
+    CBCT_REQUIRE(proj_dtype == CBCT_F32 || (const void*)proj_out != proj_in,
+                 "a 16-bit input cannot be filtered in place");
+    fdk_filter_launch(plan, i, proj_in, proj_out, filter, flags, S(stream), proj_dtype);
+  });
+}
+
+cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj, float* vol, const float* filter,
+                        uint32_t flags, float* work, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && proj && vol, "NULL argument");
+    require_dtype(proj_dtype);
+    CBCT_REQUIRE(proj_dtype == CBCT_F32 || (const void*)work != proj, "a 16-bit input cannot be filtered in place");
+    fdk_run(plan, proj, vol, filter, flags, work, S(stream), proj_dtype);
   });
 }
 
@@ -546,10 +606,11 @@ static cbct_solver_params solver_defaults(const cbct_solver_params* p) {
   d.use_graph = 0;
   d.storage = CBCT_F32;
   d.refine_every = 0;
+  d.proj_storage = CBCT_F32;
   return p ? *p : d;
 }
 
-cbct_status cbct_osmom_solve(cbct_plan* plan, const float* b, const float* x0, float* z_out,
+cbct_status cbct_osmom_solve(cbct_plan* plan, const void* b, const float* x0, float* z_out,
                              const cbct_solver_params* params, double* resid_norm2_out, void* stream) {
   return guard([&] {
     CBCT_REQUIRE(plan && b && z_out, "NULL argument");
@@ -565,6 +626,7 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
     CBCT_REQUIRE(plan && b && x_out, "NULL argument");
     const cbct_solver_params prm = solver_defaults(params);
     CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
+    if (prm.proj_storage != CBCT_F32) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART takes float projections");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
   });
 }

@@ -16,9 +16,6 @@
 
 namespace cbct {
 
-void osmom_solve(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
-                 double* resid, cudaStream_t st);
-
 namespace {
 
 // Streams of the pool, per device, created on first use and kept.

@@ -5,6 +5,7 @@
 #include <cudaTypedefs.h>
 #include <algorithm>
 #include <cstdint>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -36,6 +37,32 @@ struct Error : std::runtime_error {
     if (!(cond)) throw ::cbct::Error(CBCT_ERR_INVALID_ARGUMENT, msg);                   \
   } while (0)
 
+// Thread-local message of the calling thread's last failed entry point (abi.cu).
+std::string& last_error_slot();
+
+// Runs f and converts what it throws into a status and the thread's message.
+// Every C entry point is one guard call; nothing throws across the ABI.
+template <class F>
+cbct_status guard(F&& f) {
+  try {
+    f();
+    last_error_slot().clear();
+    return CBCT_OK;
+  } catch (const Error& e) {
+    last_error_slot() = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    last_error_slot() = "host allocation failed";
+    return CBCT_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    last_error_slot() = e.what();
+    return CBCT_ERR_INTERNAL;
+  } catch (...) {
+    last_error_slot() = "unknown error";
+    return CBCT_ERR_INTERNAL;
+  }
+}
+
 // Host threads used for plan set-up loops.
 inline int host_threads() {
   const unsigned hc = std::thread::hardware_concurrency();
@@ -56,6 +83,9 @@ void parallel_for(int n, F&& f) {
   f(0, std::min(n, chunk), 0);
   for (auto& x : th) x.join();
 }
+
+// Bytes per element of a storage type.
+inline size_t dtype_size(cbct_dtype dt) { return dt == CBCT_F32 ? 4 : 2; }
 
 inline void check_launch(const char* what) {
   cudaError_t e = cudaGetLastError();
@@ -163,11 +193,33 @@ struct cbct_plan {
   int force_gather = 0;
   const unsigned char* d_mask = nullptr;  // voxel mask applied after back-projection (caller-owned)
   const float* d_pweights = nullptr;      // projection weights, all views in subset order (caller-owned)
+
+  // Device memory source.  Plans of the serving loop draw every buffer from
+  // its stream-ordered pool on `pool_stream` (cudaMallocFromPoolAsync /
+  // cudaFreeAsync), so that concurrent requests never meet the implicit
+  // device synchronisation of cudaMalloc/cudaFree; such a plan is used on
+  // `pool_stream` only.  Other plans use cudaMalloc.
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t pool_stream = nullptr;
+  std::vector<std::pair<void*, size_t>> allocs;  // live plan-owned buffers
+  size_t dev_bytes = 0, dev_bytes_peak = 0;
 };
 
 namespace cbct {
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+// Plan-owned device memory (abi.cu): cudaMalloc, or the serving pool in
+// stream order (see cbct_plan::pool).  plan_upload copies host data that may
+// be released as soon as the call returns.
+void* plan_alloc(cbct_plan* p, size_t bytes);
+void plan_dealloc(cbct_plan* p, void* ptr);
+void plan_upload(cbct_plan* p, void* dst, const void* src, size_t bytes);
+void plan_memset(cbct_plan* p, void* dst, int value, size_t bytes);
+template <class T>
+T* plan_alloc_n(cbct_plan* p, size_t n) {
+  return static_cast<T*>(plan_alloc(p, n * sizeof(T)));
+}
 
 // Raises a kernel's dynamic shared-memory limit once (no-op when already high
 // enough, so it is safe to call before launches that may be captured).
@@ -175,9 +227,10 @@ void ensure_smem_attr(const void* func, size_t bytes);
 
 // forward.cu
 void forward_prepare(cbct_plan* p);
-void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
+// b: measured projections of storage type b_dtype (residual mode).
+void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const void* b,
                        const float* pw, float scale, int mode, int apply_offset, int accumulate,
-                       double* norm2_out, cudaStream_t st);
+                       double* norm2_out, cudaStream_t st, cbct_dtype b_dtype = CBCT_F32);
 void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out,
                     const float* b, float scale, int mode, int apply_offset, int accumulate,
                     double* norm2_out, cudaStream_t st);
@@ -190,8 +243,11 @@ void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int 
 // weights.cu
 void offset_weight_launch(cbct_plan* p, int s, const float* in, float* out, int variant,
                           cudaStream_t st);
-void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const float* filter,
-                       uint32_t flags, cudaStream_t st);
+// in: projections of storage type in_dtype; out: float (may alias in when float).
+void fdk_filter_launch(cbct_plan* p, int s, const void* in, float* out, const float* filter,
+                       uint32_t flags, cudaStream_t st, cbct_dtype in_dtype = CBCT_F32);
+// Builds the FDK tables for `filter` now (they are otherwise made on first use).
+void fdk_prepare(cbct_plan* p, const float* filter);
 // solver.cu
 void reduce_launch(int kind, const float* a, const float* b, size_t n, double* partials,
                    size_t n_partials, double* out, cudaStream_t st);
@@ -205,6 +261,22 @@ void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, uns
                         cudaStream_t st);
 void apply_mask_launch(float* vol, const unsigned char* mask, size_t n, cudaStream_t st);
 void mul_launch(float* out, const float* in, const float* w, size_t n, cudaStream_t st);
+
+// plans and set-up rules (abi.cu)
+void validate_geometry(const cbct_geometry* g);
+// forward_buffers = false leaves out the forward projector's transposed-volume
+// buffer (plans that only back-project; their forward calls take the gather path).
+cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float* offsets, int n_views,
+                       const int* subset_sizes, int n_subsets, const int* offcorr, cudaMemPool_t pool,
+                       cudaStream_t pool_stream, bool forward_buffers);
+void plan_free(cbct_plan* p);
+bool short_scan_rule(const cbct_geometry& g, const float* angles, int n);
+bool offset_override_rule(const cbct_geometry& g, const float* offsets, int n);
+// solver.cu
+void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const cbct_solver_params& prm,
+                 double* resid, cudaStream_t st);
+void fdk_run(cbct_plan* p, const void* proj, float* vol, const float* filter, uint32_t flags, float* work,
+             cudaStream_t st, cbct_dtype proj_dtype);
 
 // host helpers (abi.cu)
 void default_filter(int W, float* out);

@@ -19,6 +19,13 @@ template <> __device__ __forceinline__ float ld_f<__half>(const __half* p) {
 template <> __device__ __forceinline__ float ld_f<__nv_bfloat16>(const __nv_bfloat16* p) {
   return __bfloat162float(__ldg(p));
 }
+// Element i of an array whose storage type is chosen at run time (cbct_dtype).
+__device__ __forceinline__ float ld_any(const void* p, size_t i, int dtype) {
+  if (dtype == CBCT_F16) return ld_f(static_cast<const __half*>(p) + i);
+  if (dtype == CBCT_BF16) return ld_f(static_cast<const __nv_bfloat16*>(p) + i);
+  return ld_f(static_cast<const float*>(p) + i);
+}
+
 template <class V> __device__ __forceinline__ float sm_f(V v);
 template <> __device__ __forceinline__ float sm_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ float sm_f<__half>(__half v) { return __half2float(v); }

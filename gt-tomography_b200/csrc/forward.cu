@@ -33,7 +33,8 @@ enum { kModeStore = 0, kModeResidual = 1, kModeRecip = 2 };
 
 struct FwdOut {
   float* out;            // projections of the subset (W,H,P_s)
-  const float* b;        // measured projections (residual mode; NULL reads as 0)
+  const void* b;         // measured projections (residual mode; NULL reads as 0)
+  int b_dtype;           // storage type of b (cbct_dtype)
   const float* pw;       // per-pixel weight (residual mode; nullable)
   float scale;           // residual scale
   int mode;
@@ -99,7 +100,7 @@ __device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& g
     } else if (o.mode == kModeRecip) {
       o.out[idx] = 1.f / fmaxf(val, 1e-6f);
     } else {
-      const float d = o.b ? val - o.b[idx] : val;
+      const float d = o.b ? val - ld_any(o.b, idx, o.b_dtype) : val;
       sq = double(d) * double(d);
       float w = o.scale * wp;
       if (o.pw) w *= o.pw[idx];
@@ -407,8 +408,6 @@ __global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant_
 }
 
 // ------------------------------------------------------------------ host
-size_t dtype_size(cbct_dtype dt) { return dt == CBCT_F32 ? 4 : 2; }
-
 CUtensorMapDataType tma_dtype(cbct_dtype dt) {
   switch (dt) {
     case CBCT_F32: return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -615,7 +614,7 @@ void forward_prepare(cbct_plan* p) {
   bool any_x = false;
   for (int s = 0; s <= p->n_subsets; ++s) any_x = any_x || p->subset_has_xdom[s];
   if (any_x && !p->d_volT)
-    CBCT_CUDA(cudaMalloc(&p->d_volT, (size_t)p->g.nx * p->g.ny * p->g.nz * sizeof(float)));
+    p->d_volT = plan_alloc_n<float>(p, (size_t)p->g.nx * p->g.ny * p->g.nz);
 }
 
 void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
@@ -624,13 +623,14 @@ void forward_launch(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* 
   forward_launch_ex(p, s, dt, vol, out, b, nullptr, scale, mode, apply_offset, accumulate, norm2_out, st);
 }
 
-void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
+void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const void* b,
                        const float* pw, float scale, int mode, int apply_offset, int accumulate,
-                       double* norm2_out, cudaStream_t st) {
+                       double* norm2_out, cudaStream_t st, cbct_dtype b_dtype) {
   FwdOut o;
   o.out = out;
   o.pw = pw;
   o.b = b;
+  o.b_dtype = b_dtype;
   o.scale = scale;
   o.mode = mode;
   o.apply_offset = apply_offset;

@@ -14,10 +14,13 @@
 // operation, a fresh device image per subset step (:153) and in denoise (:209),
 // and host-synchronised norms (:147-149, :206).
 #include <cuda_runtime.h>
+#include <cufft.h>
+#include <dlfcn.h>
 #include <math_constants.h>
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -79,6 +82,8 @@ __global__ void fwd_kernel(float* __restrict__ projections, const float* __restr
   projections[idx] = accumulate ? projections[idx] + result * sampling_distance : result * sampling_distance;
 }
 
+// FBP: the 1/U^2 weight of conebeam_projection.cu:1008-1026 (filtered back-projection).
+template <bool FBP>
 __global__ void bp_kernel(float* __restrict__ image, const float* __restrict__ angles,
                           const float2* __restrict__ offsets, int nx, int ny, int nz, float3 L, float2 ps_mm, int P,
                           float SDD, float SAD, bool accumulate, cudaTextureObject_t tex) {
@@ -98,7 +103,14 @@ __global__ void bp_kernel(float* __restrict__ image, const float* __restrict__ a
     d.x /= d.y; d.z /= d.y; d.y = 1.0f;
     const float ex = SDD * d.x - offsets[p].x, ez = SDD * d.z - offsets[p].y;
     const float uu = ex / ps_mm.x + 0.5f, vv = ez / ps_mm.y + 0.5f;
-    result += tex2DLayered<float>(tex, uu, vv, p);
+    float weight = 1.0f;
+    if (FBP) {
+      const float beta = angles[p] * (CUDART_PI_F / 180.0f);
+      const float r = hypotf(px, py), phi = atan2f(py, px);
+      const float U = (SAD + r * sinf(beta - phi)) / SAD;
+      weight = 1.0f / (U * U);
+    }
+    result += weight * tex2DLayered<float>(tex, uu, vv, p);
   }
   image[idx] = incoming + result;
 }
@@ -149,6 +161,34 @@ __global__ void red_abs(const float* a, size_t n, double* out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+// FDK pre-processing passes of conebeam_projection.cu:1483-1521, one kernel
+// per Gadgetron array operation.
+__global__ void ew_mul_bcast(float* a, const float* w, size_t n, size_t m) {   // a *= w (broadcast)
+  size_t i = gidx();
+  if (i < n) a[i] *= w[i % m];
+}
+__global__ void ew_cmul_bcast(float2* a, const float* f, size_t n, size_t m) {  // complex *= real filter
+  size_t i = gidx();
+  if (i < n) {
+    const float w = f[i % m];
+    a[i].x *= w;
+    a[i].y *= w;
+  }
+}
+__global__ void pad_rows(const float* in, float* out, int W, size_t n_out) {    // centred pad to 2W
+  size_t i = gidx();
+  if (i >= n_out) return;
+  const size_t r = i / (2 * W);
+  const int x = int(i % (2 * W)) - W / 2;
+  out[i] = (x >= 0 && x < W) ? in[r * W + x] : 0.0f;
+}
+__global__ void crop_rows(const float* in, float* out, int W, size_t n_out) {   // crop at W/2 (:1510)
+  size_t i = gidx();
+  if (i >= n_out) return;
+  const size_t r = i / W;
+  out[i] = in[r * 2 * W + (i % W) + W / 2];
 }
 
 template <class K, class... A>
@@ -262,7 +302,7 @@ void backproject(const cbct_geometry& g, const float* angles, const float* offse
   check(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
   dim3 b, gr;
   setup_grid((size_t)g.nx * g.ny * g.nz, &b, &gr);
-  bp_kernel<<<gr, b>>>(vol, up.angles, up.offsets, g.nx, g.ny, g.nz, make_float3(g.lx, g.ly, g.lz),
+  bp_kernel<false><<<gr, b>>>(vol, up.angles, up.offsets, g.nx, g.ny, g.nz, make_float3(g.lx, g.ly, g.lz),
                        make_float2(g.fov_u, g.fov_v), P, g.SDD, g.SAD, accumulate, tex);
   check(cudaGetLastError(), "plain bp_kernel");
   check(cudaDeviceSynchronize(), "plain bp_kernel");
@@ -338,22 +378,158 @@ void osmom(const cbct_geometry& g, const float* angles, const float* offsets, in
   cudaFree(tmp_proj);
 }
 
-template <class F>
-cbct_status guard(F&& f) {
-  try {
-    f();
-    return CBCT_OK;
-  } catch (const Error& e) {
-    return e.status;
-  } catch (...) {
-    return CBCT_ERR_INTERNAL;
+// cuFFT, as the reference's cb_fft/cb_ifft call it (conebeam_projection.cu:87-139).
+// Only this baseline uses it; it is opened on first use so that the library
+// itself has no link-time dependency on cuFFT.
+struct Cufft {
+  decltype(&cufftPlanMany) plan_many = nullptr;
+  decltype(&cufftExecR2C) exec_r2c = nullptr;
+  decltype(&cufftExecC2R) exec_c2r = nullptr;
+  decltype(&cufftDestroy) destroy = nullptr;
+};
+
+const Cufft& cufft() {
+  static Cufft api;
+  static std::once_flag once;
+  static std::string err;
+  std::call_once(once, [] {
+    void* h = dlopen("libcufft.so.11", RTLD_NOW | RTLD_LOCAL);
+    if (!h) h = dlopen("libcufft.so", RTLD_NOW | RTLD_LOCAL);
+    if (!h) {
+      err = "plain FDK path: cannot open libcufft";
+      return;
+    }
+    api.plan_many = reinterpret_cast<decltype(api.plan_many)>(dlsym(h, "cufftPlanMany"));
+    api.exec_r2c = reinterpret_cast<decltype(api.exec_r2c)>(dlsym(h, "cufftExecR2C"));
+    api.exec_c2r = reinterpret_cast<decltype(api.exec_c2r)>(dlsym(h, "cufftExecC2R"));
+    api.destroy = reinterpret_cast<decltype(api.destroy)>(dlsym(h, "cufftDestroy"));
+    if (!api.plan_many || !api.exec_r2c || !api.exec_c2r || !api.destroy) err = "plain FDK path: cuFFT symbols missing";
+  });
+  if (!err.empty()) throw Error(CBCT_ERR_UNSUPPORTED, err);
+  return api;
+}
+
+void cufft_check(cufftResult r, const char* what) {
+  if (r != CUFFT_SUCCESS) throw Error(CBCT_ERR_CUDA, std::string(what) + " failed (cufftResult " + std::to_string(int(r)) + ")");
+}
+
+// hoCuConebeamProjectionOperator::mult_MH with FBP (hoCuConebeamProjectionOperator.cpp:235-254)
+// over conebeam_backwards_projection<true> (conebeam_projection.cu:1300-1649):
+// cosine weights computed on the host per operator (.cpp:64-102), batches of
+// views uploaded from host memory on two alternating streams, per batch the
+// cosine multiply, centred pad to 2W, cuFFT R2C (plan made and destroyed per
+// call), filter multiply, C2R, /2W, crop, offset weight, a layered cudaArray
+// copy and the 1/U^2-weighted texture back-projection; the volume comes back
+// to the host and is scaled by 2/P there.
+void fdk(const cbct_geometry& g, const float* angles, const float* offsets, int P, const float* proj_host,
+         float* vol_host, const float* filter, bool offset_correction, int per_batch) {
+  const Cufft& F = cufft();
+  const int W = g.width, H = g.height;
+  const size_t plane = (size_t)W * H, nv = (size_t)g.nx * g.ny * g.nz;
+  std::vector<float> cw(plane), filt(W + 1);
+  const double SAD = g.SAD, SDD = g.SDD;
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const double xx = (double(x) / W - 0.5) * g.fov_u, yy = (double(y) / H - 0.5) * g.fov_v;
+      const double s = SAD * xx / SDD, v = SAD * yy / SDD;
+      cw[(size_t)y * W + x] = float(SAD / std::sqrt(SAD * SAD + s * s + v * v));
+    }
+  if (filter) std::copy(filter, filter + W + 1, filt.begin());
+  else default_filter(W, filt.data());
+  float *d_cw = nullptr, *d_filter = nullptr, *image = nullptr, *buf = nullptr, *buf2 = nullptr;
+  check(cudaMalloc(&d_cw, plane * 4), "cudaMalloc");
+  check(cudaMemcpy(d_cw, cw.data(), plane * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+  check(cudaMalloc(&d_filter, (W + 1) * 4), "cudaMalloc");
+  check(cudaMemcpy(d_filter, filt.data(), (W + 1) * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+  check(cudaMalloc(&image, nv * 4), "cudaMalloc");
+  const int B = std::max(1, std::min(per_batch, P));
+  const int nb = (P + B - 1) / B;
+  check(cudaMalloc(&buf, plane * B * 4), "cudaMalloc");
+  check(cudaMalloc(&buf2, plane * B * 4), "cudaMalloc");
+  cudaStream_t main_st, indy_st;
+  check(cudaStreamCreate(&main_st), "cudaStreamCreate");
+  check(cudaStreamCreate(&indy_st), "cudaStreamCreate");
+  {
+    Uploads up(angles, offsets, P);
+    check(cudaMemcpyAsync(buf, proj_host, plane * B * 4, cudaMemcpyHostToDevice, main_st), "cudaMemcpyAsync");
+    for (int batch = 0; batch < nb; ++batch) {
+      const int from = batch * B, n = std::min(P, from + B) - from;
+      const size_t nproj = plane * n, npad = 2 * plane * n, nspec = (size_t)(W + 1) * H * n;
+      launch_ew(ew_mul_bcast, nproj, buf, (const float*)d_cw, nproj, plane);
+      float* padded = nullptr;
+      float2* spec = nullptr;
+      check(cudaMalloc(&padded, npad * 4), "cudaMalloc");
+      launch_ew(pad_rows, npad, (const float*)buf, padded, W, npad);
+      check(cudaMalloc(&spec, nspec * 8), "cudaMalloc");
+      int len = 2 * W;
+      cufftHandle pl;
+      cufft_check(F.plan_many(&pl, 1, &len, nullptr, 1, 2 * W, nullptr, 1, W + 1, CUFFT_R2C, H * n), "cufftPlanMany");
+      cufft_check(F.exec_r2c(pl, padded, reinterpret_cast<cufftComplex*>(spec)), "cufftExecR2C");
+      cufft_check(F.destroy(pl), "cufftDestroy");
+      launch_ew(ew_cmul_bcast, nspec, spec, (const float*)d_filter, nspec, (size_t)(W + 1));
+      cufft_check(F.plan_many(&pl, 1, &len, nullptr, 1, W + 1, nullptr, 1, 2 * W, CUFFT_C2R, H * n), "cufftPlanMany");
+      cufft_check(F.exec_c2r(pl, reinterpret_cast<cufftComplex*>(spec), padded), "cufftExecC2R");
+      cufft_check(F.destroy(pl), "cufftDestroy");
+      launch_ew(ew_scale, npad, padded, 1.0f / float(2 * W), npad);
+      launch_ew(crop_rows, nproj, (const float*)padded, buf, W, nproj);
+      cudaFree(spec);
+      cudaFree(padded);
+      if (offset_correction)
+        launch_ew(offset_kernel, nproj, buf, (const float2*)up.offsets + from, W, H, n, make_float2(g.fov_u, g.fov_v));
+      cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+      cudaExtent ext = make_cudaExtent(W, H, n);
+      cudaArray_t arr = nullptr;
+      check(cudaMalloc3DArray(&arr, &ch, ext, cudaArrayLayered), "cudaMalloc3DArray(layered)");
+      cudaMemcpy3DParms cp = {};
+      cp.srcPtr = make_cudaPitchedPtr((void*)buf, W * sizeof(float), W, H);
+      cp.dstArray = arr;
+      cp.extent = ext;
+      cp.kind = cudaMemcpyDeviceToDevice;
+      check(cudaMemcpy3DAsync(&cp, main_st), "cudaMemcpy3DAsync");
+      cudaResourceDesc rd = {};
+      rd.resType = cudaResourceTypeArray;
+      rd.res.array.array = arr;
+      cudaTextureDesc td = {};
+      td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+      td.filterMode = cudaFilterModeLinear;
+      td.readMode = cudaReadModeElementType;
+      td.normalizedCoords = 1;
+      cudaTextureObject_t tex = 0;
+      check(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+      if (batch + 1 < nb) {
+        const int nf = std::min(P, from + 2 * B) - (from + B);
+        check(cudaMemcpyAsync(buf2, proj_host + plane * (from + B), plane * nf * 4, cudaMemcpyHostToDevice, indy_st),
+              "cudaMemcpyAsync");
+      }
+      dim3 b, gr;
+      setup_grid(nv, &b, &gr);
+      bp_kernel<true><<<gr, b, 0, main_st>>>(image, up.angles + from, up.offsets + from, g.nx, g.ny, g.nz,
+                                             make_float3(g.lx, g.ly, g.lz), make_float2(g.fov_u, g.fov_v), n,
+                                             g.SDD, g.SAD, batch > 0, tex);
+      check(cudaGetLastError(), "plain bp_kernel<FBP>");
+      cudaDestroyTextureObject(tex);
+      cudaFreeArray(arr);
+      std::swap(buf, buf2);
+      std::swap(main_st, indy_st);
+    }
+    check(cudaMemcpy(vol_host, image, nv * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
   }
+  const float sc = 2.0f / float(P);  // image_3d *= 2/P on the host array (.cpp:253)
+  for (size_t i = 0; i < nv; ++i) vol_host[i] *= sc;
+  cudaFree(buf);
+  cudaFree(buf2);
+  cudaFree(image);
+  cudaFree(d_cw);
+  cudaFree(d_filter);
+  cudaStreamDestroy(main_st);
+  cudaStreamDestroy(indy_st);
 }
 
 }  // namespace plain
 }  // namespace cbct
 
 using namespace cbct::plain;
+using cbct::guard;
 
 extern "C" {
 
@@ -380,6 +556,16 @@ cbct_status cbct_plain_osmom_solve(const cbct_geometry* g, const float* angles, 
     if (!g || !angles || !offsets || !sizes || !offcorr || !b || !z_out || S < 1)
       throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
     osmom(*g, angles, offsets, n, sizes, S, offcorr, b, z_out, iterations, nonneg != 0, resid);
+  });
+}
+
+cbct_status cbct_plain_fdk(const cbct_geometry* g, const float* angles, const float* offsets, int32_t n,
+                           const float* proj_host, float* vol_host, const float* filter, int32_t offset_correction,
+                           int32_t views_per_batch) {
+  return guard([&] {
+    if (!g || !angles || !offsets || !proj_host || !vol_host || n < 1 || views_per_batch < 1)
+      throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
+    fdk(*g, angles, offsets, n, proj_host, vol_host, filter, offset_correction != 0, views_per_batch);
   });
 }
 

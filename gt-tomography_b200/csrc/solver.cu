@@ -35,9 +35,6 @@ void backproject_mom_launch(cbct_plan* p, int s, const float* proj, float* z, fl
                             const float* precon, float step, float mom, int nonneg, cudaStream_t st);
 void backproject_sart_launch(cbct_plan* p, int s, const float* proj, float* x, const float* V,
                              float step, int nonneg, cudaStream_t st);
-void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, float* out, const float* b,
-                       const float* pw, float scale, int mode, int apply_offset, int accumulate,
-                       double* norm2_out, cudaStream_t st);
 
 namespace {
 
@@ -188,17 +185,21 @@ static size_t plane_elems(const cbct_plan* p) { return (size_t)p->g.width * p->g
 //  OS-SART: Wp (all views) | r (all views) | V_0 .. V_{S-1}
 static float* workspace(cbct_plan* p, size_t elems) {
   if (p->ws_elems < elems) {
-    if (p->ws) cudaFree(p->ws);
+    plan_dealloc(p, p->ws);
     p->ws = nullptr;
     p->ws_elems = 0;
-    CBCT_CUDA(cudaMalloc(&p->ws, elems * sizeof(float)));
+    p->ws = plan_alloc_n<float>(p, elems);
     p->ws_elems = elems;
   }
   return p->ws;
 }
 
-static void run_osmom(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+static void run_osmom(cbct_plan* p, const void* b, const float* x0, float* z, const cbct_solver_params& prm,
                       double* resid, float* xold, float* D, float* r, void* shadow, cudaStream_t st) {
+  const cbct_dtype bt = prm.proj_storage;
+  auto b_of = [&](int s) {
+    return static_cast<const char*>(b) + plane_elems(p) * p->first[s] * dtype_size(bt);
+  };
   const size_t nv = vol_elems(p);
   const int S = p->n_subsets;
   // Preconditioner: D = 1/max(A^T (W A 1), 1e-6) over every subset, the
@@ -226,11 +227,11 @@ static void run_osmom(cbct_plan* p, const float* b, const float* x0, float* z, c
       float* rs = r + plane_elems(p) * p->first[s];
       if (lowp) {
         convert_launch(z, shadow, nv, prm.storage, st);
-        forward_launch_ex(p, s, prm.storage, shadow, rs, b + plane_elems(p) * p->first[s], nullptr, 1.f, 1,
-                          p->offcorr[s], 0, resid ? resid + step : nullptr, st);
+        forward_launch_ex(p, s, prm.storage, shadow, rs, b_of(s), nullptr, 1.f, 1, p->offcorr[s], 0,
+                          resid ? resid + step : nullptr, st, bt);
       } else {
-        forward_launch_ex(p, s, CBCT_F32, z, rs, b + plane_elems(p) * p->first[s], nullptr, 1.f, 1,
-                          p->offcorr[s], 0, resid ? resid + step : nullptr, st);
+        forward_launch_ex(p, s, CBCT_F32, z, rs, b_of(s), nullptr, 1.f, 1, p->offcorr[s], 0,
+                          resid ? resid + step : nullptr, st, bt);
       }
       const double stepsz = double(prm.beta) / (1.0 + double(prm.gamma) * it) * S;
       const double mom = (told - 1.0) / t;
@@ -329,8 +330,10 @@ static void run_maybe_graph(cbct_plan* p, bool use_graph, const std::vector<uint
   CBCT_CUDA(cudaGraphLaunch(gc->exec, st));
 }
 
-void osmom_solve(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const cbct_solver_params& prm,
                  double* resid, cudaStream_t st) {
+  CBCT_REQUIRE(prm.proj_storage == CBCT_F32 || prm.proj_storage == CBCT_F16 || prm.proj_storage == CBCT_BF16,
+               "unknown projection storage type");
   const size_t nv = vol_elems(p), np = proj_elems(p);
   const bool lowp = prm.storage != CBCT_F32;
   const size_t need = 2 * nv + np + (lowp ? (nv + 1) / 2 + 64 : 0);
@@ -341,7 +344,7 @@ void osmom_solve(cbct_plan* p, const float* b, const float* x0, float* z, const 
   void* shadow = lowp ? (void*)(((uintptr_t)(ws + 2 * nv + np) + 255) & ~uintptr_t(255)) : nullptr;
   std::vector<uint64_t> key = {1, (uint64_t)b, (uint64_t)x0, (uint64_t)z, (uint64_t)resid,
                                (uint64_t)prm.iterations, (uint64_t)prm.non_negativity, (uint64_t)prm.storage,
-                               (uint64_t)prm.refine_every};
+                               (uint64_t)prm.refine_every, (uint64_t)prm.proj_storage};
   uint32_t bb, gg;
   std::memcpy(&bb, &prm.beta, 4);
   std::memcpy(&gg, &prm.gamma, 4);
@@ -372,21 +375,21 @@ void ossart_solve(cbct_plan* p, const float* b, const float* x0, float* x, const
   });
 }
 
-void fdk_run(cbct_plan* p, const float* proj, float* vol, const float* filter, uint32_t flags, float* work,
-             cudaStream_t st) {
+void fdk_run(cbct_plan* p, const void* proj, float* vol, const float* filter, uint32_t flags, float* work,
+             cudaStream_t st, cbct_dtype proj_dtype) {
   const size_t np = proj_elems(p);
   if (!work) {
     if (p->fdk_work_elems < np) {
-      if (p->d_fdk_work) cudaFree(p->d_fdk_work);
+      plan_dealloc(p, p->d_fdk_work);
       p->d_fdk_work = nullptr;
       p->fdk_work_elems = 0;
-      CBCT_CUDA(cudaMalloc(&p->d_fdk_work, np * sizeof(float)));
+      p->d_fdk_work = plan_alloc_n<float>(p, np);
       p->fdk_work_elems = np;
     }
     work = p->d_fdk_work;
   }
   const uint32_t f = flags | CBCT_FDK_RAMP | CBCT_FDK_COSINE;
-  fdk_filter_launch(p, p->n_subsets, proj, work, filter, f, st);
+  fdk_filter_launch(p, p->n_subsets, proj, work, filter, f, st, proj_dtype);
   backproject_launch(p, p->n_subsets, work, vol, 1, 0, 2.f / float(p->n_views), st);
 }
 

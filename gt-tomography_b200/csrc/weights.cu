@@ -48,8 +48,11 @@ constexpr int kFftThreads = 256;
 //   pre[u + W*v]     cosine weight (nullable)
 //   parker[u + W*p]  Parker weight (nullable)
 //   post[u + W*p]    sin^2 offset weight (nullable)
+// T: storage type of the input projections (float, __half, __nv_bfloat16);
+// arithmetic is FP32.  For T = float, in and out may alias.
+template <class T>
 __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(
-    const float* in, float* out, int W, int H, long rows, int L, int logL,
+    const T* in, float* out, int W, int H, long rows, int L, int logL,
     const float* __restrict__ spec, const float2* __restrict__ tw, const float* __restrict__ pre,
     const float* __restrict__ parker, const float* __restrict__ post) {
   extern __shared__ float2 fsm[];
@@ -70,11 +73,11 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(
     for (int n = tid; n < L; n += kFftThreads) {
       float xa = 0.f, xb = 0.f;
       if (n < W) {
-        xa = in[ra * W + n];
+        xa = sm_f(in[ra * W + n]);
         if (pre) xa *= pre[(size_t)va * W + n];
         if (parker) xa *= parker[(size_t)pa * W + n];
         if (hasb) {
-          xb = in[rb * W + n];
+          xb = sm_f(in[rb * W + n]);
           if (pre) xb *= pre[(size_t)vb * W + n];
           if (parker) xb *= parker[(size_t)pb * W + n];
         }
@@ -169,11 +172,11 @@ struct FdkState {
 void fdk_state_free(cbct_plan* p) {
   FdkState* f = static_cast<FdkState*>(p->fdk_state);
   if (!f) return;
-  cudaFree(f->t.spec);
-  cudaFree(f->t.tw);
-  cudaFree(f->t.cosw);
-  cudaFree(f->t.parker);
-  cudaFree(f->t.post);
+  plan_dealloc(p, f->t.spec);
+  plan_dealloc(p, f->t.tw);
+  plan_dealloc(p, f->t.cosw);
+  plan_dealloc(p, f->t.parker);
+  plan_dealloc(p, f->t.post);
   delete f;
   p->fdk_state = nullptr;
 }
@@ -193,9 +196,9 @@ static FdkState* fdk_state(cbct_plan* p, const float* filter) {
     const double pi = 3.14159265358979323846;
     for (int k = 0; k < L / 2; ++k)
       tw[k] = make_float2(float(std::cos(2 * pi * k / L)), float(-std::sin(2 * pi * k / L)));
-    CBCT_CUDA(cudaMalloc(&f->t.tw, sizeof(float2) * tw.size()));
-    CBCT_CUDA(cudaMemcpy(f->t.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
-    CBCT_CUDA(cudaMalloc(&f->t.spec, sizeof(float) * L));
+    f->t.tw = plan_alloc_n<float2>(p, tw.size());
+    plan_upload(p, f->t.tw, tw.data(), sizeof(float2) * tw.size());
+    f->t.spec = plan_alloc_n<float>(p, L);
     // Cosine weights (hoCuConebeamProjectionOperator.cpp:84-97): double, stored float.
     std::vector<float> cw((size_t)W * H);
     const double SAD = p->g.SAD, SDD = p->g.SDD;
@@ -205,8 +208,8 @@ static FdkState* fdk_state(cbct_plan* p, const float* filter) {
         const double s = SAD * xx / SDD, v = SAD * yy / SDD;
         cw[(size_t)y * W + x] = float(SAD / std::sqrt(SAD * SAD + s * s + v * v));
       }
-    CBCT_CUDA(cudaMalloc(&f->t.cosw, sizeof(float) * cw.size()));
-    CBCT_CUDA(cudaMemcpy(f->t.cosw, cw.data(), sizeof(float) * cw.size(), cudaMemcpyHostToDevice));
+    f->t.cosw = plan_alloc_n<float>(p, cw.size());
+    plan_upload(p, f->t.cosw, cw.data(), sizeof(float) * cw.size());
     // Parker weights per (view, u) in FP64 (conebeam_projection.cu:169-194).
     std::vector<float> pk((size_t)W * P), po((size_t)W * P);
     const double eps = 0.001, q = 0.1;
@@ -236,17 +239,17 @@ static FdkState* fdk_state(cbct_plan* p, const float* filter) {
         po[(size_t)v * W + u] = float(w);
       }
     }
-    CBCT_CUDA(cudaMalloc(&f->t.parker, sizeof(float) * pk.size()));
-    CBCT_CUDA(cudaMemcpy(f->t.parker, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice));
-    CBCT_CUDA(cudaMalloc(&f->t.post, sizeof(float) * po.size()));
-    CBCT_CUDA(cudaMemcpy(f->t.post, po.data(), sizeof(float) * po.size(), cudaMemcpyHostToDevice));
+    f->t.parker = plan_alloc_n<float>(p, pk.size());
+    plan_upload(p, f->t.parker, pk.data(), sizeof(float) * pk.size());
+    f->t.post = plan_alloc_n<float>(p, po.size());
+    plan_upload(p, f->t.post, po.data(), sizeof(float) * po.size());
   }
   std::vector<float> want(W + 1);
   if (filter) std::copy(filter, filter + W + 1, want.begin());
   else default_filter(W, want.data());
   if (want != f->filter) {
     std::vector<float> spec = filter_spectrum(want.data(), W, f->L);
-    CBCT_CUDA(cudaMemcpy(f->t.spec, spec.data(), sizeof(float) * f->L, cudaMemcpyHostToDevice));
+    plan_upload(p, f->t.spec, spec.data(), sizeof(float) * f->L);
     f->filter = want;
   }
   return f;
@@ -262,8 +265,24 @@ void offset_weight_launch(cbct_plan* p, int s, const float* in, float* out, int 
   check_launch("offset_weight_kernel");
 }
 
-void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const float* filter,
-                       uint32_t flags, cudaStream_t st) {
+void fdk_prepare(cbct_plan* p, const float* filter) { fdk_state(p, filter); }
+
+template <class T>
+static void fdk_filter_typed(const void* in, float* out, int W, int H, long rows, const FdkState* f,
+                             const float* pre, const float* pk, const float* post, cudaStream_t st) {
+  const int L = f->L;
+  const size_t smem = sizeof(float2) * (L + L / 2) + sizeof(float) * L;
+  if (smem > 200 * 1024) throw Error(CBCT_ERR_UNSUPPORTED, "detector too wide for the FDK filter");
+  ensure_smem_attr((const void*)fdk_filter_kernel<T>, smem);
+  const long npairs = (rows + 1) / 2;
+  const int blocks = (int)std::min<long>(npairs, 148L * 8);
+  fdk_filter_kernel<T><<<blocks, kFftThreads, smem, st>>>(static_cast<const T*>(in), out, W, H, rows, L, f->logL,
+                                                          f->t.spec, f->t.tw, pre, pk, post);
+  check_launch("fdk_filter_kernel");
+}
+
+void fdk_filter_launch(cbct_plan* p, int s, const void* in, float* out, const float* filter,
+                       uint32_t flags, cudaStream_t st, cbct_dtype in_dtype) {
   const int first = p->first[s], cnt = p->count[s];
   const int W = p->g.width, H = p->g.height;
   if (cnt == 0) return;
@@ -277,15 +296,12 @@ void fdk_filter_launch(cbct_plan* p, int s, const float* in, float* out, const f
     // the element-wise path instead.
     throw Error(CBCT_ERR_UNSUPPORTED, "cbct_fdk_filter without CBCT_FDK_RAMP is not implemented");
   }
-  const int L = f->L;
-  const size_t smem = sizeof(float2) * (L + L / 2) + sizeof(float) * L;
-  if (smem > 200 * 1024) throw Error(CBCT_ERR_UNSUPPORTED, "detector too wide for the FDK filter");
-  ensure_smem_attr((const void*)fdk_filter_kernel, smem);
-  const long npairs = (rows + 1) / 2;
-  const int blocks = (int)std::min<long>(npairs, 148L * 8);
-  fdk_filter_kernel<<<blocks, kFftThreads, smem, st>>>(in, out, W, H, rows, L, f->logL, f->t.spec, f->t.tw,
-                                                       pre, pk, post);
-  check_launch("fdk_filter_kernel");
+  switch (in_dtype) {
+    case CBCT_F32: fdk_filter_typed<float>(in, out, W, H, rows, f, pre, pk, post, st); break;
+    case CBCT_F16: fdk_filter_typed<__half>(in, out, W, H, rows, f, pre, pk, post, st); break;
+    case CBCT_BF16: fdk_filter_typed<__nv_bfloat16>(in, out, W, H, rows, f, pre, pk, post, st); break;
+    default: throw Error(CBCT_ERR_INVALID_ARGUMENT, "unknown projection storage type");
+  }
 }
 
 }  // namespace cbct

@@ -61,6 +61,28 @@ def _need_cuda_f32(t, shape, what):
         raise ValueError(f"{what} has shape {tuple(t.shape)}, expected {tuple(shape)}")
 
 
+def _dtype_code(dtype) -> int:
+    """cbct_dtype of a torch dtype (float32, float16, bfloat16)."""
+    T = torch()
+    codes = {T.float32: L.CBCT_F32, T.float16: L.CBCT_F16, T.bfloat16: L.CBCT_BF16}
+    if dtype not in codes:
+        raise TypeError(f"storage type must be float32, float16 or bfloat16, got {dtype}")
+    return codes[dtype]
+
+
+def _storage_of(t, shape, what) -> int:
+    """Checks a contiguous CUDA tensor of the given shape; returns its cbct_dtype."""
+    T = torch()
+    if not isinstance(t, T.Tensor) or not t.is_cuda:
+        raise TypeError(f"{what} must be a CUDA tensor")
+    code = _dtype_code(t.dtype)
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{what} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    return code
+
+
 # ----------------------------------------------------------------- data model
 @dataclass
 class CBCT_geometry:
@@ -271,10 +293,12 @@ class Plan:
         return proj_out
 
     def fdk(self, proj, out, filt=None, flags=0, work=None, stream=None):
-        _need_cuda_f32(proj, self.proj_shape(-1), "projections")
+        """FDK of every view (cbct_fdk / cbct_fdk_ex): proj may be float32,
+        float16 or bfloat16 (the storage type); arithmetic is FP32."""
+        dt = _storage_of(proj, self.proj_shape(-1), "projections")
         _need_cuda_f32(out, self.vol_shape, "volume")
         f = None if filt is None else np.ascontiguousarray(filt, np.float32)
-        L.call("cbct_fdk", self._h, _ptr(proj), _ptr(out), None if f is None else f.ctypes.data, flags,
+        L.call("cbct_fdk_ex", self._h, dt, _ptr(proj), _ptr(out), None if f is None else f.ctypes.data, flags,
                _ptr(work), _stream(stream))
         return out
 
@@ -314,8 +338,12 @@ class Plan:
 
     def osmom(self, b, z_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
               storage=L.CBCT_F32, refine_every=0, resid=None, stream=None):
+        """osMOMSolverD::solve on the device.  storage: type of the forward
+        projector's volume input (16-bit shadow of z); b may be float32,
+        float16 or bfloat16 (its storage type is taken from the tensor)."""
+        bt = _storage_of(b, self.proj_shape(-1), "b")
         prm = L.CbctSolverParams(int(iterations), float(beta), float(gamma), int(nonneg), int(use_graph),
-                                 int(storage), int(refine_every))
+                                 int(storage), int(refine_every), bt)
         L.call("cbct_osmom_solve", self._h, _ptr(b), _ptr(x0), _ptr(z_out), C.byref(prm), _ptr(resid),
                _stream(stream))
         return z_out
@@ -323,7 +351,7 @@ class Plan:
     def ossart(self, b, x_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
                cost=None, stream=None):
         prm = L.CbctSolverParams(int(iterations), float(beta), float(gamma), int(nonneg), int(use_graph),
-                                 L.CBCT_F32, 0)
+                                 L.CBCT_F32, 0, L.CBCT_F32)
         L.call("cbct_ossart_solve", self._h, _ptr(b), _ptr(x0), _ptr(x_out), C.byref(prm), _ptr(cost),
                _stream(stream))
         return x_out
@@ -360,7 +388,8 @@ def batch_osmom(jobs, n_streams=8, stream=None):
     for i, j in enumerate(jobs):
         prm = L.CbctSolverParams(int(j.get("iterations", 10)), float(j.get("beta", 1.0)), float(j.get("gamma", 0.0)),
                                  int(j.get("nonneg", False)), 1, int(j.get("storage", L.CBCT_F32)),
-                                 int(j.get("refine_every", 0)))
+                                 int(j.get("refine_every", 0)),
+                                 _storage_of(j["b"], j["plan"].proj_shape(-1), "b"))
         items[i] = L.CbctBatchItem(j["plan"].handle.value, _ptr(j["b"]), _ptr(j.get("x0")), _ptr(j["z"]), prm,
                                    _ptr(j.get("resid")))
     L.call("cbct_batch_osmom", items, len(jobs), int(n_streams), _stream(stream))

@@ -197,6 +197,15 @@ CBCT_API cbct_status cbct_fdk_filter(cbct_plan* plan, int32_t s, const float* pr
 CBCT_API cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float* filter,
                      uint32_t flags, float* work, void* stream);
 
+/* cbct_fdk_filter and cbct_fdk for projections stored as proj_dtype
+ * (CBCT_F32, CBCT_F16 or CBCT_BF16); the filter computes in FP32 and writes
+ * FP32.  cbct_fdk_ex with a 16-bit proj needs work (or the plan buffer); with
+ * CBCT_F32 it behaves as cbct_fdk. */
+CBCT_API cbct_status cbct_fdk_filter_ex(cbct_plan* plan, int32_t s, cbct_dtype proj_dtype, const void* proj_in,
+                                        float* proj_out, const float* filter, uint32_t flags, void* stream);
+CBCT_API cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj, float* vol,
+                                 const float* filter, uint32_t flags, float* work, void* stream);
+
 /* ----------------------------------------------------------------------------
  * Voxel masks
  * Masks are uint8 arrays of nx*ny*nz voxels (1 = keep), the layout of the
@@ -283,15 +292,17 @@ typedef struct {
   int32_t use_graph;       /* capture one iteration in a CUDA graph and replay it */
   cbct_dtype storage;      /* storage type of the forward projector's volume input */
   int32_t refine_every;    /* mixed precision: FP32 forward every n iterations (0 = never) */
+  cbct_dtype proj_storage; /* storage type of the measured projections b (OS-MOM); the residual stays FP32 */
 } cbct_solver_params;
 
 /* osMOMSolverD<cuNDArray<float>>::solve without regularisers
  * (solvers/osMOMSolverD.h:82-196) on the plan's subsets.
- * b: measured projections (subset-contiguous), x0: initial image or NULL,
+ * b: measured projections (subset-contiguous) of type params->proj_storage,
+ * x0: initial image or NULL,
  * z_out: result (the momentum point z, as the reference returns).
  * resid_norm2_out: NULL or device array of iterations*n_subsets doubles that
  * receives ||A_s x - b_s||^2 of every subset step. */
-CBCT_API cbct_status cbct_osmom_solve(cbct_plan* plan, const float* b, const float* x0, float* z_out,
+CBCT_API cbct_status cbct_osmom_solve(cbct_plan* plan, const void* b, const float* x0, float* z_out,
                              const cbct_solver_params* params, double* resid_norm2_out,
                              void* stream);
 
@@ -307,7 +318,7 @@ CBCT_API cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const fl
 
 typedef struct {
   cbct_plan* plan;              /* the scan's geometry and subsets */
-  const float* b;               /* measured projections (subset-contiguous), device */
+  const void* b;                /* measured projections (subset-contiguous, type params.proj_storage), device */
   const float* x0;              /* initial image or NULL */
   float* z_out;                 /* result, device */
   cbct_solver_params params;    /* use_graph is forced on */
@@ -324,6 +335,82 @@ typedef struct {
  * finished (later work on `stream` is ordered after it).
  * No counterpart in the reference (its drivers reconstruct one scan per process). */
 CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Serving loop: continuous batching of FDK and OS-MOM reconstructions
+ *
+ * No counterpart in the reference (its drivers reconstruct one scan per
+ * process).  A server owns max_inflight request slots, each a host worker
+ * with its own CUDA stream, and a stream-ordered device memory pool.  A
+ * submitted request waits until a slot is idle and its device footprint
+ * (cbct_server_request_bytes) fits into what the admitted requests leave of
+ * the budget; the oldest waiting request that fits is admitted first, and a
+ * request passed over 8 times blocks younger ones until it fits.  An admitted
+ * request builds its plan (set-up rules of CBSubsetOperator::setup and
+ * hoCuConebeamProjectionOperator::setup), copies its projections host ->
+ * device into subset order, reconstructs, copies the volume device -> host
+ * and releases its memory.  Requests on different slots overlap on the GPU;
+ * no kernel of one request reads another's memory, so each result is bitwise
+ * identical to the same request served alone.
+ * ------------------------------------------------------------------------- */
+
+typedef struct cbct_server cbct_server;
+
+typedef struct {
+  size_t hbm_budget_bytes;   /* device memory the admitted requests may hold together */
+  int32_t max_inflight;      /* request slots (streams and host workers), >= 1 */
+  int32_t device;            /* CUDA device ordinal */
+} cbct_server_config;
+
+enum { CBCT_REQ_FDK = 0, CBCT_REQ_OSMOM = 1 };
+
+typedef struct {
+  int32_t kind;                /* CBCT_REQ_FDK or CBCT_REQ_OSMOM */
+  cbct_geometry geometry;
+  const float* angles_deg;     /* host, n_views, acquisition order (copied at submit) */
+  const float* offsets_xy;     /* host, 2*n_views, or NULL for zero offsets (copied at submit) */
+  int32_t n_views;
+  int32_t n_subsets;           /* OS-MOM: round-robin subsets of CBSubsetOperator::setup */
+  cbct_dtype storage;          /* device storage of the projections; OS-MOM also keeps its
+                                  forward-projector volume input in this type (FP32 master) */
+  const void* proj_host;       /* host, W*H*n_views values of type `storage`, acquisition order;
+                                  must stay valid until the request completes */
+  float* vol_host;             /* host, nx*ny*nz floats, written when the request completes */
+  cbct_solver_params params;   /* OS-MOM; storage and proj_storage are set from `storage` */
+  const float* filter;         /* FDK: host array of W+1 floats, or NULL for the default (copied) */
+  uint32_t fdk_flags;          /* FDK: CBCT_FDK_OFFSET / CBCT_FDK_PARKER in addition to the rules */
+  int32_t offset_correction;   /* -1: the reference's override rule (per subset for OS-MOM); 0 off; 1 on */
+} cbct_request;
+
+typedef struct {
+  cbct_status status;          /* the request's outcome */
+  int32_t slot;                /* slot that ran it */
+  double t_submit, t_admit, t_done;  /* seconds on the server's clock */
+  size_t bytes_reserved;       /* admission footprint */
+  size_t bytes_peak;           /* peak of the device buffers the request held */
+  char message[256];           /* error message when status != CBCT_OK */
+} cbct_request_info;
+
+CBCT_API cbct_status cbct_server_create(const cbct_server_config* cfg, cbct_server** server_out);
+
+/* Device bytes the request will hold while it runs (its admission footprint). */
+CBCT_API cbct_status cbct_server_request_bytes(const cbct_request* req, size_t* bytes_out);
+
+/* Queues a request; returns at once.  CBCT_ERR_BUDGET when its footprint
+ * exceeds the whole budget. */
+CBCT_API cbct_status cbct_server_submit(cbct_server* server, const cbct_request* req, uint64_t* ticket_out);
+
+/* Waits up to timeout_s seconds (< 0: no limit) for a request.  Returns
+ * CBCT_OK once it has completed (info->status is its outcome; the ticket is
+ * then released) and CBCT_ERR_TIMEOUT if it has not. */
+CBCT_API cbct_status cbct_server_wait(cbct_server* server, uint64_t ticket, double timeout_s,
+                                      cbct_request_info* info_out);
+
+/* Seconds on the server's clock (steady, zero at creation). */
+CBCT_API cbct_status cbct_server_now(cbct_server* server, double* t_out);
+
+/* Serves every queued request, then releases the slots and the pool. */
+CBCT_API cbct_status cbct_server_destroy(cbct_server* server);
 
 /* ----------------------------------------------------------------------------
  * Synthetic phantoms (seeded ellipsoids; used by the benchmarks and tests)

@@ -45,6 +45,17 @@ CBCT_API cbct_status cbct_plain_osmom_solve(const cbct_geometry* g, const float*
                                             float* z_out, int32_t iterations, int32_t non_negativity,
                                             double* resid_norm2);
 
+/* hoCuConebeamProjectionOperator::mult_MH with filtered back-projection
+ * (hoCuConebeamProjectionOperator.cpp:235-254 over conebeam_backwards_projection<true>,
+ * conebeam_projection.cu:1300-1649): HOST projections (W,H,P) in, HOST volume
+ * out, views_per_batch views per batch (the operator's default is 20), cuFFT
+ * for the row filter as in the reference (loaded on first use), no Parker
+ * weights (full-scan orbits only).  filter: W+1 floats or NULL (default).
+ * Angles are used as given (start them at 0 as the operator's setup does). */
+CBCT_API cbct_status cbct_plain_fdk(const cbct_geometry* g, const float* angles_deg, const float* offsets_xy,
+                                    int32_t n_views, const float* proj_host, float* vol_host, const float* filter,
+                                    int32_t offset_correction, int32_t views_per_batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,3 +103,70 @@ def test_missing_library_fails_loudly(gtb, monkeypatch, tmp_path):
     monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "libcbct.so"))
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         L.lib()
+
+
+_LAYOUT_PROBE = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "cbct.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m));
+#define S(T) printf(#T " %zu\n", sizeof(T));
+int main(void) {
+  S(cbct_geometry) S(cbct_solver_params) S(cbct_batch_item) S(cbct_server_config) S(cbct_request)
+  S(cbct_request_info)
+  F(cbct_solver_params, proj_storage) F(cbct_batch_item, params) F(cbct_batch_item, resid_norm2_out)
+  F(cbct_server_config, device) F(cbct_request, geometry) F(cbct_request, angles_deg)
+  F(cbct_request, proj_host) F(cbct_request, params) F(cbct_request, filter) F(cbct_request, offset_correction)
+  F(cbct_request_info, t_submit) F(cbct_request_info, bytes_peak) F(cbct_request_info, message)
+  return 0;
+}
+"""
+
+
+def test_struct_layouts_match_ctypes(gtb, tmp_path):
+    """Every struct the ABI passes has the same size and field offsets in C
+    (gcc on include/cbct.h) and in the ctypes binding."""
+    src = tmp_path / "probe.c"
+    src.write_text(_LAYOUT_PROBE)
+    exe = tmp_path / "probe"
+    cuda_inc = "/usr/local/cuda/include"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src), "-o",
+                    str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    L = gtb._lib
+    types = {"cbct_geometry": L.CbctGeometry, "cbct_solver_params": L.CbctSolverParams,
+             "cbct_batch_item": L.CbctBatchItem, "cbct_server_config": L.CbctServerConfig,
+             "cbct_request": L.CbctRequest, "cbct_request_info": L.CbctRequestInfo}
+    for key, val in got.items():
+        if "." in key:
+            t, m = key.split(".")
+            assert getattr(types[t], m).offset == int(val), key
+        else:
+            assert C.sizeof(types[key]) == int(val), key
+
+
+def test_server_request_validation(gtb):
+    """Host-side checks of the serving API: footprint estimate, rejected
+    requests (no device work is issued)."""
+    L = gtb._lib
+    g = L.CbctGeometry(1000.0, 1500.0, 300.0, 225.0, 256, 192, 128, 128, 128, 128.0, 128.0, 128.0, 1.5)
+    ang = np.arange(90, dtype=np.float32) * 4.0
+    proj = np.zeros((90, 192, 256), np.float32)
+    vol = np.zeros((128, 128, 128), np.float32)
+    fdk = gtb.Server.fdk_request(g, ang, None, proj, vol)
+    nb = gtb.Server.request_bytes(fdk)
+    # projections + volume + FDK tables, no FP32 copy for float storage
+    lower = 90 * 192 * 256 * 4 + 128 ** 3 * 4
+    assert lower < nb < lower * 1.05
+    mom = gtb.Server.osmom_request(g, ang, None, proj, vol, n_subsets=9)
+    nm = gtb.Server.request_bytes(mom)
+    assert nm > 2 * 90 * 192 * 256 * 4 + 4 * 128 ** 3 * 4
+    half = gtb.Server.fdk_request(g, ang, None, proj.astype(np.float16), vol)
+    assert gtb.Server.request_bytes(half) > nb  # 16-bit projections + an FP32 filtered copy
+    with pytest.raises(gtb.CbctError, match="n_subsets"):
+        gtb.Server.request_bytes(gtb.Server.osmom_request(g, ang, None, proj, vol, n_subsets=0))
+    with pytest.raises(ValueError):
+        gtb.Server.fdk_request(g, ang, None, proj[:10], vol)
+    with pytest.raises(TypeError):
+        gtb.Server.fdk_request(g, ang, None, proj, vol.astype(np.float16))

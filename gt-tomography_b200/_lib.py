@@ -21,6 +21,7 @@ CBCT_FDK_OFFSET = 0x4
 CBCT_FDK_RAMP = 0x8
 CBCT_OPT_DEBUG_CHECKS = 1
 CBCT_OPT_FORCE_GATHER = 2
+CBCT_OPT_FORWARD_KERNEL = 3
 
 # Every symbol the header declares (checked by the CPU tests).
 EXPORTED = [

@@ -261,7 +261,7 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   p->pool_stream = pool_stream;
   p->d_views = plan_alloc_n<ViewParams>(p.get(), n_views);
   plan_upload(p.get(), p->d_views, p->hviews.data(), sizeof(ViewParams) * n_views);
-  const size_t tiles = (size_t)((g->width + kTU - 1) / kTU) * ((g->height + kTV - 1) / kTV);
+  const size_t tiles = forward_tiles(g->width, g->height);
   p->n_partials = std::max<size_t>(tiles * n_views, 148 * 4);
   p->d_partials = plan_alloc_n<double>(p.get(), p->n_partials);
   p->d_flags = plan_alloc_n<int>(p.get(), 4);
@@ -386,7 +386,7 @@ cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_ou
 
 const char* cbct_plan_forward_variant(const cbct_plan* plan) {
   if (!plan) return "";
-  return plan->fwd_variant == 1 ? "tma-slab" : "gather";
+  return plan->fwd_variant == 2 ? "tma-fan" : plan->fwd_variant == 1 ? "tma-slab" : "gather";
 }
 
 cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value) {
@@ -394,8 +394,13 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
     CBCT_REQUIRE(plan, "plan is NULL");
     if (option == CBCT_OPT_DEBUG_CHECKS) {
       plan->debug_checks = value != 0;
-    } else if (option == CBCT_OPT_FORCE_GATHER) {
-      plan->force_gather = value != 0;
+    } else if (option == CBCT_OPT_FORCE_GATHER || option == CBCT_OPT_FORWARD_KERNEL) {
+      if (option == CBCT_OPT_FORCE_GATHER) plan->force_gather = value != 0;
+      else {
+        CBCT_REQUIRE(value >= 0 && value <= 3, "forward kernel must be 0 (automatic), 1 (slab), 2 (gather) or 3 (fan)");
+        plan->fwd_pref = value;
+      }
+      graph_cache_free(plan);
       forward_choose_variant(plan);
       forward_prepare(plan);
       backproject_choose_variant(plan);

@@ -148,6 +148,21 @@ constexpr int kMaxSlabs = 260;
 constexpr int kSmemBudget = 200 * 1024;
 // Box widths (memory x) the slab kernel is compiled for; each is 8 mod 16.
 constexpr int kBoxWidths[] = {40, 56, 72, 104, 136};
+// Fan forward projector: kFU detector columns (one per warp) x kFV rows per
+// CTA; the column's samples are interpolated in e and d kFKC at a time.
+constexpr int kFU = 8;
+constexpr int kFV = 32;
+constexpr int kFKC = 16;
+constexpr int kFanWidths[] = {24, 40, 56, 72};
+
+// Forward-projector blocks per view: the larger of the slab and fan tilings
+// (one FP64 partial sum per block).
+inline size_t forward_tiles(int W, int H) {
+  const size_t slab = (size_t)((W + kTU - 1) / kTU) * ((H + kTV - 1) / kTV);
+  const size_t fan = (size_t)((W + kFU - 1) / kFU) * ((H + kFV - 1) / kFV);
+  return std::max(slab, fan);
+}
+
 
 }  // namespace cbct
 
@@ -163,8 +178,12 @@ struct cbct_plan {
   int device = 0;
   int max_subset = 0;
 
-  // forward variant: 0 = gather (global loads), 1 = TMA slab
+  // forward variant: 0 = gather (global loads), 1 = TMA slab, 2 = TMA fan
   int fwd_variant = 0;
+  int fwd_pref = 0;         // CBCT_OPT_FORWARD_KERNEL: 0 automatic, 1 slab, 2 gather, 3 fan
+  cbct::SlabBox fan{};      // fan kernel box for fp32 storage
+  cbct::SlabBox fan16{};    // fan kernel box for 16-bit storage
+  int fan_lz = 0;           // line length (planes) of the fan kernel, odd
   cbct::SlabBox slab{};     // box in the view frame for fp32 storage (x starts aligned to 4)
   cbct::SlabBox slab16{};   // box for 16-bit storage (x starts aligned to 8)
   size_t slab_smem = 0;     // dynamic shared memory of the fp32 slab kernel (bytes)

@@ -209,41 +209,47 @@ struct SlabSample {
   }
 };
 
-// Samples of one ray inside one slab, two per iteration (independent chains
-// for the scheduler).  (ce, cd, cz) are frame texel coordinates; samples are
-// consumed while floor(cd) stays inside the slab, in ray order.
+// Samples of one ray inside one slab.  The number of samples the slab holds
+// is found first (the first k whose d coordinate leaves the slab; d is
+// monotone along the ray), then they are taken in a counted loop, kFwdUnroll
+// independent evaluations per iteration, added to acc in ray order.
+// (ce, cd, cz) are frame texel coordinates.
+constexpr int kFwdUnroll = 2;
+
 template <class V, int BX, int SGN, bool CHECK>
 __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
                                              float cz0, float dce, float dcd, float dcz, float lo, float hi,
                                              float orgf, unsigned maxidx, float& acc, int& bad) {
   using SS = SlabSample<V, BX>;
   const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
-  auto outside = [&](float fd) { return SGN > 0 ? (fd >= hi) : (fd < lo); };
-  while (kf + 1.f < Nf) {
-    const float2 pa = __ffma2_rn(make_float2(kf, kf), dc, c0);
-    const float2 pb = __ffma2_rn(make_float2(kf + 1.f, kf + 1.f), dc, c0);
-    const float fda = floorf(pa.y), fdb = floorf(pb.y);
-    if (outside(fda)) return;
-    const float cza = fmaf(kf, dcz, cz0), czb = fmaf(kf + 1.f, dcz, cz0);
-    const float va = SS::eval(s, pa, cza, floorf(pa.x), fda, floorf(cza), orgf, maxidx, bad, CHECK);
-    if (outside(fdb)) {
-      acc += va;
-      kf += 1.f;
-      return;
+  // floor(x) >= hi <=> x >= hi and floor(x) < lo <=> x < lo, lo and hi being integers.
+  auto out_at = [&](float k) {
+    const float x = fmaf(k, dcd, cd0);
+    return SGN > 0 ? (x >= hi) : (x < lo);
+  };
+  float ke = ceilf(((SGN > 0 ? hi : lo) - cd0) / dcd);
+  ke = fminf(fmaxf(ke, kf), Nf);
+  while (ke > kf && out_at(ke - 1.f)) ke -= 1.f;
+  while (ke < Nf && !out_at(ke)) ke += 1.f;
+  float k = kf;
+  for (; k + float(kFwdUnroll - 1) < ke; k += float(kFwdUnroll)) {
+    float v[kFwdUnroll];
+#pragma unroll
+    for (int q = 0; q < kFwdUnroll; ++q) {
+      const float kq = k + float(q);
+      const float2 pq = __ffma2_rn(make_float2(kq, kq), dc, c0);
+      const float czq = fmaf(kq, dcz, cz0);
+      v[q] = SS::eval(s, pq, czq, floorf(pq.x), floorf(pq.y), floorf(czq), orgf, maxidx, bad, CHECK);
     }
-    const float vb = SS::eval(s, pb, czb, floorf(pb.x), fdb, floorf(czb), orgf, maxidx, bad, CHECK);
-    acc += va;
-    acc += vb;
-    kf += 2.f;
+#pragma unroll
+    for (int q = 0; q < kFwdUnroll; ++q) acc += v[q];
   }
-  if (kf < Nf) {
-    const float2 pa = __ffma2_rn(make_float2(kf, kf), dc, c0);
-    const float fda = floorf(pa.y);
-    if (outside(fda)) return;
-    const float cza = fmaf(kf, dcz, cz0);
-    acc += SS::eval(s, pa, cza, floorf(pa.x), fda, floorf(cza), orgf, maxidx, bad, CHECK);
-    kf += 1.f;
+  for (; k < ke; k += 1.f) {
+    const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
+    const float czq = fmaf(k, dcz, cz0);
+    acc += SS::eval(s, pq, czq, floorf(pq.x), floorf(pq.y), floorf(czq), orgf, maxidx, bad, CHECK);
   }
+  kf = ke;
 }
 
 template <class V, int BX, bool CHECK>
@@ -308,6 +314,7 @@ __global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant_
   }
   __syncthreads();
   const int ue = min(u0 + kTU, gc.W) - 1, ve = min(v0 + kTV, gc.H) - 1;
+  const int ne = dom ? gc.nx : gc.ny;  // volume extent along e
   for (int q = tid; q < nslab * 8; q += blockDim.x) {
     const int i = q >> 3, c = q & 7;
     const int m = mlo + i;
@@ -321,12 +328,14 @@ __global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant_
     float ce = fmaf(fmaf(t, de, Se), ke, be);
     float cz = fmaf(t * dz, gc.kz, gc.bz);
     // Clamp before the int conversion so that far-away planes stay finite.
-    ce = fminf(fmaxf(ce, -1.0e5f), 1.0e5f);
-    cz = fminf(fmaxf(cz, -1.0e5f), 1.0e5f);
-    atomicMin(&sh.emin[i], int(floorf(ce)));
-    atomicMax(&sh.emax[i], int(floorf(ce)));
-    atomicMin(&sh.zmin[i], int(floorf(cz)));
-    atomicMax(&sh.zmax[i], int(floorf(cz)));
+    // Samples lie inside the volume (texel floors in [-1, n-1]; outside it the
+    // border reads 0), so the box only has to cover the footprint's part in it.
+    const int fe = min(max(int(floorf(fminf(fmaxf(ce, -1.0e5f), 1.0e5f))), -1), ne - 1);
+    const int fz = min(max(int(floorf(fminf(fmaxf(cz, -1.0e5f), 1.0e5f))), -1), gc.nz - 1);
+    atomicMin(&sh.emin[i], fe);
+    atomicMax(&sh.emax[i], fe);
+    atomicMin(&sh.zmin[i], fz);
+    atomicMax(&sh.zmax[i], fz);
   }
   __syncthreads();
 
@@ -407,6 +416,291 @@ __global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant_
   fwd_epilogue(o, gc, vp, p, u, v, active, val, sh.red, tid);
 }
 
+// ------------------------------------------------------------------ fan
+// The rays of one detector column lie in one vertical plane (the detector's
+// v axis is the world z axis).  A ray that enters and leaves the volume
+// through its side faces has the clip (a1, a2) of the column's in-plane path,
+// so its k-th sample sits at the column's k-th in-plane position (e_k, d_k);
+// only z differs between the rows.  The fan kernel gives each warp one column
+// of a kFU x kFV tile (lane = detector row).  Per slab, the warp first
+// interpolates the column's samples in e and d on every z plane its rays
+// reach ("lines", one value per sample and plane), then every ray takes its
+// samples as linear interpolations in z between two line entries.  This is
+// the slab kernel's trilinear tree (e, then d, then z) with the e/d part
+// shared by the column's rays, so results are bitwise those of the per-ray
+// kernels.  Rays clipped by the top or bottom face (their own a1/a2) take the
+// per-ray trilinear path on the same box.
+struct FanShared {
+  uint64_t bars[kNStage];
+  int mlo, mhi, abort_flag;
+  double red[8];
+  float tile[kFV][kFU + 1];  // results, transposed for a coalesced epilogue
+};
+
+// The column's samples inside one slab, in chunks of kFKC (warp-level; every
+// lane of the warp calls it).  kcol: the column's next sample (warp-uniform).
+template <class V, int BX, int SGN, bool CHECK>
+__device__ __forceinline__ void fan_slab(const V* __restrict__ s, float* __restrict__ lines, int LZ, int BZ,
+                                         int lane, int N, int& kcol, float2 c0, float2 dc, bool shared, float c0z,
+                                         float dcz, float lo, float hi, int oz, float orgf, float& acc, int& bad) {
+  constexpr int BXY = BX * kBoxY;
+  constexpr unsigned FULL = 0xffffffffu;
+  const unsigned maxidx = unsigned(BXY * BZ - BX - 2);
+  auto outside = [&](float fd) { return SGN > 0 ? (fd >= hi) : (fd < lo); };
+  for (;;) {
+    if (kcol >= N) return;
+    // Samples of the chunk still inside the slab (a prefix, floor(d) being
+    // monotone along the ray).
+    bool in = false;
+    if (lane < kFKC && kcol + lane < N) {
+      const float kj = float(kcol + lane);
+      in = !outside(floorf(fmaf(kj, dc.y, c0.y)));
+    }
+    const int nk = __ffs(~__ballot_sync(FULL, in)) - 1;
+    if (nk <= 0) return;
+    // z planes the shared rays reach over the chunk.
+    int zl = INT_MAX, zh = INT_MIN;
+    if (shared) {
+      const int fa = int(floorf(fmaf(float(kcol), dcz, c0z)));
+      const int fb = int(floorf(fmaf(float(kcol + nk - 1), dcz, c0z)));
+      zl = min(fa, fb);
+      zh = max(fa, fb);
+    }
+    zl = __reduce_min_sync(FULL, zl);
+    zh = __reduce_max_sync(FULL, zh);
+    int nz = zh - zl + 2;
+    if (CHECK && (nz > LZ || zl < oz || zh + 1 >= oz + BZ)) bad = 1;
+    nz = min(nz, LZ);
+    // Lines: lane (j, g) interpolates sample j on planes g, g + G, ...
+    const int G = 32 / nk;
+    const int j = lane % nk, g = lane / nk;
+    if (g < G) {
+      const float kfj = float(kcol + j);
+      const float2 pa = __ffma2_rn(make_float2(kfj, kfj), dc, c0);
+      const float fe = floorf(pa.x), fd = floorf(pa.y);
+      const float2 aed = __fadd2_rn(pa, make_float2(-fe, -fd));
+      const float2 te = make_float2(aed.x, aed.x);
+      const float td = aed.y;
+      int idx = int(fmaf(float(zl + g), float(BXY), fmaf(fd, float(BX), fe)) - orgf);
+      float* L = lines + j * LZ;
+      for (int z = g; z < nz; z += G, idx += G * BXY) {
+        if (CHECK) bad |= (unsigned)idx > maxidx;
+        const V* q = s + min((unsigned)idx, maxidx);
+        const float2 a0 = make_float2(sm_f(q[0]), sm_f(q[BX]));
+        const float2 b0 = make_float2(sm_f(q[1]), sm_f(q[BX + 1]));
+        const float2 e = lerp2(a0, b0, te);  // (d0, d1) rows on plane z
+        L[z] = fmaf(td, e.y, fmaf(-td, e.x, e.x));
+      }
+    }
+    __syncwarp();
+    if (shared) {
+      const float* L = lines;
+      for (int jj = 0; jj < nk; ++jj, L += LZ) {
+        const float cz = fmaf(float(kcol + jj), dcz, c0z);
+        const float fz = floorf(cz);
+        const float az = cz - fz;
+        int iz = int(fz) - zl;
+        if (CHECK) bad |= (unsigned)iz > (unsigned)(nz - 2);
+        iz = min(max(iz, 0), nz - 2);
+        acc += fmaf(az, L[iz + 1] - L[iz], L[iz]);
+      }
+    }
+    kcol += nk;
+    __syncwarp();
+    if (nk < kFKC) return;
+  }
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(256, 3) fwd_fan_kernel(const __grid_constant__ CUtensorMap map_v,
+                                                      const __grid_constant__ CUtensorMap map_t,
+                                                      const V* __restrict__ vol,
+                                                      const ViewParams* __restrict__ views, GridConst gc,
+                                                      int BZ, int LZ, int nsl_max, FwdOut o, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ FanShared sh;
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  constexpr int BXY = BX * kBoxY;
+  const ViewParams vp = views[blockIdx.z];
+  const int dom = vp.dom;
+  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p = blockIdx.z;
+  const int u0 = blockIdx.x * kFU, v0 = blockIdx.y * kFV;
+  const int u = u0 + warp, v = v0 + lane;
+  const bool active = (u < gc.W) && (v < gc.H);
+  const int uc = min(u, gc.W - 1);
+  const Ray r = make_ray(vp, gc, uc, min(v, gc.H - 1));
+  const bool hit = active && (r.a2 > r.a1);
+  // The column's in-plane clip: make_ray's without the z faces.
+  const float dx = fmaf(float(uc), vp.Eux, vp.D0x);
+  const float dy = fmaf(float(uc), vp.Euy, vp.D0y);
+  const float tx1 = __fdiv_rn(gc.hx - vp.Sx, dx), tx2 = __fdiv_rn(-gc.hx - vp.Sx, dx);
+  const float ty1 = __fdiv_rn(gc.hy - vp.Sy, dy), ty2 = __fdiv_rn(-gc.hy - vp.Sy, dy);
+  const float a1c = fmaxf(fmaxf(fminf(tx1, tx2), fminf(ty1, ty2)), 0.f);
+  const float a2c = fminf(fminf(fmaxf(tx1, tx2), fmaxf(ty1, ty2)), 1.f);
+  const bool shared = hit && r.a1 == a1c && r.a2 == a2c;
+  const bool own = hit && !shared;
+  const bool any_shared = __any_sync(0xffffffffu, shared);
+  // Frame coordinates (e = cross axis, d = slab axis) of this lane's ray; for
+  // shared rays they are the column's.
+  const float ce0 = dom ? r.c0x : r.c0y, dce = dom ? r.dcx : r.dcy;
+  const float cd0 = dom ? r.c0y : r.c0x, dcd = dom ? r.dcy : r.dcx;
+  // The column's frame coordinates, from the first shared lane.
+  const int src = any_shared ? __ffs(__ballot_sync(0xffffffffu, shared)) - 1 : 0;
+  const float2 cc0 = make_float2(__shfl_sync(0xffffffffu, ce0, src), __shfl_sync(0xffffffffu, cd0, src));
+  const float2 cdc = make_float2(__shfl_sync(0xffffffffu, dce, src), __shfl_sync(0xffffffffu, dcd, src));
+
+  if (tid == 0) {
+    sh.mlo = INT_MAX;
+    sh.mhi = INT_MIN;
+    sh.abort_flag = 0;
+    for (int s = 0; s < kNStage; ++s) mbar_init(&sh.bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (hit) {
+    const int f0 = int(floorf(cd0));
+    const int f1 = int(floorf(fmaf(float(gc.N - 1), dcd, cd0)));
+    const int m0 = (max(f0, kSlabBase) - kSlabBase) / kTS;
+    const int m1 = (max(f1, kSlabBase) - kSlabBase) / kTS;
+    atomicMin(&sh.mlo, min(m0, m1));
+    atomicMax(&sh.mhi, max(m0, m1));
+  }
+  __syncthreads();
+  const int mlo = sh.mlo, mhi = sh.mhi;
+  int nslab = (mhi >= mlo) ? (mhi - mlo + 1) : 0;
+  if (nslab > nsl_max) {
+    if (tid == 0) atomicAdd(&flags[0], 1);
+    nslab = 0;
+  }
+  // Per-slab footprints (e min, e max, z min, z max) live after the lines.
+  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
+  int* foot = reinterpret_cast<int*>(smem_raw + kNStage * stage_stride + (size_t)kFU * kFKC * LZ * sizeof(float));
+  const float ke = dom ? gc.kx : gc.ky, be = dom ? gc.bx : gc.by;
+  const float kd = dom ? gc.ky : gc.kx, bd = dom ? gc.by : gc.bx;
+  const float Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
+  for (int i = tid; i < nslab; i += blockDim.x) {
+    foot[i] = INT_MAX; foot[nsl_max + i] = INT_MIN;
+    foot[2 * nsl_max + i] = INT_MAX; foot[3 * nsl_max + i] = INT_MIN;
+  }
+  __syncthreads();
+  // Footprint of every slab: the four corner rays of the tile at the slab's
+  // two bounding planes.
+  const int ue = min(u0 + kFU, gc.W) - 1, ve = min(v0 + kFV, gc.H) - 1;
+  const int ne = dom ? gc.nx : gc.ny;  // volume extent along e
+  for (int q = tid; q < nslab * 8; q += blockDim.x) {
+    const int i = q >> 3, c = q & 7;
+    const int m = mlo + i;
+    const float plane = float(kSlabBase + m * kTS + ((c & 4) ? kTS : 0));
+    const int ucc = (c & 1) ? ue : u0, vcc = (c & 2) ? ve : v0;
+    const float ddx = fmaf(float(ucc), vp.Eux, vp.D0x);
+    const float ddy = fmaf(float(ucc), vp.Euy, vp.D0y);
+    const float ddz = fmaf(float(vcc), vp.Evz, vp.D0z);
+    const float de = dom ? ddx : ddy, dd = dom ? ddy : ddx;
+    const float t = ((plane - bd) / kd - Sd) / dd;
+    float ce = fmaf(fmaf(t, de, Se), ke, be);
+    float cz = fmaf(t * ddz, gc.kz, gc.bz);
+    // Samples lie inside the volume (texel floors in [-1, n-1]; outside it the
+    // border reads 0), so the box only has to cover the footprint's part in it.
+    const int fe = min(max(int(floorf(fminf(fmaxf(ce, -1.0e5f), 1.0e5f))), -1), ne - 1);
+    const int fz = min(max(int(floorf(fminf(fmaxf(cz, -1.0e5f), 1.0e5f))), -1), gc.nz - 1);
+    atomicMin(&foot[i], fe);
+    atomicMax(&foot[nsl_max + i], fe);
+    atomicMin(&foot[2 * nsl_max + i], fz);
+    atomicMax(&foot[3 * nsl_max + i], fz);
+  }
+  __syncthreads();
+
+  const unsigned maxidx = unsigned(BXY * (BZ - 1) - BX - 2);
+  float* lines = reinterpret_cast<float*>(smem_raw + kNStage * stage_stride) + warp * (kFKC * LZ);
+  auto origin = [&](int i, int& oe, int& od, int& oz, int& m) {
+    m = (vp.dsgn > 0) ? mlo + i : mhi - i;
+    const int ii = m - mlo;
+    oe = (foot[ii] - 1) & ~(int(16 / sizeof(V)) - 1);
+    od = kSlabBase + m * kTS;
+    oz = foot[2 * nsl_max + ii] - 1;
+  };
+  auto issue = [&](int i) {
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    uint64_t* bar = &sh.bars[i % kNStage];
+    mbar_arrive_expect_tx(bar, box_bytes);
+    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, oe, od, oz, bar);
+  };
+  if (tid == 0) {
+    for (int i = 0; i < min(kNStage, nslab); ++i) issue(i);
+  }
+
+  float acc = 0.f;
+  float kf = 0.f;   // own rays: next sample
+  int kcol = 0;     // the column's next sample
+  const float Nf = float(gc.N);
+  int bad = 0;
+  int done = 0;
+  for (int i = 0; i < nslab; ++i) {
+    const int slot = i % kNStage;
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
+      break;
+    }
+    done = i + 1;
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    if (CHECK && tid == 0) {
+      const int ii = m - mlo;
+      if (foot[nsl_max + ii] + 2 - oe >= BX || foot[3 * nsl_max + ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
+    }
+    const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
+    const float lo = float(od), hi = lo + float(kTS);
+    const float orgf = float(oe + od * BX + oz * BXY);
+    if (any_shared) {
+      if (vp.dsgn > 0)
+        fan_slab<V, BX, 1, CHECK>(s, lines, LZ, BZ, lane, gc.N, kcol, cc0, cdc, shared, r.c0z, r.dcz, lo, hi, oz,
+                                  orgf, acc, bad);
+      else
+        fan_slab<V, BX, -1, CHECK>(s, lines, LZ, BZ, lane, gc.N, kcol, cc0, cdc, shared, r.c0z, r.dcz, lo, hi, oz,
+                                   orgf, acc, bad);
+    }
+    if (own) {
+      if (vp.dsgn > 0)
+        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+      else
+        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+    }
+    __syncthreads();
+    if (tid == 0 && i + kNStage < nslab) {
+      fence_proxy_async();
+      issue(i + kNStage);
+    }
+  }
+  if (sh.abort_flag && tid == 0) {
+    for (int i = done; i < min(done + kNStage, nslab); ++i)
+      (void)mbar_wait_bounded(&sh.bars[i % kNStage], (i / kNStage) & 1, kWaitLimit);
+  }
+  if (CHECK && !sh.abort_flag) {
+    if ((shared && kcol != gc.N) || (own && kf != Nf)) bad = 1;  // every sample of a hit ray is consumed
+    if (bad) atomicAdd(&flags[0], 1);
+  }
+
+  float val = 0.f;
+  if (hit) {
+    val = acc * r.delta;
+  } else if (active) {
+    int k0, k1;
+    if (grown_range(vp, gc, u, v, r, k0, k1)) val = march_global(vol, gc, r, k0, k1) * r.delta;
+  }
+  // Transpose through shared memory so that the epilogue's accesses run along u.
+  sh.tile[lane][warp] = val;
+  __syncthreads();
+  const int tu = tid % kFU, tv = tid / kFU;
+  const int eu = u0 + tu, ev = v0 + tv;
+  fwd_epilogue(o, gc, vp, p, eu, ev, eu < gc.W && ev < gc.H, sh.tile[tv][tu], sh.red, tid);
+}
+
 // ------------------------------------------------------------------ host
 CUtensorMapDataType tma_dtype(cbct_dtype dt) {
   switch (dt) {
@@ -430,6 +724,18 @@ CUtensorMap make_map(cbct_dtype dt, const void* vol, int n0, int n1, int n2, con
   if (res != CUDA_SUCCESS)
     throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)res));
   return m;
+}
+
+// Dynamic shared memory of a slab or fan launch: kNStage TMA stages of the
+// box (128-byte aligned) + the fan kernel's lines + alignment slack.
+static size_t forward_smem(const SlabBox& b, size_t es, int lz, int nsl = 0) {
+  return kNStage * ((b.bx * b.by * b.bz * es + 127) & ~size_t(127)) + (size_t)kFU * kFKC * lz * sizeof(float) +
+         4 * sizeof(int) * (size_t)nsl + 128;
+}
+
+// Slabs a ray can cross in the larger in-plane direction.
+static int slabs_max(const cbct_geometry& g) {
+  return (std::max(g.nx, g.ny) + 1 - kSlabBase + kTS - 1) / kTS + 1;
 }
 
 template <class V>
@@ -456,6 +762,31 @@ void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim
 }
 
 template <class V>
+const SlabBox& fan_box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->fan : p->fan16; }
+
+template <class V, int BX>
+void launch_fan(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, int first, int cnt, cudaStream_t st,
+                cbct_dtype dt) {
+  const SlabBox& b = fan_box_for<V>(p);
+  const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
+  const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
+                                  volT ? p->g.nx : p->g.ny, p->g.nz, b);
+  const int nsl = slabs_max(p->g);
+  const size_t smem = forward_smem(b, sizeof(V), p->fan_lz, nsl);
+  const dim3 grid((p->g.width + kFU - 1) / kFU, (p->g.height + kFV - 1) / kFV, cnt);
+  if (p->debug_checks) {
+    auto k = fwd_fan_kernel<V, BX, true>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kFU * 32, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, p->fan_lz, nsl, o, p->d_flags);
+  } else {
+    auto k = fwd_fan_kernel<V, BX, false>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kFU * 32, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, p->fan_lz, nsl, o, p->d_flags);
+  }
+  check_launch("fwd_fan_kernel");
+}
+
+template <class V>
 void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaStream_t st, cbct_dtype dt,
                   bool use_slab) {
   const V* vol = static_cast<const V*>(vol_v);
@@ -474,6 +805,16 @@ void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaS
     check_launch("transpose_xy_kernel");
     volT = t;
   }
+  if (p->fwd_variant == 2) {
+    switch (fan_box_for<V>(p).bx) {
+      case 24: launch_fan<V, 24>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 40: launch_fan<V, 40>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 56: launch_fan<V, 56>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 72: launch_fan<V, 72>(p, vol, volT, o, first, cnt, st, dt); break;
+      default: throw Error(CBCT_ERR_INTERNAL, "unsupported fan box width");
+    }
+    return;
+  }
   switch (box_for<V>(p).bx) {
     case 40: launch_slab<V, 40>(p, vol, volT, o, grid, first, st, dt); break;
     case 56: launch_slab<V, 56>(p, vol, volT, o, grid, first, st, dt); break;
@@ -490,10 +831,27 @@ void prepare_width(size_t smem) {
   ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, true>, smem);
 }
 
+template <class V, int BX>
+void prepare_fan_width(size_t smem) {
+  ensure_smem_attr((const void*)fwd_fan_kernel<V, BX, false>, smem);
+  ensure_smem_attr((const void*)fwd_fan_kernel<V, BX, true>, smem);
+}
+
 template <class V>
 void prepare_typed(const cbct_plan* p) {
+  if (p->fwd_variant == 2) {
+    const SlabBox& f = fan_box_for<V>(p);
+    const size_t fs = forward_smem(f, sizeof(V), p->fan_lz, slabs_max(p->g));
+    switch (f.bx) {
+      case 24: prepare_fan_width<V, 24>(fs); break;
+      case 40: prepare_fan_width<V, 40>(fs); break;
+      case 56: prepare_fan_width<V, 56>(fs); break;
+      case 72: prepare_fan_width<V, 72>(fs); break;
+      default: break;
+    }
+  }
   const SlabBox& b = box_for<V>(p);
-  const size_t smem = kNStage * ((b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127)) + 128;
+  const size_t smem = forward_smem(b, sizeof(V), 0);
   switch (b.bx) {
     case 40: prepare_width<V, 40>(smem); break;
     case 56: prepare_width<V, 56>(smem); break;
@@ -506,22 +864,15 @@ void prepare_typed(const cbct_plan* p) {
 
 }  // namespace
 
-// Chooses the slab variant and its TMA box from the plan geometry: for every
-// view and tile, the footprint of every slab (corner-ray bounding box in the
-// view's frame, computed in FP64) sets the largest box extent, plus margins.
-void forward_choose_variant(cbct_plan* p) {
+// Largest footprint of one slab over every view and tile of a TU x TV tiling
+// (corner-ray bounding box in the view's frame, computed in FP64): e extent
+// and z extent in elements, including margins.  False when some view cannot
+// use slabs (a ray not dominated by its view's slab axis, or too many slabs).
+static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ext_z) {
   const cbct_geometry& g = p->g;
-  p->fwd_variant = 0;
-  p->slab = SlabBox{0, 0, 0, 0};
-  p->subset_has_xdom.assign(p->n_subsets + 1, 0);
-  for (int s = 0; s <= p->n_subsets; ++s)
-    for (int i = p->first[s]; i < p->first[s] + p->count[s]; ++i)
-      if (p->hviews[i].dom == 0) p->subset_has_xdom[s] = 1;
-  if (p->force_gather) return;
   const double kx = g.nx / (double)g.lx, ky = g.ny / (double)g.ly, kz = g.nz / (double)g.lz;
   const double bx = g.nx / 2.0 - 0.5, by = g.ny / 2.0 - 0.5, bz = g.nz / 2.0 - 0.5;
-  const int tiles_u = (g.width + kTU - 1) / kTU, tiles_v = (g.height + kTV - 1) / kTV;
-  // Per thread: largest e extent, largest z extent, and whether every view fits.
+  const int tiles_u = (g.width + TU - 1) / TU, tiles_v = (g.height + TV - 1) / TV;
   struct Acc { int e = 0, z = 0, ok = 1; };
   std::vector<Acc> acc(host_threads());
   // The in-plane coordinate of a ray does not depend on the detector row, so the
@@ -539,12 +890,12 @@ void forward_choose_variant(cbct_plan* p) {
       const int nsl = (Nd + 1 - kSlabBase + kTS - 1) / kTS + 1;
       if (nsl > kMaxSlabs) { a.ok = 0; break; }
       for (int tv = 0; tv < tiles_v; ++tv) {
-        const int v0 = tv * kTV, ve = std::min(v0 + kTV, g.height) - 1;
+        const int v0 = tv * TV, ve = std::min(v0 + TV, g.height) - 1;
         dz0[tv] = vp.D0z + v0 * (double)vp.Evz;
         dz1[tv] = vp.D0z + ve * (double)vp.Evz;
       }
       for (int tu = 0; tu < tiles_u && a.ok; ++tu) {
-        const int uc[2] = {tu * kTU, std::min(tu * kTU + kTU, g.width) - 1};
+        const int uc[2] = {tu * TU, std::min(tu * TU + TU, g.width) - 1};
         double de[2], dd[2];
         for (int c = 0; c < 2; ++c) {
           const double dx = vp.D0x + uc[c] * (double)vp.Eux, dy = vp.D0y + uc[c] * (double)vp.Euy;
@@ -563,8 +914,10 @@ void forward_choose_variant(cbct_plan* p) {
             emn = std::min(emn, ce); emx = std::max(emx, ce);
             tmn = std::min(tmn, t); tmx = std::max(tmx, t);
           }
-          // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin
-          a.e = std::max(a.e, (int)(std::floor(emx) - std::floor(emn)) + 3 + 2);
+          // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin; the
+          // kernels clamp footprints to the volume, whose extent bounds the box
+          const int Ne = dom ? g.nx : g.ny;
+          a.e = std::max(a.e, std::min((int)(std::floor(emx) - std::floor(emn)) + 3 + 2, Ne + 4));
           for (int tv = 0; tv < tiles_v; ++tv) {
             const double z00 = tmn * dz0[tv], z01 = tmn * dz1[tv], z10 = tmx * dz0[tv], z11 = tmx * dz1[tv];
             const double zmn = std::min(std::min(z00, z01), std::min(z10, z11)) * kz + bz;
@@ -576,38 +929,66 @@ void forward_choose_variant(cbct_plan* p) {
       }
     }
   });
-  int ext_e = 0, ext_z = 0;
+  ext_e = ext_z = 0;
   bool ok = true;
   for (const Acc& a : acc) {
     ext_e = std::max(ext_e, a.e);
     ext_z = std::max(ext_z, a.z);
     ok = ok && a.ok;
   }
-  if (!ok) return;
+  return ok;
+}
+
+// Chooses the forward variant and its TMA boxes from the plan geometry: the
+// per-ray slab kernel where its boxes fit, else the gather kernel; the fan
+// kernel on request (CBCT_OPT_FORWARD_KERNEL = 3).
+void forward_choose_variant(cbct_plan* p) {
+  p->fwd_variant = 0;
+  p->slab = SlabBox{0, 0, 0, 0};
+  p->fan = SlabBox{0, 0, 0, 0};
+  p->subset_has_xdom.assign(p->n_subsets + 1, 0);
+  for (int s = 0; s <= p->n_subsets; ++s)
+    for (int i = p->first[s]; i < p->first[s] + p->count[s]; ++i)
+      if (p->hviews[i].dom == 0) p->subset_has_xdom[s] = 1;
+  if (p->force_gather || p->fwd_pref == 2) return;
   // The x start of a box is rounded down to a 16-byte boundary (4 fp32 or 8
   // 16-bit elements), which widens the box by up to 3 or 7 elements.
-  auto width = [&](int slack) {
-    for (int w : kBoxWidths)
-      if (w >= ext_e + slack) return w;
+  auto width = [](const auto& list, int ext, int slack) {
+    for (int w : list)
+      if (w >= ext + slack) return w;
     return 0;
   };
-  const int w32 = width(3), w16 = width(7);
-  if (w32 == 0 || w16 == 0) return;
-  const int boxz = std::max(ext_z, 2);
-  if (boxz > 256) return;
-  SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
-  auto smem_of = [](const SlabBox& b, size_t es) {
-    return kNStage * ((b.bx * b.by * b.bz * es + 127) & ~size_t(127)) + 128;
-  };
-  if (smem_of(b32, 4) > (size_t)kSmemBudget || smem_of(b16, 2) > (size_t)kSmemBudget) return;
-  p->slab = b32;
-  p->slab16 = b16;
-  p->slab_smem = smem_of(b32, 4);
-  p->fwd_variant = 1;
+  int e, z;
+  if (slab_extents(p, kTU, kTV, e, z)) {
+    const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
+    const int boxz = std::max(z, 2);
+    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    if (w32 && w16 && boxz <= 256 && forward_smem(b32, 4, 0) <= (size_t)kSmemBudget &&
+        forward_smem(b16, 2, 0) <= (size_t)kSmemBudget) {
+      p->slab = b32;
+      p->slab16 = b16;
+      p->slab_smem = forward_smem(b32, 4, 0);
+      p->fwd_variant = 1;
+    }
+  }
+  if (p->fwd_pref == 3 && slab_extents(p, kFU, kFV, e, z)) {
+    const int w32 = width(kFanWidths, e, 3), w16 = width(kFanWidths, e, 7);
+    const int boxz = std::max(z, 2);
+    const int lz = (boxz + 1) | 1;  // odd: consecutive lines start in different banks
+    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    const int nsl = slabs_max(p->g);
+    if (w32 && w16 && boxz <= 256 && forward_smem(b32, 4, lz, nsl) <= (size_t)kSmemBudget &&
+        forward_smem(b16, 2, lz, nsl) <= (size_t)kSmemBudget) {
+      p->fan = b32;
+      p->fan16 = b16;
+      p->fan_lz = lz;
+      p->fwd_variant = 2;
+    }
+  }
 }
 
 void forward_prepare(cbct_plan* p) {
-  if (p->fwd_variant != 1) return;
+  if (p->fwd_variant < 1) return;
   prepare_typed<float>(p);
   prepare_typed<__half>(p);
   prepare_typed<__nv_bfloat16>(p);
@@ -639,15 +1020,18 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
   const int cnt = p->count[s];
   if (cnt == 0) return;
   o.wproj = p->d_pweights ? p->d_pweights + (size_t)p->g.width * p->g.height * p->first[s] : nullptr;
-  const size_t nblocks = (size_t)((p->g.width + kTU - 1) / kTU) * ((p->g.height + kTV - 1) / kTV) * cnt;
+  const size_t es = dtype_size(dt);
+  const bool use_slab = p->fwd_variant >= 1 && ((size_t)p->g.nx * es) % 16 == 0 &&
+                        ((size_t)p->g.ny * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
+                        (!p->subset_has_xdom[s] || p->d_volT != nullptr);
+  // One partial sum per block of the kernel that will run.
+  const bool fan = use_slab && p->fwd_variant == 2;
+  const int TU = fan ? kFU : kTU, TV = fan ? kFV : kTV;
+  const size_t nblocks = (size_t)((p->g.width + TU - 1) / TU) * ((p->g.height + TV - 1) / TV) * cnt;
   if (norm2_out) {
     if (nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");
     o.partials = p->d_partials;
   }
-  const size_t es = dtype_size(dt);
-  const bool use_slab = p->fwd_variant == 1 && ((size_t)p->g.nx * es) % 16 == 0 &&
-                        ((size_t)p->g.ny * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
-                        (!p->subset_has_xdom[s] || p->d_volT != nullptr);
   switch (dt) {
     case CBCT_F32: launch_typed<float>(p, s, vol, o, st, dt, use_slab); break;
     case CBCT_F16: launch_typed<__half>(p, s, vol, o, st, dt, use_slab); break;

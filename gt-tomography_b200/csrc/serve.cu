@@ -71,7 +71,7 @@ void validate_request(const cbct_request& r) {
 size_t request_bytes(const cbct_request& r) {
   const cbct_geometry& g = r.geometry;
   const size_t P = (size_t)r.n_views, pl = plane(g), nv = (size_t)g.nx * g.ny * g.nz;
-  const size_t tiles = (size_t)((g.width + kTU - 1) / kTU) * ((g.height + kTV - 1) / kTV);
+  const size_t tiles = forward_tiles(g.width, g.height);
   size_t b = 0;
   int n = 0;
   auto add = [&](size_t x) { b += x; ++n; };

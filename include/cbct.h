@@ -135,7 +135,7 @@ CBCT_API cbct_status cbct_plan_destroy(cbct_plan* plan);
 CBCT_API cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_out,
                              int32_t* count_out);
 
-/* Name of the forward-projector variant the plan selected ("tma-slab" or "gather"). */
+/* Name of the forward-projector variant the plan selected ("tma-fan", "tma-slab" or "gather"). */
 CBCT_API const char* cbct_plan_forward_variant(const cbct_plan* plan);
 
 /* Plan options (no reference counterpart; diagnostics of this library).
@@ -144,6 +144,11 @@ CBCT_API const char* cbct_plan_forward_variant(const cbct_plan* plan);
  * CBCT_OPT_FORCE_GATHER: use the global-gather forward projector. */
 #define CBCT_OPT_DEBUG_CHECKS 1
 #define CBCT_OPT_FORCE_GATHER 2
+/* CBCT_OPT_FORWARD_KERNEL: 0 = automatic (the per-ray slab kernel where its
+ * boxes fit, else gather), 1 = slab, 2 = gather, 3 = the column-fan kernel
+ * (e/d interpolation shared by the rays of a detector column; same results,
+ * slower on B200 at the sizes measured so far). */
+#define CBCT_OPT_FORWARD_KERNEL 3
 CBCT_API cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value);
 
 /* Reads (and optionally clears) the plan's device flag words:

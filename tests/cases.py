@@ -53,10 +53,13 @@ def make(name: str) -> Case:
     if name == "odd":           # nx not a multiple of 4: gather fallback for fp32 TMA pitch
         return Case(name, 30, 26, 18, 30.0, 26.0, 18.0, 36, 28, 60.0, 46.0, 700.0, 1100.0,
                     _ang(10, 200.0, 7.0), np.zeros((10, 2), np.float32))
+    if name == "short":         # short volume under a tall detector: most rows leave through top/bottom
+        return Case(name, 40, 48, 12, 40.0, 48.0, 12.0, 64, 48, 96.0, 96.0, 600.0, 1000.0,
+                    _ang(14, 360.0, 3.0), np.zeros((14, 2), np.float32))
     if name == "c1small":       # config 1 geometry scaled down (128^3 -> 64^3, 180 -> 45 views)
         return Case(name, 64, 64, 64, 64.0, 64.0, 64.0, 128, 96, 192.0, 144.0, 1000.0, 1500.0,
                     _ang(45), np.zeros((45, 2), np.float32))
     raise KeyError(name)
 
 
-ALL = ["cube", "aniso", "offset", "odd"]
+ALL = ["cube", "aniso", "offset", "odd", "short"]

@@ -19,7 +19,7 @@ def _phantom(case, O, seed=3):
 
 
 @pytest.mark.parametrize("name", ALL)
-@pytest.mark.parametrize("variant", ["auto", "gather"])
+@pytest.mark.parametrize("variant", ["auto", "gather", "fan"])
 def test_forward_matches_oracle(gtb, O, cuda, name, variant):
     import torch
     case = make(name)
@@ -28,6 +28,8 @@ def test_forward_matches_oracle(gtb, O, cuda, name, variant):
     plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets)
     if variant == "gather":
         plan.set_option(gtb._lib.CBCT_OPT_FORCE_GATHER, 1)
+    elif variant == "fan":
+        plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 3)
     plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
     v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
     out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
@@ -42,6 +44,33 @@ def test_slab_variant_selected(gtb, cuda):
     case = make("cube")
     plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets)
     assert plan.forward_variant() == "tma-slab"
+    plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 3)
+    assert plan.forward_variant() == "tma-fan"
+    plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 2)
+    assert plan.forward_variant() == "gather"
+
+
+@pytest.mark.parametrize("name", ["short", "cube"])
+def test_kernels_bitwise_equal(gtb, O, cuda, name):
+    """Slab, fan and gather kernels evaluate the same samples in the same order."""
+    import torch
+    case = make(name)
+    _, vol = _phantom(case, O, seed=9)
+    plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets)
+    plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
+    v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
+    outs = {}
+    for k in (1, 3, 2):
+        plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, k)
+        out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
+        plan.forward(v, out)
+        outs[plan.forward_variant()] = out
+        assert plan.read_flags() == (0, 0)
+    assert set(outs) == {"tma-slab", "tma-fan", "gather"}
+    assert torch.equal(outs["tma-slab"], outs["tma-fan"])
+    # the gather kernel interpolates with another FMA arrangement: equal to rounding
+    a, b = outs["tma-slab"].double(), outs["gather"].double()
+    assert float((a - b).norm() / b.norm()) < 1e-6
 
 
 def test_forward_accumulate_and_subsets(gtb, O, cuda):

@@ -590,10 +590,9 @@ def served(args):
     """Serving loop (the north star's fifth configuration): Poisson arrivals
     at --rate requests/s of FDK (70 %, Hann-windowed ramp) and OS-MOM (30 %,
     8 subsets x 10 iterations, positivity) reconstructions with the batched
-    configuration's scan shapes (seeds 2000+i), storage bfloat16 or float32
-    per request (seeded coin; bfloat16 OS-MOM refines in FP32 every 5
-    iterations), admitted against a --budget-gb HBM budget on --slots request
-    slots.  Inputs are made on the device beforehand and held in pinned host
+    configuration's scan shapes (seeds 2000+i), projections stored as
+    bfloat16 or float32 per request (seeded coin; arithmetic FP32), admitted
+    against a --budget-gb HBM budget on --slots request slots.  Inputs are made on the device beforehand and held in pinned host
     memory; every request copies its projections in and its volume out.
     Latency = completion - submission on the host clock (a request is
     submitted at its arrival time).  The plain FP32 path then serves the same
@@ -616,8 +615,7 @@ def served(args):
         g, ang, off = inputs[i][:3]
         if kinds[i] == "fdk":
             return gtb.Server.fdk_request(g, ang, off, proj, vol, filt=gtb.hann_ramp_filter(g.width))
-        return gtb.Server.osmom_request(g, ang, off, proj, vol, 8, iterations=10, nonneg=True, use_graph=True,
-                                        refine_every=5 if proj.dtype == torch.bfloat16 else 0)
+        return gtb.Server.osmom_request(g, ang, off, proj, vol, 8, iterations=10, nonneg=True, use_graph=True)
 
     inputs, reqs, vols = [], [], []
     for i, sp in enumerate(specs):
@@ -698,7 +696,7 @@ def served(args):
             "config": {"workload": f"{n} requests at {args.rate}/s, sizes of the batched configuration (seeds 2000+i)",
                        "fdk": int(sum(k == "fdk" for k in kinds)), "osmom": int(sum(k == "osmom" for k in kinds)),
                        "bf16_requests": int(use_bf16.sum()), "slots": args.slots, "budget_gb": args.budget_gb,
-                       "osmom": "8 subsets x 10 iterations, positivity, CUDA graph; bf16 refines every 5",
+                       "osmom": "8 subsets x 10 iterations, positivity, CUDA graph; bf16 = projections stored bf16",
                        "fdk_filter": "Hann-windowed ramp", "latency": "host clock, completion - arrival"},
             "latency_p50_s": round(float(np.percentile(lat, 50)), 3),
             "latency_p99_s": round(float(np.percentile(lat, 99)), 3),

@@ -39,7 +39,9 @@ std::string& last_error_slot() {
 void ensure_smem_attr(const void* func, size_t bytes) {
   static std::mutex mu;
   static std::map<std::pair<int, const void*>, size_t> done;
-  if (bytes <= 48 * 1024) return;
+  // The 48 KB default covers static plus dynamic shared memory, so the limit
+  // is raised for any dynamic size (once per kernel, device and size).
+  if (bytes == 0) return;
   int dev = 0;
   CBCT_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
@@ -266,6 +268,9 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   p->d_partials = plan_alloc_n<double>(p.get(), p->n_partials);
   p->d_flags = plan_alloc_n<int>(p.get(), 4);
   plan_memset(p.get(), p->d_flags, 0, sizeof(int) * 4);
+  // Plans that never project forward skip the box sizing (a host loop over
+  // every view, tile and slab); a forward call on them takes the gather kernel.
+  if (!forward_buffers) p->fwd_pref = 2;
   forward_choose_variant(p.get());
   if (forward_buffers) forward_prepare(p.get());
   backproject_choose_variant(p.get());

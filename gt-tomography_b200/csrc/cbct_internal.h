@@ -240,8 +240,9 @@ T* plan_alloc_n(cbct_plan* p, size_t n) {
   return static_cast<T*>(plan_alloc(p, n * sizeof(T)));
 }
 
-// Raises a kernel's dynamic shared-memory limit once (no-op when already high
-// enough, so it is safe to call before launches that may be captured).
+// Raises a kernel's dynamic shared-memory limit to `bytes` once per kernel
+// and device (no-op when already high enough, so it is safe to call before
+// launches that may be captured).
 void ensure_smem_attr(const void* func, size_t bytes);
 
 // forward.cu

@@ -252,8 +252,13 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
   kf = ke;
 }
 
+// 16-bit boxes take half the shared memory, so those instantiations ask for a
+// register budget that lets four CTAs share an SM.
+template <class V>
+constexpr int slab_min_blocks() { return sizeof(V) == 4 ? 3 : 4; }
+
 template <class V, int BX, bool CHECK>
-__global__ void __launch_bounds__(256, 3) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
+__global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
                                                        const __grid_constant__ CUtensorMap map_t,
                                                        const V* __restrict__ vol,
                                                        const ViewParams* __restrict__ views, GridConst gc,

@@ -91,8 +91,7 @@ size_t request_bytes(const cbct_request& r) {
     if (r.storage != CBCT_F32) add(sizeof(float) * pl * P);  // FP32 filtered copy
   } else {
     add(nv * sizeof(float));  // transposed volume of the forward projector (upper bound)
-    const bool lowp = r.storage != CBCT_F32;
-    add((2 * nv + pl * P + (lowp ? (nv + 1) / 2 + 64 : 0)) * sizeof(float));  // solver workspace
+    add((2 * nv + pl * P) * sizeof(float));  // solver workspace (FP32 volume input)
   }
   return b + n * kAllocSlack;
 }
@@ -200,8 +199,11 @@ void run_request(cbct_server* sv, Request& q, cudaStream_t st) {
     float* work = r.storage == CBCT_F32 ? static_cast<float*>(proj) : nullptr;
     fdk_run(p, proj, vol, filter, flags, work, st, r.storage);
   } else {
+    // Only the measured projections take the request's storage type: a 16-bit
+    // copy of the volume for the forward projector saves no memory (the FP32
+    // master stays) and its reads cost a conversion per tap.
     cbct_solver_params prm = r.params;
-    prm.storage = r.storage;
+    prm.storage = CBCT_F32;
     prm.proj_storage = r.storage;
     osmom_solve(p, proj, nullptr, vol, prm, nullptr, st);
   }

@@ -376,12 +376,12 @@ typedef struct {
   const float* offsets_xy;     /* host, 2*n_views, or NULL for zero offsets (copied at submit) */
   int32_t n_views;
   int32_t n_subsets;           /* OS-MOM: round-robin subsets of CBSubsetOperator::setup */
-  cbct_dtype storage;          /* device storage of the projections; OS-MOM also keeps its
-                                  forward-projector volume input in this type (FP32 master) */
+  cbct_dtype storage;          /* device storage of the measured projections (FP32 arithmetic;
+                                  volumes stay FP32) */
   const void* proj_host;       /* host, W*H*n_views values of type `storage`, acquisition order;
                                   must stay valid until the request completes */
   float* vol_host;             /* host, nx*ny*nz floats, written when the request completes */
-  cbct_solver_params params;   /* OS-MOM; storage and proj_storage are set from `storage` */
+  cbct_solver_params params;   /* OS-MOM; proj_storage is set from `storage`, storage to CBCT_F32 */
   const float* filter;         /* FDK: host array of W+1 floats, or NULL for the default (copied) */
   uint32_t fdk_flags;          /* FDK: CBCT_FDK_OFFSET / CBCT_FDK_PARKER in addition to the rules */
   int32_t offset_correction;   /* -1: the reference's override rule (per subset for OS-MOM); 0 off; 1 on */

@@ -34,7 +34,7 @@ EXPORTED = [
     "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
     "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
-    "cbct_fdk_filter_ex", "cbct_fdk_ex",
+    "cbct_fdk_filter_ex", "cbct_fdk_ex", "cbct_host_forward", "cbct_host_backproject", "cbct_plan_set_bins",
     "cbct_server_create", "cbct_server_request_bytes", "cbct_server_submit", "cbct_server_wait",
     "cbct_server_now", "cbct_server_destroy",
 ]
@@ -135,6 +135,9 @@ _SIGS = {
     "cbct_plan_set_projection_weights": (C.c_int, [_vp, _vp]),
     "cbct_fdk_filter_ex": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _vp, _u32, _vp]),
     "cbct_fdk_ex": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _u32, _vp, _vp]),
+    "cbct_host_forward": (C.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _vp]),
+    "cbct_plan_set_bins": (C.c_int, [_vp, _i32, _vp]),
+    "cbct_host_backproject": (C.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _u32, _i32, _f, _i32, _vp]),
     "cbct_server_create": (C.c_int, [C.POINTER(CbctServerConfig), C.POINTER(_vp)]),
     "cbct_server_request_bytes": (C.c_int, [C.POINTER(CbctRequest), C.POINTER(_sz)]),
     "cbct_server_submit": (C.c_int, [_vp, C.POINTER(CbctRequest), C.POINTER(C.c_uint64)]),

@@ -251,6 +251,9 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   p->first.push_back(0);
   p->count.push_back(n_views);
   p->offcorr.push_back(0);
+  p->seg_begin.assign(n_subsets, 0);
+  p->seg_end.assign(n_subsets, 0);
+  p->seg_bin.assign(n_subsets + 1, -1);
   p->angles.assign(angles, angles + n_views);
   p->offsets.assign(offsets, offsets + 2 * (size_t)n_views);
   for (int i = 0; i < n_views; ++i) {
@@ -282,6 +285,10 @@ static int subset_index(const cbct_plan* p, int s) {
   CBCT_REQUIRE(p != nullptr, "plan is NULL");
   CBCT_REQUIRE(s >= -1 && s < p->n_subsets, "subset index out of range");
   return s < 0 ? p->n_subsets : s;
+}
+
+static void require_one_bin(const cbct_plan* p, const char* what) {
+  if (p->n_bins > 1) throw Error(CBCT_ERR_UNSUPPORTED, std::string(what) + " does not take a binned plan");
 }
 
 static float* proj_scratch(cbct_plan* p, size_t elems) {
@@ -428,13 +435,73 @@ cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t re
   });
 }
 
+// Segments (view ranges of one bin) of subset i, or of every subset for the
+// all-views entry, in view order.
+static std::vector<int> segments_of(const cbct_plan* p, int i) {
+  std::vector<int> ks;
+  const int s0 = i < p->n_subsets ? i : 0, s1 = i < p->n_subsets ? i + 1 : p->n_subsets;
+  for (int s = s0; s < s1; ++s)
+    for (int k = p->seg_begin[s]; k < p->seg_end[s]; ++k) ks.push_back(k);
+  return ks;
+}
+
 cbct_status cbct_forward(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol, float* proj,
                          int32_t accumulate, void* stream) {
   return guard([&] {
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(vol && proj, "NULL array");
+    if (plan->n_bins > 1) {
+      // Each bin's views project that bin's volume (cuConebeamProjectionOperator.cpp:49-78).
+      const size_t plane = (size_t)plan->g.width * plan->g.height;
+      const size_t vb = (size_t)plan->g.nx * plan->g.ny * plan->g.nz * dtype_size(vol_dtype);
+      for (int k : segments_of(plan, i))
+        forward_launch(plan, k, vol_dtype, static_cast<const char*>(vol) + vb * plan->seg_bin[k],
+                       proj + plane * (plan->first[k] - plan->first[i]), nullptr, 1.f, 0, 0, accumulate, nullptr,
+                       S(stream));
+      return;
+    }
     forward_launch(plan, i, vol_dtype, vol, proj, nullptr, 1.f, 0, 0, accumulate, nullptr, S(stream));
   });
+}
+
+// mult_MH of one view range (a subset, a bin segment, or every view: i =
+// n_subsets) into one volume.
+static void backproject_range(cbct_plan* plan, int i, const float* proj, float* vol, uint32_t flags,
+                              int32_t use_plan_offset, int32_t accumulate, cudaStream_t st) {
+  const size_t plane = (size_t)plan->g.width * plan->g.height;
+  const bool single = i != plan->n_subsets;
+  // Which views get the Wang weight: every view of the call with the explicit
+  // flag, else the subsets whose offset correction is on (all subsets, s = -1).
+  auto weighted = [&](int k) {
+    return (flags & CBCT_BP_OFFSET_WEIGHT) != 0 || (use_plan_offset && plan->offcorr[k] != 0);
+  };
+  bool any = plan->d_pweights != nullptr || (flags & CBCT_BP_OFFSET_WEIGHT) != 0;
+  if (!any && use_plan_offset) {
+    if (single) any = weighted(i);
+    else for (int k = 0; k < plan->n_subsets; ++k) any = any || weighted(k);
+  }
+  const float* in = proj;
+  if (any) {
+    // mult_MH works on a weighted copy of its input (CBSubsetWeightOperator.h:44-49,
+    // cuConebeamProjectionOperator.cpp:101-102); the input itself is not modified.
+    float* w = proj_scratch(plan, plane * plan->count[i]);
+    const int k0 = single ? i : 0, k1 = single ? i + 1 : plan->n_subsets;
+    for (int k = k0; k < k1; ++k) {
+      const size_t o = single ? 0 : plane * plan->first[k];
+      const size_t n = plane * plan->count[k];
+      if (n == 0) continue;
+      const float* src = proj + o;
+      if (plan->d_pweights) {
+        mul_launch(w + o, src, plan->d_pweights + plane * plan->first[k], n, st);
+        src = w + o;
+      }
+      const bool off = weighted(k);
+      if (off) offset_weight_launch(plan, k, src, w + o, 0, st);
+      else if (src != w + o) CBCT_CUDA(cudaMemcpyAsync(w + o, src, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    in = w;
+  }
+  backproject_launch(plan, i, in, vol, (flags & CBCT_BP_FDK_WEIGHT) ? 1 : 0, accumulate, 1.f, st);
 }
 
 cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, float* vol, uint32_t flags,
@@ -443,39 +510,64 @@ cbct_status cbct_backproject(cbct_plan* plan, int32_t s, const float* proj, floa
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(vol && proj, "NULL array");
     CBCT_REQUIRE((flags & ~(CBCT_BP_OFFSET_WEIGHT | CBCT_BP_FDK_WEIGHT)) == 0, "unknown flags");
-    const size_t plane = (size_t)plan->g.width * plan->g.height;
-    // Which views get the Wang weight: every view of the call with the explicit
-    // flag, else the subsets whose offset correction is on (all subsets, s = -1).
-    auto weighted = [&](int k) {
-      return (flags & CBCT_BP_OFFSET_WEIGHT) != 0 || (use_plan_offset && plan->offcorr[k] != 0);
-    };
-    bool any = plan->d_pweights != nullptr || (flags & CBCT_BP_OFFSET_WEIGHT) != 0;
-    if (!any && use_plan_offset) {
-      if (i < plan->n_subsets) any = weighted(i);
-      else for (int k = 0; k < plan->n_subsets; ++k) any = any || weighted(k);
-    }
-    const float* in = proj;
-    if (any) {
-      // mult_MH works on a weighted copy of its input (CBSubsetWeightOperator.h:44-49,
-      // cuConebeamProjectionOperator.cpp:101-102); the input itself is not modified.
-      float* w = proj_scratch(plan, plane * plan->count[i]);
-      const int k0 = i < plan->n_subsets ? i : 0, k1 = i < plan->n_subsets ? i + 1 : plan->n_subsets;
-      for (int k = k0; k < k1; ++k) {
-        const size_t o = i < plan->n_subsets ? 0 : plane * plan->first[k];
-        const size_t n = plane * plan->count[k];
-        if (n == 0) continue;
-        const float* src = proj + o;
-        if (plan->d_pweights) {
-          mul_launch(w + o, src, plan->d_pweights + plane * plan->first[k], n, S(stream));
-          src = w + o;
-        }
-        const bool off = i < plan->n_subsets ? weighted(i) : weighted(k);
-        if (off) offset_weight_launch(plan, k, src, w + o, 0, S(stream));
-        else if (src != w + o) CBCT_CUDA(cudaMemcpyAsync(w + o, src, n * sizeof(float), cudaMemcpyDeviceToDevice, S(stream)));
+    if (plan->n_bins > 1) {
+      // Every bin's volume receives its own views; a bin without views in the
+      // call is cleared unless accumulating (cuConebeamProjectionOperator.cpp:82-116).
+      const size_t plane = (size_t)plan->g.width * plan->g.height;
+      const size_t nv = (size_t)plan->g.nx * plan->g.ny * plan->g.nz;
+      std::vector<int> seen(plan->n_bins, 0);
+      for (int k : segments_of(plan, i)) {
+        const int b = plan->seg_bin[k];
+        backproject_range(plan, k, proj + plane * (plan->first[k] - plan->first[i]), vol + nv * b, flags,
+                          use_plan_offset, accumulate || seen[b], S(stream));
+        seen[b] = 1;
       }
-      in = w;
+      for (int b = 0; b < plan->n_bins; ++b)
+        if (!seen[b] && !accumulate) CBCT_CUDA(cudaMemsetAsync(vol + nv * b, 0, nv * sizeof(float), S(stream)));
+      return;
     }
-    backproject_launch(plan, i, in, vol, (flags & CBCT_BP_FDK_WEIGHT) ? 1 : 0, accumulate, 1.f, S(stream));
+    backproject_range(plan, i, proj, vol, flags, use_plan_offset, accumulate, S(stream));
+  });
+}
+
+cbct_status cbct_plan_set_bins(cbct_plan* plan, int32_t n_bins, const int32_t* view_bin) {
+  return guard([&] {
+    CBCT_REQUIRE(plan, "plan is NULL");
+    const int S = plan->n_subsets;
+    // Back to the subsets and the all-views entry.
+    plan->first.resize(S + 1);
+    plan->count.resize(S + 1);
+    plan->offcorr.resize(S + 1);
+    plan->seg_begin.assign(S, 0);
+    plan->seg_end.assign(S, 0);
+    plan->seg_bin.assign(S + 1, -1);
+    plan->n_bins = 1;
+    graph_cache_free(plan);
+    if (view_bin && n_bins > 1) {
+      for (int v = 0; v < plan->n_views; ++v)
+        CBCT_REQUIRE(view_bin[v] >= 0 && view_bin[v] < n_bins, "view bin out of range");
+      for (int s = 0; s < S; ++s) {
+        plan->seg_begin[s] = (int)plan->first.size();
+        std::vector<int> used(n_bins, 0);
+        for (int i = 0; i < plan->count[s];) {
+          const int v = plan->first[s] + i, b = view_bin[v];
+          int n = 1;
+          while (i + n < plan->count[s] && view_bin[v + n] == b) ++n;
+          // CBSubsetOperator::setup sorts each subset by bin (CBSubsetOperator.cpp:86-87).
+          CBCT_REQUIRE(!used[b], "the views of a bin must be contiguous within each subset");
+          used[b] = 1;
+          plan->first.push_back(v);
+          plan->count.push_back(n);
+          plan->offcorr.push_back(plan->offcorr[s]);
+          plan->seg_bin.push_back(b);
+          i += n;
+        }
+        plan->seg_end[s] = (int)plan->first.size();
+      }
+      plan->n_bins = n_bins;
+    }
+    forward_choose_variant(plan);
+    forward_prepare(plan);
   });
 }
 
@@ -499,6 +591,7 @@ cbct_status cbct_offset_correct(cbct_plan* plan, int32_t s, float* proj, int32_t
 cbct_status cbct_fdk_filter(cbct_plan* plan, int32_t s, const float* proj_in, float* proj_out, const float* filter,
                             uint32_t flags, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_fdk_filter");
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(proj_in && proj_out, "NULL array");
     fdk_filter_launch(plan, i, proj_in, proj_out, filter, flags, S(stream));
@@ -508,6 +601,7 @@ cbct_status cbct_fdk_filter(cbct_plan* plan, int32_t s, const float* proj_in, fl
 cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float* filter, uint32_t flags,
                      float* work, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_fdk");
     CBCT_REQUIRE(plan && proj && vol, "NULL argument");
     fdk_run(plan, proj, vol, filter, flags, work, S(stream), CBCT_F32);
   });
@@ -520,6 +614,7 @@ static void require_dtype(cbct_dtype dt) {
 cbct_status cbct_fdk_filter_ex(cbct_plan* plan, int32_t s, cbct_dtype proj_dtype, const void* proj_in,
                                float* proj_out, const float* filter, uint32_t flags, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_fdk_filter_ex");
     const int i = subset_index(plan, s);
     require_dtype(proj_dtype);
     CBCT_REQUIRE(proj_in && proj_out, "NULL array");
@@ -532,6 +627,7 @@ cbct_status cbct_fdk_filter_ex(cbct_plan* plan, int32_t s, cbct_dtype proj_dtype
 cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj, float* vol, const float* filter,
                         uint32_t flags, float* work, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_fdk_ex");
     CBCT_REQUIRE(plan && proj && vol, "NULL argument");
     require_dtype(proj_dtype);
     CBCT_REQUIRE(proj_dtype == CBCT_F32 || (const void*)work != proj, "a 16-bit input cannot be filtered in place");
@@ -542,6 +638,7 @@ cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj
 cbct_status cbct_spacecarver(cbct_plan* plan, int32_t s, const float* proj, float limit, uint8_t* mask,
                              int32_t combine, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_spacecarver");
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(proj && mask, "NULL array");
     spacecarver_launch(plan, i, proj, limit, mask, combine, S(stream));
@@ -567,6 +664,7 @@ cbct_status cbct_plan_set_mask(cbct_plan* plan, const uint8_t* mask) {
 cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtype vol_dtype, const void* vol, const float* b,
                                   float* r, float scale, int32_t apply_offset, double* norm2_out, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_forward_residual");
     const int i = subset_index(plan, s);
     CBCT_REQUIRE(vol && b && r, "NULL array");
     forward_launch(plan, i, vol_dtype, vol, r, b, scale, 1, apply_offset, 0, norm2_out, S(stream));
@@ -633,11 +731,29 @@ cbct_status cbct_osmom_solve(cbct_plan* plan, const void* b, const float* x0, fl
 cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, float* x_out,
                               const cbct_solver_params* params, double* cost_out, void* stream) {
   return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_ossart_solve");
     CBCT_REQUIRE(plan && b && x_out, "NULL argument");
     const cbct_solver_params prm = solver_defaults(params);
     CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
     if (prm.proj_storage != CBCT_F32) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART takes float projections");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
+  });
+}
+
+cbct_status cbct_host_forward(cbct_plan* plan, int32_t s_first, int32_t n_batches, const float* vol_host,
+                              float* proj_host, const int32_t* view_index, int32_t offset_sqrt, void* stream) {
+  return guard([&] {
+    host_forward(plan, s_first, n_batches, vol_host, proj_host, view_index, offset_sqrt, S(stream));
+  });
+}
+
+cbct_status cbct_host_backproject(cbct_plan* plan, int32_t s_first, int32_t n_batches, const float* proj_host,
+                                  float* vol_host, const int32_t* view_index, int32_t fbp, const float* filter,
+                                  uint32_t fdk_flags, int32_t offset_sqrt, float scale, int32_t accumulate,
+                                  void* stream) {
+  return guard([&] {
+    host_backproject(plan, s_first, n_batches, proj_host, vol_host, view_index, fbp, filter, fdk_flags, offset_sqrt,
+                     scale, accumulate, S(stream));
   });
 }
 

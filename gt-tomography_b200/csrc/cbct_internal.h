@@ -203,6 +203,9 @@ struct cbct_plan {
   float* d_fdk_work = nullptr;      // filtered projections for cbct_fdk
   size_t fdk_work_elems = 0;
   void* graph_cache = nullptr;      // captured solver graph (solver.cu)
+  float* d_stream_buf[2] = {nullptr, nullptr};  // batch buffers of the host-array operators
+  size_t stream_buf_elems = 0;
+  float* d_stream_vol = nullptr;    // bin volume of the host-array operators
 
   // solver workspace (allocated on first solve, reused)
   float* ws = nullptr;
@@ -212,6 +215,14 @@ struct cbct_plan {
   int force_gather = 0;
   const unsigned char* d_mask = nullptr;  // voxel mask applied after back-projection (caller-owned)
   const float* d_pweights = nullptr;      // projection weights, all views in subset order (caller-owned)
+
+  // Bins (CBCT_binning): with n_bins > 1 every view belongs to one bin and
+  // images hold n_bins volumes.  Subset s splits into the runs of its views
+  // that share a bin ("segments"); they are kept as further view ranges after
+  // index n_subsets of first/count/offcorr: range indices seg_begin[s] ..
+  // seg_end[s]-1, bin seg_bin[k] (-1 for the subsets and the all-views entry).
+  int n_bins = 1;
+  std::vector<int> seg_begin, seg_end, seg_bin;
 
   // Device memory source.  Plans of the serving loop draw every buffer from
   // its stream-ordered pool on `pool_stream` (cudaMallocFromPoolAsync /
@@ -275,6 +286,13 @@ void finalize_partials(const double* partials, int n, double* out, cudaStream_t 
 void reduce_noalloc_launch(int kind, const float* a, const float* b, size_t n, double* out, cudaStream_t st);
 void osmom_update_launch(float* z, float* xold, const float* precon, const float* g, size_t n,
                          float step, float mom, int nonneg, cudaStream_t st);
+
+// host_stream.cu: host-array operators over the plan's subsets [s0, s0 + ns)
+void host_forward(cbct_plan* p, int s0, int ns, const float* vol_host, float* proj_host, const int* view_index,
+                  int offset_sqrt, cudaStream_t caller);
+void host_backproject(cbct_plan* p, int s0, int ns, const float* proj_host, float* vol_host, const int* view_index,
+                      int fbp, const float* filter, uint32_t fdk_flags, int offset_sqrt, float scale, int accumulate,
+                      cudaStream_t caller);
 
 // mask.cu
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,

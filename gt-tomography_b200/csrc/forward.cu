@@ -951,8 +951,9 @@ void forward_choose_variant(cbct_plan* p) {
   p->fwd_variant = 0;
   p->slab = SlabBox{0, 0, 0, 0};
   p->fan = SlabBox{0, 0, 0, 0};
-  p->subset_has_xdom.assign(p->n_subsets + 1, 0);
-  for (int s = 0; s <= p->n_subsets; ++s)
+  // Per view range (subsets, the all-views entry and bin segments).
+  p->subset_has_xdom.assign(p->first.size(), 0);
+  for (size_t s = 0; s < p->first.size(); ++s)
     for (int i = p->first[s]; i < p->first[s] + p->count[s]; ++i)
       if (p->hviews[i].dom == 0) p->subset_has_xdom[s] = 1;
   if (p->force_gather || p->fwd_pref == 2) return;
@@ -998,7 +999,7 @@ void forward_prepare(cbct_plan* p) {
   prepare_typed<__half>(p);
   prepare_typed<__nv_bfloat16>(p);
   bool any_x = false;
-  for (int s = 0; s <= p->n_subsets; ++s) any_x = any_x || p->subset_has_xdom[s];
+  for (size_t s = 0; s < p->subset_has_xdom.size(); ++s) any_x = any_x || p->subset_has_xdom[s];
   if (any_x && !p->d_volT)
     p->d_volT = plan_alloc_n<float>(p, (size_t)p->g.nx * p->g.ny * p->g.nz);
 }

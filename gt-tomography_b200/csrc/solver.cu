@@ -70,11 +70,18 @@ __global__ void osmom_update_kernel(float* __restrict__ z, float* __restrict__ x
                                     const float* __restrict__ precon, const float* __restrict__ g,
                                     size_t n, float step, float mom, int nonneg) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const float zt = fmaf(-step, precon[i] * g[i], z[i]);
+    const float zt = fmaf(-step, precon[i] * (g ? g[i] : 0.f), z[i]);  // g = NULL: no gradient
     const float xc = nonneg ? fmaxf(zt, 0.f) : zt;
     z[i] = fmaf(-mom, xold[i], xc * (1.f + mom));
     xold[i] = xc;
   }
+}
+
+// x = 1 / max(x, 1e-6): the preconditioner of osMOMSolverD.h:115-120 when
+// its back-projection is accumulated over several launches.
+__global__ void recip_kernel(float* __restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = 1.f / fmaxf(x[i], 1e-6f);
 }
 
 __global__ void fill_kernel(float* __restrict__ x, size_t n, float v) {
@@ -161,6 +168,12 @@ void osmom_update_launch(float* z, float* xold, const float* precon, const float
   check_launch("osmom_update_kernel");
 }
 
+static void recip_launch(float* x, size_t n, cudaStream_t st) {
+  if (n == 0) return;
+  recip_kernel<<<ew_blocks(n), 256, 0, st>>>(x, n);
+  check_launch("recip_kernel");
+}
+
 void fill_launch(float* x, size_t n, float v, cudaStream_t st) {
   if (n == 0) return;
   fill_kernel<<<ew_blocks(n), 256, 0, st>>>(x, n, v);
@@ -236,6 +249,62 @@ static void run_osmom(cbct_plan* p, const void* b, const float* x0, float* z, co
       const double stepsz = double(prm.beta) / (1.0 + double(prm.gamma) * it) * S;
       const double mom = (told - 1.0) / t;
       backproject_mom_launch(p, s, rs, z, xold, D, float(stepsz), float(mom), prm.non_negativity, st);
+      told = t;
+    }
+  }
+}
+
+// osMOMSolverD with bins (the subset operator of CBSubsetOperator over
+// binned cuConebeamProjectionOperators, CBSubsetOperator.cpp:66-135 and
+// cuConebeamProjectionOperator.cpp:49-116): z, xold and D hold n_bins volumes;
+// a subset's segments project and back-project their own bin's volume, and
+// the bins without views in the subset take the momentum step with a zero
+// gradient (their mult_MH output is 0).
+static void run_osmom_bins(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+                           float* xold, float* D, float* r, cudaStream_t st) {
+  const size_t nv = vol_elems(p), pl = plane_elems(p);
+  const int S = p->n_subsets, NB = p->n_bins;
+  const size_t nall = nv * NB;
+  // D = 1/max(A^T (W A 1), 1e-6) per bin; one ones-volume serves every bin.
+  fill_launch(xold, nv, 1.f, st);
+  for (int s = 0; s < S; ++s)
+    for (int k = p->seg_begin[s]; k < p->seg_end[s]; ++k)
+      forward_launch_ex(p, k, CBCT_F32, xold, r + pl * p->first[k], nullptr, nullptr, 1.f, 1, p->offcorr[k], 0,
+                        nullptr, st);
+  CBCT_CUDA(cudaMemsetAsync(D, 0, nall * sizeof(float), st));
+  for (int s = 0; s < S; ++s)
+    for (int k = p->seg_begin[s]; k < p->seg_end[s]; ++k)
+      backproject_launch(p, k, r + pl * p->first[k], D + nv * p->seg_bin[k], 0, 1, 1.f, st);
+  recip_launch(D, nall, st);
+  if (x0) {
+    CBCT_CUDA(cudaMemcpyAsync(z, x0, nall * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CBCT_CUDA(cudaMemcpyAsync(xold, x0, nall * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  } else {
+    CBCT_CUDA(cudaMemsetAsync(z, 0, nall * sizeof(float), st));
+    CBCT_CUDA(cudaMemsetAsync(xold, 0, nall * sizeof(float), st));
+  }
+  std::vector<int> seg_of_bin(NB);
+  double t = 1.0, told = 1.0;
+  for (int it = 0; it < prm.iterations; ++it) {
+    for (int s = 0; s < S; ++s) {
+      t = 0.5 * (1.0 + std::sqrt(1.0 + 4.0 * t * t));
+      std::fill(seg_of_bin.begin(), seg_of_bin.end(), -1);
+      for (int k = p->seg_begin[s]; k < p->seg_end[s]; ++k) {
+        seg_of_bin[p->seg_bin[k]] = k;
+        forward_launch_ex(p, k, CBCT_F32, z + nv * p->seg_bin[k], r + pl * p->first[k], b + pl * p->first[k], nullptr,
+                          1.f, 1, p->offcorr[k], 0, nullptr, st);
+      }
+      const double stepsz = double(prm.beta) / (1.0 + double(prm.gamma) * it) * S;
+      const double mom = (told - 1.0) / t;
+      for (int bb = 0; bb < NB; ++bb) {
+        const int k = seg_of_bin[bb];
+        if (k >= 0)
+          backproject_mom_launch(p, k, r + pl * p->first[k], z + nv * bb, xold + nv * bb, D + nv * bb, float(stepsz),
+                                 float(mom), prm.non_negativity, st);
+        else
+          osmom_update_launch(z + nv * bb, xold + nv * bb, D + nv * bb, nullptr, nv, float(stepsz), float(mom),
+                              prm.non_negativity, st);
+      }
       told = t;
     }
   }
@@ -334,6 +403,24 @@ void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const c
                  double* resid, cudaStream_t st) {
   CBCT_REQUIRE(prm.proj_storage == CBCT_F32 || prm.proj_storage == CBCT_F16 || prm.proj_storage == CBCT_BF16,
                "unknown projection storage type");
+  if (p->n_bins > 1) {
+    if (prm.storage != CBCT_F32 || prm.proj_storage != CBCT_F32 || resid)
+      throw Error(CBCT_ERR_UNSUPPORTED, "binned OS-MOM: fp32 storage, no residual trace");
+    const size_t nall = vol_elems(p) * p->n_bins;
+    float* ws = workspace(p, 2 * nall + proj_elems(p));
+    std::vector<uint64_t> key = {3, (uint64_t)b, (uint64_t)x0, (uint64_t)z, (uint64_t)prm.iterations,
+                                 (uint64_t)prm.non_negativity, (uint64_t)p->n_bins};
+    uint32_t bb, gg;
+    std::memcpy(&bb, &prm.beta, 4);
+    std::memcpy(&gg, &prm.gamma, 4);
+    key.push_back(bb);
+    key.push_back(gg);
+    const float* bf = static_cast<const float*>(b);
+    run_maybe_graph(p, prm.use_graph != 0, key, st, [&](cudaStream_t s) {
+      run_osmom_bins(p, bf, x0, z, prm, ws, ws + nall, ws + 2 * nall, s);
+    });
+    return;
+  }
   const size_t nv = vol_elems(p), np = proj_elems(p);
   const bool lowp = prm.storage != CBCT_F32;
   const size_t need = 2 * nv + np + (lowp ? (nv + 1) / 2 + 64 : 0);

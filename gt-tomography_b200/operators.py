@@ -220,6 +220,7 @@ class Plan:
         self._h = h
         self.n_views = P
         self.n_subsets = S
+        self.n_bins = 1
         self.first = np.concatenate([[0], np.cumsum(self.subset_sizes)[:-1]]).astype(np.int64)
 
     @property
@@ -239,7 +240,24 @@ class Plan:
 
     @property
     def vol_shape(self):
-        return (self.g.nz, self.g.ny, self.g.nx)
+        """(nz, ny, nx), or (bins, nz, ny, nx) for a binned plan."""
+        v = (self.g.nz, self.g.ny, self.g.nx)
+        return ((self.n_bins,) + v) if getattr(self, "n_bins", 1) > 1 else v
+
+    def set_bins(self, view_bin, n_bins: int):
+        """Bins of the plan's views (cbct_plan_set_bins): view_bin per view in
+        plan order, the views of a bin contiguous within every subset; volumes
+        then hold n_bins images.  n_bins <= 1 or None returns to one bin."""
+        if view_bin is None or int(n_bins) <= 1:
+            L.call("cbct_plan_set_bins", self._h, 1, None)
+            self.n_bins = 1
+            return
+        vb = np.ascontiguousarray(view_bin, np.int32)
+        if vb.size != self.n_views:
+            raise ValueError("view_bin needs one entry per view")
+        L.call("cbct_plan_set_bins", self._h, int(n_bins), vb.ctypes.data)
+        self.n_bins = int(n_bins)
+        self.view_bin = vb
 
     def proj_shape(self, s=-1):
         n = self.n_views if s < 0 else int(self.subset_sizes[s])
@@ -551,8 +569,7 @@ class CBSubsetOperator:
         P = geo.angles.size
         if binning is None:
             binning = CBCT_binning([list(range(P))])
-        if binning.get_number_of_bins() != 1:
-            raise NotImplementedError("4-D binning is not supported by this build")
+        self.n_bins = binning.get_number_of_bins()
         all_angles = geo.angles - geo.angles.min()
         view_bin = np.full(P, -1, np.int32)
         for b, views in enumerate(binning.bins):
@@ -560,6 +577,7 @@ class CBSubsetOperator:
         order, sizes = subset_partition(P, self.number_of_subsets, view_bin)
         self.permutation = order
         self.subset_sizes = sizes
+        self.view_bin = view_bin[order]   # bin of each view in subset order
         if acq.projections is not None:
             acq.set_projections(np.ascontiguousarray(acq.projections[order]))
         geo.set_angles(all_angles[order])
@@ -588,6 +606,8 @@ class CBSubsetOperator:
         H, W = proj.shape[1], proj.shape[2]
         g = _cgeom(self.acq.geometry, W, H, self.domain_dims[:3], self.is_dims_in_mm, self.samples_per_pixel)
         self.plan = Plan(g, self.acq.geometry.angles, self.acq.geometry.offsets, self.subset_sizes, self.offcorr)
+        if self.n_bins > 1:
+            self.plan.set_bins(self.view_bin, self.n_bins)
 
     def set_use_offset_correction(self, use: bool):
         self.use_offset_override = bool(use)
@@ -671,12 +691,30 @@ class CBSubsetWeightOperator(CBSubsetOperator):
         self.plan.set_projection_weights(self.weights)
 
 
+def _host_f32(a, what):
+    """Pointer of a C-contiguous float32 host array (numpy or CPU torch tensor)."""
+    T = torch()
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError(f"{what} must be a C-contiguous float32 array")
+        return a.ctypes.data
+    if isinstance(a, T.Tensor) and not a.is_cuda:
+        if a.dtype != T.float32 or not a.is_contiguous():
+            raise TypeError(f"{what} must be a contiguous float32 tensor")
+        return a.data_ptr()
+    raise TypeError(f"{what} must be a host array")
+
+
 class hoCuConebeamProjectionOperator:
     """Host-array operator with optional FDK (hoCuConebeamProjectionOperator.h:17-156).
 
-    Host arrays are numpy float32 of shape (P, H, W) / (nz, ny, nx).  Whole
-    bins are staged on the device at once (B200 HBM holds the configs' data);
-    the reference's 20-view batching (.h:23) is accepted and ignored."""
+    Host arrays are float32 numpy arrays (or CPU torch tensors, page-locked for
+    overlapped copies) of shape (P, H, W) for projections and (nz, ny, nx) or
+    (bins, nz, ny, nx) for images.  Each bin's volume stays on the device while
+    its projections stream through two device buffers of
+    `projections_per_batch` views (default 20, .h:23), as the reference's
+    host-array projectors do (conebeam_projection.cu:640-819, :1300-1649);
+    cbct_host_forward / cbct_host_backproject do the streaming."""
 
     def __init__(self):
         self.samples_per_pixel = 1.5
@@ -688,6 +726,7 @@ class hoCuConebeamProjectionOperator:
         self.allow_offset_correction_override = True
         self.frequency_filter = None
         self.domain_dims = None
+        self._cache = None
 
     def setup(self, acquisition: CBCT_acquisition, binning: Optional[CBCT_binning] = None, is_dims_in_mm=None,
               transform_angles=True, is_dims=None):
@@ -702,11 +741,13 @@ class hoCuConebeamProjectionOperator:
         self.binning = binning if binning is not None else CBCT_binning([list(range(geo.angles.size))])
         self.is_dims_in_mm = tuple(float(v) for v in is_dims_in_mm)
         self.preprocessed = True
+        self._cache = None
         if is_dims is not None:
             self.domain_dims = tuple(int(d) for d in is_dims)
 
     def set_domain_dimensions(self, dims):
         self.domain_dims = tuple(int(d) for d in dims)
+        self._cache = None
 
     def set_use_filtered_backprojection(self, use: bool):
         self.use_fbp = bool(use)
@@ -719,70 +760,93 @@ class hoCuConebeamProjectionOperator:
         return self.use_offset_correction
 
     def set_num_projections_per_batch(self, n: int):
+        if int(n) < 1:
+            raise ValueError("projections_per_batch must be >= 1")
         self.projections_per_batch = int(n)
+        self._cache = None
 
     def set_num_samples_per_pixel(self, spp: float):
         self.samples_per_pixel = float(spp)
+        self._cache = None
 
     def set_frequency_filter(self, filt):
         self.frequency_filter = np.ascontiguousarray(filt, np.float32)
 
-    def _plan(self, views, W, H):
+    def _stream_plan(self, W, H):
+        """Plan whose views are the bins' views in bin order, cut into batches
+        of projections_per_batch views (the plan's subsets)."""
+        key = (W, H, self.domain_dims[:3], self.projections_per_batch, self.samples_per_pixel)
+        if self._cache is not None and self._cache[0] == key:
+            return self._cache[1]
+        if not self.preprocessed:
+            raise RuntimeError("hoCuConebeamProjectionOperator: setup not performed")
         geo = self.acquisition.geometry
         g = _cgeom(geo, W, H, self.domain_dims[:3], self.is_dims_in_mm, self.samples_per_pixel)
-        idx = np.asarray(views, np.int64)
-        return Plan(g, geo.angles[idx], geo.offsets[idx], None, [int(self.use_offset_correction)])
+        order, sizes, bins = [], [], []
+        B = self.projections_per_batch
+        for views in self.binning.bins:
+            v = [int(i) for i in views]
+            for i in v:
+                if not 0 <= i < geo.angles.size:
+                    raise ValueError("illegal index in bin")
+            first = len(sizes)
+            for k in range(0, len(v), B):
+                sizes.append(len(v[k:k + B]))
+            bins.append((first, len(sizes) - first, len(v)))
+            order += v
+        idx = np.asarray(order, np.int64)
+        plan = Plan(g, geo.angles[idx], geo.offsets[idx], np.asarray(sizes if sizes else [0], np.int32))
+        st = dict(plan=plan, view_index=np.ascontiguousarray(idx, np.int32), bins=bins)
+        self._cache = (key, st)
+        return st
 
-    def mult_M(self, image: np.ndarray, projections: np.ndarray, accumulate=False):
+    def _bin_image(self, image, b):
+        if image.ndim == 4:
+            return image[b]
+        if len(self.binning.bins) != 1:
+            raise ValueError("several bins need a 4-D image (bins, nz, ny, nx)")
+        return image
+
+    def mult_M(self, image, projections, accumulate=False):
         """hoCuConebeamProjectionOperator::mult_M (.cpp:104-176)."""
-        T = torch()
         P, H, W = projections.shape
-        result = np.zeros_like(projections) if accumulate else projections
-        vol3 = image if image.ndim == 3 else None
-        for b, views in enumerate(self.binning.bins):
-            if not views:
+        if P != self.acquisition.geometry.angles.size:
+            raise ValueError("inconsistent sizes of input arrays/vectors")
+        st = self._stream_plan(W, H)
+        result = np.zeros(projections.shape, np.float32) if accumulate else projections
+        offset = int(self.use_offset_correction and not self.use_fbp)
+        for b, (first, nb, n) in enumerate(st["bins"]):
+            if n == 0:
                 continue
-            pl = self._plan(views, W, H)
-            v = T.from_numpy(np.ascontiguousarray(vol3 if vol3 is not None else image[b])).cuda()
-            out = T.empty(pl.proj_shape(), dtype=T.float32, device="cuda")
-            pl.forward(v, out)
-            if self.use_offset_correction and not self.use_fbp:
-                pl.offset_correct(out, -1, 1)
-            result[np.asarray(views, np.int64)] = out.cpu().numpy()
+            vol = self._bin_image(image, b)
+            L.call("cbct_host_forward", st["plan"].handle, first, nb, _host_f32(vol, "image"),
+                   _host_f32(result, "projections"), st["view_index"].ctypes.data, offset, None)
         if accumulate:
             projections += result
         return projections
 
-    def mult_MH(self, projections: np.ndarray, image: np.ndarray, accumulate=False):
+    def mult_MH(self, projections, image, accumulate=False):
         """hoCuConebeamProjectionOperator::mult_MH (.cpp:178-265), FDK when FBP is on."""
-        T = torch()
         P, H, W = projections.shape
-        for b, views in enumerate(self.binning.bins):
-            tgt = image if image.ndim == 3 else image[b]
-            if not views:
-                if not accumulate:
-                    tgt[...] = 0
-                continue
-            pl = self._plan(views, W, H)
-            p = T.from_numpy(np.ascontiguousarray(projections[np.asarray(views, np.int64)])).cuda()
-            out = T.empty(pl.vol_shape, dtype=T.float32, device="cuda")
+        if P != self.acquisition.geometry.angles.size:
+            raise ValueError("inconsistent sizes of input arrays/vectors")
+        st = self._stream_plan(W, H)
+        filt = None if self.frequency_filter is None else self.frequency_filter
+        if filt is not None and filt.size != W + 1:
+            raise ValueError("frequency filter must have W+1 entries")
+        for b, (first, nb, n) in enumerate(st["bins"]):
+            tgt = self._bin_image(image, b)
             if self.use_fbp:
                 flags = (L.CBCT_FDK_PARKER if self.short_scan else 0) | \
                         (L.CBCT_FDK_OFFSET if self.use_offset_correction else 0)
-                pl.fdk(p, out, self.frequency_filter, flags)
-                res = out.cpu().numpy()
-                if accumulate:
-                    tgt *= 2.0 / float(len(views))
-                    tgt += res
-                else:
-                    tgt[...] = res
+                scale = 2.0 / float(n) if n else 1.0
+                L.call("cbct_host_backproject", st["plan"].handle, first, nb, _host_f32(projections, "projections"),
+                       _host_f32(tgt, "image"), st["view_index"].ctypes.data, 1,
+                       None if filt is None else filt.ctypes.data, flags, 0, scale, int(accumulate), None)
             else:
-                if self.use_offset_correction:
-                    pl.offset_correct(p, -1, 1)
-                if accumulate:
-                    out.copy_(T.from_numpy(np.ascontiguousarray(tgt)))
-                pl.backproject(p, out, -1, 0, False, accumulate)
-                tgt[...] = out.cpu().numpy()
+                L.call("cbct_host_backproject", st["plan"].handle, first, nb, _host_f32(projections, "projections"),
+                       _host_f32(tgt, "image"), st["view_index"].ctypes.data, 0, None, 0,
+                       int(self.use_offset_correction), 1.0, int(accumulate), None)
         return image
 
 
@@ -890,23 +954,28 @@ class osSARTSolver:
         return x
 
 
-def fdk_reconstruct_3d(acquisition: CBCT_acquisition, is_dims, is_dims_in_mm, filt=None, binning=None):
-    """The FDK recipe of FDK_reconstruct_3d.cpp:135-161: FDK, then a least-squares
-    rescale s = <A x, p>/<A x, A x>.  Runs on the device; returns a host volume."""
+def fdk_reconstruct_3d(acquisition: CBCT_acquisition, is_dims, is_dims_in_mm, filt=None, binning=None,
+                       projections_per_batch=20):
+    """The FDK recipe of FDK_reconstruct_3d.cpp:135-161 over the host-array
+    operator: FDK (mult_MH with filtered back-projection, streamed in batches of
+    views), the forward projection of the result (mult_M), then the
+    least-squares rescale s = <A x, p> / <A x, A x> (dot products in FP64).
+    Returns the host volume (nz, ny, nx)."""
     T = torch()
     E = hoCuConebeamProjectionOperator()
+    E.set_num_projections_per_batch(projections_per_batch)
+    if binning is not None and binning.get_number_of_bins() > 1:
+        binning = binning.get_3d_binning()
     E.setup(acquisition, binning, is_dims_in_mm, is_dims=is_dims)
     E.set_use_filtered_backprojection(True)
     if filt is not None:
         E.set_frequency_filter(filt)
-    P, H, W = acquisition.projections.shape
-    views = list(range(P))
-    pl = E._plan(views, W, H)
-    p = T.from_numpy(np.ascontiguousarray(acquisition.projections)).cuda()
-    x = T.empty(pl.vol_shape, dtype=T.float32, device="cuda")
-    flags = (L.CBCT_FDK_PARKER if E.short_scan else 0) | (L.CBCT_FDK_OFFSET if E.use_offset_correction else 0)
-    pl.fdk(p, x, E.frequency_filter, flags)
-    tmp = T.empty_like(p)
-    pl.forward(x, tmp)
-    s = (reduce_f64(0, tmp, p) / reduce_f64(0, tmp, tmp)).item()
-    return (x.cpu().numpy() * np.float32(s)).astype(np.float32)
+    p = T.from_numpy(np.ascontiguousarray(acquisition.projections, np.float32)).pin_memory()
+    nx, ny, nz = (int(v) for v in is_dims)
+    x = T.zeros((nz, ny, nx), dtype=T.float32).pin_memory()
+    E.mult_MH(p, x)
+    tmp = T.zeros_like(p).pin_memory()
+    E.mult_M(x, tmp)
+    a = tmp.numpy().astype(np.float64).ravel()
+    s = float(np.dot(a, p.numpy().astype(np.float64).ravel()) / np.dot(a, a))
+    return (x.numpy() * np.float32(s)).astype(np.float32)

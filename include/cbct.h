@@ -211,6 +211,18 @@ CBCT_API cbct_status cbct_fdk_filter_ex(cbct_plan* plan, int32_t s, cbct_dtype p
 CBCT_API cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj, float* vol,
                                  const float* filter, uint32_t flags, float* work, void* stream);
 
+/* Bins (CBCT_binning, xray/CBCT_binning.h:18-172): view_bin gives the bin of
+ * every plan view (n_views ints in [0, n_bins)); within each subset the views
+ * of a bin must be contiguous, the order CBSubsetOperator::setup produces
+ * (each subset sorted by bin, CBSubsetOperator.cpp:86-87).  Volumes then hold
+ * n_bins images (bin-major, nx*ny*nz floats each): cbct_forward projects each
+ * bin's views from that bin's image, cbct_backproject writes each bin's image
+ * from its own views (a bin without views in the call is cleared unless
+ * accumulating), as cuConebeamProjectionOperator does per bin (.cpp:49-116),
+ * and cbct_osmom_solve reconstructs all bins (fp32, without a residual trace).
+ * n_bins <= 1 or view_bin = NULL returns to one bin. */
+CBCT_API cbct_status cbct_plan_set_bins(cbct_plan* plan, int32_t n_bins, const int32_t* view_bin);
+
 /* ----------------------------------------------------------------------------
  * Voxel masks
  * Masks are uint8 arrays of nx*ny*nz voxels (1 = keep), the layout of the
@@ -340,6 +352,38 @@ typedef struct {
  * finished (later work on `stream` is ordered after it).
  * No counterpart in the reference (its drivers reconstruct one scan per process). */
 CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Host-array operators streamed in batches of views
+ *
+ * hoCuConebeamProjectionOperator::mult_M / mult_MH (hoCuConebeamProjectionOperator.cpp:104-265)
+ * over the reference's host-array projectors (conebeam_projection.cu:640-819 and
+ * :1300-1649).  The plan's subsets [s_first, s_first + n_batches) are the batches of
+ * one bin; view_index (n_views ints, plan order) gives each plan view's position in
+ * the host projection array proj_host (W*H*P_acquisition floats, acquisition
+ * order).  The bin's volume (nx*ny*nz floats, host) stays on the device while
+ * the projections pass through two device batch buffers, the copy engine moving
+ * one batch while the kernels run on another.  The work starts after the work
+ * enqueued on `stream`; the calls return once the host outputs are written.
+ * Host arrays should be page-locked for the copies to overlap the kernels.
+ * ------------------------------------------------------------------------- */
+
+/* mult_M of one bin: proj_host[view_index[v]] = A_v vol_host for every view v of
+ * the batches; offset_sqrt = 1 applies the sqrt offset weight to each projected
+ * batch (mult_M without FBP, hoCuConebeamProjectionOperator.cpp:168-169). */
+CBCT_API cbct_status cbct_host_forward(cbct_plan* plan, int32_t s_first, int32_t n_batches, const float* vol_host,
+                                       float* proj_host, const int32_t* view_index, int32_t offset_sqrt,
+                                       void* stream);
+
+/* mult_MH of one bin: vol_host = scale * ((accumulate ? vol_host : 0) + A^T p).
+ * fbp = 1: each batch is FDK-filtered first (cosine, ramp with `filter` or the
+ * default, plus fdk_flags: CBCT_FDK_PARKER, CBCT_FDK_OFFSET) and back-projected
+ * with the 1/U^2 weight, and scale is the bin's 2/P; fbp = 0: the sqrt offset
+ * weight when offset_sqrt = 1, plain back-projection, scale 1 as the reference. */
+CBCT_API cbct_status cbct_host_backproject(cbct_plan* plan, int32_t s_first, int32_t n_batches,
+                                           const float* proj_host, float* vol_host, const int32_t* view_index,
+                                           int32_t fbp, const float* filter, uint32_t fdk_flags,
+                                           int32_t offset_sqrt, float scale, int32_t accumulate, void* stream);
 
 /* ----------------------------------------------------------------------------
  * Serving loop: continuous batching of FDK and OS-MOM reconstructions

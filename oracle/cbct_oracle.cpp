@@ -22,6 +22,7 @@
 // Build: see oracle/build.py (g++ -O3 -fopenmp -shared -fPIC).
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -496,18 +497,40 @@ struct SubsetOp {
   int mode;
   const unsigned char* mask = nullptr;  // apply_mask after mult_MH (cuConebeamProjectionOperator.cpp:113-114)
   const double* weights = nullptr;      // CBSubsetWeightOperator projection weights (all views, subset order)
+  const int* view_bin = nullptr;        // bin of every view (subset order); NULL: one bin
+  int n_bins = 1;
   size_t npx() const { return (size_t)g->W * g->H; }
+  size_t nvox() const { return (size_t)g->nx * g->ny * g->nz; }
   int first(int s) const { int f = 0; for (int i = 0; i < s; ++i) f += sizes[i]; return f; }
+  // Runs of views of one bin inside subset s (a subset is sorted by bin,
+  // CBSubsetOperator.cpp:86-87): (bin, first view, count).
+  std::vector<std::array<int, 3>> runs(int s) const {
+    std::vector<std::array<int, 3>> r;
+    const int f = first(s);
+    for (int i = 0; i < sizes[s];) {
+      const int b = view_bin ? view_bin[f + i] : 0;
+      int n = 1;
+      while (i + n < sizes[s] && (view_bin ? view_bin[f + i + n] : 0) == b) ++n;
+      r.push_back({b, f + i, n});
+      i += n;
+    }
+    return r;
+  }
   // CBSubsetWeightOperator::mult_M (CBSubsetWeightOperator.h:32-43): out = w * (A x).
+  // With bins, each bin's views project that bin's volume
+  // (cuConebeamProjectionOperator.cpp:49-78).
   void M(int s, const double* x, double* out) const {
-    int f = first(s);
-    forward<double, double>(*g, angles + f, offs + 2 * f, sizes[s], spp, mode, x, out, 0);
+    const int f = first(s);
+    for (const auto& run : runs(s))
+      forward<double, double>(*g, angles + run[1], offs + 2 * run[1], run[2], spp, mode, x + nvox() * run[0],
+                              out + npx() * (run[1] - f), 0);
     if (weights)
       for (size_t i = 0; i < npx() * sizes[s]; ++i) out[i] *= weights[npx() * f + i];
   }
   // CBSubsetWeightOperator::mult_MH (.h:44-49): the input times w goes into mult_MH.
+  // With bins, every bin's volume receives its own views (none: 0 or unchanged).
   void MH(int s, const double* in_raw, double* x, int acc) const {
-    int f = first(s);
+    const int f = first(s);
     std::vector<double> wtmp;
     const double* in = in_raw;
     if (weights) {
@@ -515,16 +538,23 @@ struct SubsetOp {
       for (size_t i = 0; i < wtmp.size(); ++i) wtmp[i] *= weights[npx() * f + i];
       in = wtmp.data();
     }
+    std::vector<double> tmp;
     if (offcorr[s]) {
-      std::vector<double> tmp(in, in + npx() * sizes[s]);
+      tmp.assign(in, in + npx() * sizes[s]);
       offset_weight<double>(*g, offs + 2 * f, sizes[s], 0, tmp.data());
-      backproject<double, double>(*g, angles + f, offs + 2 * f, sizes[s], 0, mode, tmp.data(), x, acc);
-    } else {
-      backproject<double, double>(*g, angles + f, offs + 2 * f, sizes[s], 0, mode, in, x, acc);
+      in = tmp.data();
     }
+    std::vector<int> seen(n_bins, 0);
+    for (const auto& run : runs(s)) {
+      double* xb = x + nvox() * run[0];
+      backproject<double, double>(*g, angles + run[1], offs + 2 * run[1], run[2], 0, mode,
+                                  in + npx() * (run[1] - f), xb, acc || seen[run[0]]);
+      seen[run[0]] = 1;
+    }
+    for (int b = 0; b < n_bins; ++b)
+      if (!seen[b] && !acc) std::fill(x + nvox() * b, x + nvox() * (b + 1), 0.0);
     if (mask) {
-      const size_t nv = (size_t)g->nx * g->ny * g->nz;
-      for (size_t i = 0; i < nv; ++i) x[i] *= double(mask[i]);
+      for (size_t i = 0; i < nvox(); ++i) x[i] *= double(mask[i]);
     }
   }
 };
@@ -535,10 +565,18 @@ struct SubsetOp {
 // VERBOSE print of :147-149).  Returns z, the momentum point (:195).
 static const unsigned char* g_solver_mask = nullptr;
 static const double* g_solver_weights = nullptr;
+static const int* g_solver_view_bin = nullptr;
+static int g_solver_bins = 1;
 
 // Mask and projection weights used by the next oracle_osmom / oracle_ossart call (NULL = none).
 void oracle_set_solver_mask(const unsigned char* mask) { g_solver_mask = mask; }
 void oracle_set_solver_weights(const double* w) { g_solver_weights = w; }
+// Bins (CBCT_binning) of the next oracle_osmom call: view_bin per view in
+// subset order (NULL: one bin); images then hold n_bins volumes.
+void oracle_set_solver_bins(int n_bins, const int* view_bin) {
+  g_solver_bins = view_bin ? n_bins : 1;
+  g_solver_view_bin = view_bin;
+}
 
 int oracle_osmom(const Geom* g, const float* angles, const float* offs, const int* sizes,
                  const int* offcorr, int S, double spp, int iters, double beta, double gamma,
@@ -547,7 +585,9 @@ int oracle_osmom(const Geom* g, const float* angles, const float* offs, const in
   SubsetOp A{g, angles, offs, sizes, offcorr, S, spp, 0};
   A.mask = g_solver_mask;
   A.weights = g_solver_weights;
-  const size_t nv = (size_t)g->nx * g->ny * g->nz;
+  A.view_bin = g_solver_view_bin;
+  A.n_bins = g_solver_bins;
+  const size_t nv = (size_t)g->nx * g->ny * g->nz * A.n_bins;
   int P = 0;
   for (int s = 0; s < S; ++s) P += sizes[s];
   std::vector<double> z(nv, 0.0), x, xold, D(nv, 1.0), tmp_img(nv);

@@ -88,6 +88,7 @@ def _declare(L):
     L.oracle_set_num_threads.argtypes = [C.c_int]
     L.oracle_set_solver_mask.argtypes = [C.c_void_p]
     L.oracle_set_solver_weights.argtypes = [C.c_void_p]
+    L.oracle_set_solver_bins.argtypes = [C.c_int, C.c_void_p]
     L.oracle_spacecarver.argtypes = [_GP, _f32, _f32, C.c_int, _f64, C.c_double,
                                      _P(dtype=np.uint8, flags="C_CONTIGUOUS")]
 
@@ -186,12 +187,12 @@ def subset_partition(n_views: int, n_subsets: int, view_bin=None):
     return order[:n], sizes
 
 
-def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonneg, x0, spp, ntrace):
+def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonneg, x0, spp, ntrace, n_bins=1):
     a, o = _views(angles, offsets)
     sizes = np.ascontiguousarray(sizes, dtype=np.int32)
     oc = np.ascontiguousarray(offcorr, dtype=np.int32)
     b = np.ascontiguousarray(b, dtype=np.float64)
-    out = np.zeros((g.nz, g.ny, g.nx), dtype=np.float64)
+    out = np.zeros(((n_bins,) if n_bins > 1 else ()) + (g.nz, g.ny, g.nx), dtype=np.float64)
     trace = np.zeros(ntrace, dtype=np.float64)
     x0p = None
     if x0 is not None:
@@ -203,20 +204,25 @@ def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonne
 
 
 def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
-          x0=None, spp=1.5, mask=None, weights=None):
+          x0=None, spp=1.5, mask=None, weights=None, view_bin=None, n_bins=1):
     """osMOMSolverD::solve (no regulariser); returns (z, per-step ||r||^2).
     mask: optional uint8 voxel mask applied after every mult_MH; weights:
-    optional projection weights of CBSubsetWeightOperator (subset order)."""
+    optional projection weights of CBSubsetWeightOperator (subset order);
+    view_bin: bin of every view (subset order, each subset sorted by bin) for
+    n_bins volumes (z then has shape (n_bins, nz, ny, nx))."""
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    vb = None if view_bin is None else np.ascontiguousarray(view_bin, dtype=np.int32)
     lib().oracle_set_solver_mask(None if m is None else m.ctypes.data)
     lib().oracle_set_solver_weights(None if w is None else w.ctypes.data)
+    lib().oracle_set_solver_bins(int(n_bins), None if vb is None else vb.ctypes.data)
     try:
         return _solver(lib().oracle_osmom, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
-                       nonneg, x0, spp, iters * len(sizes))
+                       nonneg, x0, spp, iters * len(sizes), n_bins if vb is not None else 1)
     finally:
         lib().oracle_set_solver_mask(None)
         lib().oracle_set_solver_weights(None)
+        lib().oracle_set_solver_bins(1, None)
 
 
 def ossart(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,

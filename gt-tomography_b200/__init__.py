@@ -21,7 +21,7 @@ from . import serving  # noqa: F401
 from .serving import Server  # noqa: F401
 from .operators import (  # noqa: F401
     CBCT_acquisition, CBCT_binning, CBCT_geometry, CBSubsetOperator, CBSubsetWeightOperator, Plan, batch_osmom,
-    cuConebeamProjectionOperator,
+    cuConebeamProjectionOperator, cuTVPrimalDualOperator,
     default_frequency_filter, fdk_reconstruct_3d, hann_ramp_filter, hoCuConebeamProjectionOperator,
     osMOMSolverD, osSARTSolver, phantom_voxelize, reduce_f64, subset_partition)
 from . import phantom  # noqa: F401

@@ -53,7 +53,8 @@ class CbctGeometry(C.Structure):
 class CbctSolverParams(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("beta", C.c_float), ("gamma", C.c_float),
                 ("non_negativity", C.c_int32), ("use_graph", C.c_int32), ("storage", C.c_int32),
-                ("refine_every", C.c_int32), ("proj_storage", C.c_int32)]
+                ("refine_every", C.c_int32), ("proj_storage", C.c_int32), ("tv_weight", C.c_float),
+                ("tv_alpha", C.c_float), ("tau", C.c_float), ("reg_steps", C.c_int32)]
 
 
 class CbctBatchItem(C.Structure):

@@ -715,6 +715,10 @@ static cbct_solver_params solver_defaults(const cbct_solver_params* p) {
   d.storage = CBCT_F32;
   d.refine_every = 0;
   d.proj_storage = CBCT_F32;
+  d.tv_weight = 0.f;
+  d.tv_alpha = 0.f;
+  d.tau = 1e-3f;
+  d.reg_steps = 1;
   return p ? *p : d;
 }
 
@@ -736,6 +740,7 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
     const cbct_solver_params prm = solver_defaults(params);
     CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
     if (prm.proj_storage != CBCT_F32) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART takes float projections");
+    if (prm.tv_weight > 0.f) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART has no regulariser (osSARTSolver.h)");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
   });
 }

@@ -19,6 +19,7 @@
 //  kRecip : vol = 1 / max(sum, 1e-6)                                (precon, osMOMSolverD.h:115-120)
 //  kMom   : OS-MOM update of z and xold                              (osMOMSolverD.h:155-175)
 //  kSart  : x = x + step * V * sum, optional clamp                   (osSARTSolver.h:99-104)
+//  kStep  : s = z - step * D * sum, into a separate image            (osMOMSolverD.h:151-157 before denoise)
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -32,12 +33,12 @@ namespace {
 constexpr int kBX = 32, kBY = 4, kZB = 8;
 constexpr int kMaxViewsSmem = 1024;
 
-enum { kStore = 0, kRecip = 1, kMom = 2, kSart = 3 };
+enum { kStore = 0, kRecip = 1, kMom = 2, kSart = 3, kStep = 4 };
 
 struct BpEpi {
   const unsigned char* mask;  // voxel mask applied to the back-projection (nullable)
   float* vol;            // kStore / kRecip output, kSart: x (in/out), kMom: z (in/out)
-  float* xold;           // kMom
+  float* xold;           // kMom; kStep: z (input)
   const float* aux;      // kMom: precon D; kSart: V_s
   float scale;           // kStore: output scale; kMom/kSart: step
   float mom;             // kMom: (told-1)/t
@@ -64,6 +65,8 @@ __device__ __forceinline__ void bp_store(const BpEpi& e, size_t idx, float g) {
     const float xc = e.nonneg ? fmaxf(zt, 0.f) : zt;
     e.vol[idx] = fmaf(-e.mom, e.xold[idx], xc * (1.f + e.mom));
     e.xold[idx] = xc;
+  } else if (EPI == kStep) {
+    e.vol[idx] = fmaf(-e.scale, e.aux[idx] * g, e.xold[idx]);
   } else {  // kSart
     float xn = fmaf(e.scale, e.aux[idx] * g, e.vol[idx]);
     if (e.nonneg) xn = fmaxf(xn, 0.f);
@@ -352,6 +355,7 @@ void prepare_bp_all(size_t smem) {
   prepare_bp_width<kRecip, false, BU>(smem);
   prepare_bp_width<kMom, false, BU>(smem);
   prepare_bp_width<kSart, false, BU>(smem);
+  prepare_bp_width<kStep, false, BU>(smem);
 }
 
 template <int EPI, bool FDK>
@@ -456,6 +460,7 @@ void backproject_prepare(cbct_plan* p) {
   ensure_smem_attr((const void*)bp_kernel<kRecip, false>, smem);
   ensure_smem_attr((const void*)bp_kernel<kMom, false>, smem);
   ensure_smem_attr((const void*)bp_kernel<kSart, false>, smem);
+  ensure_smem_attr((const void*)bp_kernel<kStep, false>, smem);
 }
 
 void backproject_launch(cbct_plan* p, int s, const float* proj, float* vol, int fdk_weight,
@@ -498,6 +503,17 @@ void backproject_sart_launch(cbct_plan* p, int s, const float* proj, float* x, c
   e.scale = step;
   e.nonneg = nonneg;
   launch_bp<kSart, false>(p, s, proj, e, st);
+}
+
+void backproject_step_launch(cbct_plan* p, int s, const float* proj, const float* z, float* out,
+                             const float* precon, float step, cudaStream_t st) {
+  BpEpi e{};
+  e.mask = p->d_mask;
+  e.vol = out;
+  e.xold = const_cast<float*>(z);
+  e.aux = precon;
+  e.scale = step;
+  launch_bp<kStep, false>(p, s, proj, e, st);
 }
 
 }  // namespace cbct

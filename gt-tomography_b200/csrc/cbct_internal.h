@@ -294,6 +294,11 @@ void host_backproject(cbct_plan* p, int s0, int ns, const float* proj_host, floa
                       int fbp, const float* filter, uint32_t fdk_flags, int offset_sqrt, float scale, int accumulate,
                       cudaStream_t caller);
 
+// tv.cu: primal and fused dual + data-resolvent steps of the TV regulariser
+void tv_primal_launch(const float* x, float* P, int nx, int ny, int nz, float scale, cudaStream_t st);
+void tv_update_launch(const float* P, float* x, const float* s, const float* D, int nx, int ny, int nz, float w,
+                      float tau, float tau_lambda, cudaStream_t st);
+
 // mask.cu
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,
                         cudaStream_t st);

@@ -35,6 +35,8 @@ void backproject_mom_launch(cbct_plan* p, int s, const float* proj, float* z, fl
                             const float* precon, float step, float mom, int nonneg, cudaStream_t st);
 void backproject_sart_launch(cbct_plan* p, int s, const float* proj, float* x, const float* V,
                              float step, int nonneg, cudaStream_t st);
+void backproject_step_launch(cbct_plan* p, int s, const float* proj, const float* z, float* out,
+                             const float* precon, float step, cudaStream_t st);
 
 namespace {
 
@@ -310,6 +312,90 @@ static void run_osmom_bins(cbct_plan* p, const float* b, const float* x0, float*
   }
 }
 
+// osMOMSolverD with a total-variation regulariser (osMOMSolverD.h:82-196 with
+// denoise, :205-247): after the gradient step s = z - step D A^T r, reg_steps
+// primal-dual steps move the momentum point toward s under the TV prior
+// (cuTVPrimalDualOperator with weight 1 after the solver's normalisation by
+// avg_lambda = tv_weight; updateG with avg_lambda), then the clamp and the
+// momentum step.  Works on one bin or several (each bin's TV is 3-D).
+static void run_osmom_tv(cbct_plan* p, const float* b, const float* x0, float* z, const cbct_solver_params& prm,
+                         float* xold, float* D, float* r, float* sbuf, float* P, double* asum_dev, cudaStream_t st) {
+  const size_t nv = vol_elems(p), pl = plane_elems(p);
+  const int S = p->n_subsets, NB = p->n_bins;
+  const size_t nall = nv * NB;
+  const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz;
+  std::vector<std::vector<int>> segs(S);
+  for (int s = 0; s < S; ++s) {
+    if (NB == 1) segs[s].push_back(s);
+    else
+      for (int k = p->seg_begin[s]; k < p->seg_end[s]; ++k) segs[s].push_back(k);
+  }
+  auto bin_of = [&](int k) { return NB == 1 ? 0 : p->seg_bin[k]; };
+  // D = 1/max(A^T (W A 1), 1e-6), per bin.
+  fill_launch(xold, nv, 1.f, st);
+  for (int s = 0; s < S; ++s)
+    for (int k : segs[s])
+      forward_launch_ex(p, k, CBCT_F32, xold, r + pl * p->first[k], nullptr, nullptr, 1.f, 1, p->offcorr[k], 0,
+                        nullptr, st);
+  CBCT_CUDA(cudaMemsetAsync(D, 0, nall * sizeof(float), st));
+  for (int s = 0; s < S; ++s)
+    for (int k : segs[s]) backproject_launch(p, k, r + pl * p->first[k], D + nv * bin_of(k), 0, 1, 1.f, st);
+  recip_launch(D, nall, st);
+  // denoise's gam needs asum(D) on the host (osMOMSolverD.h:206).
+  reduce_launch(2, D, nullptr, nall, p->d_partials, p->n_partials, asum_dev, st);
+  double asum = 0.0;
+  CBCT_CUDA(cudaMemcpyAsync(&asum, asum_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CBCT_CUDA(cudaStreamSynchronize(st));
+  const float lambda = prm.tv_weight;
+  const float gam = 0.35f / lambda / (float(nall) / float(asum));
+  if (x0) {
+    CBCT_CUDA(cudaMemcpyAsync(z, x0, nall * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CBCT_CUDA(cudaMemcpyAsync(xold, x0, nall * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  } else {
+    CBCT_CUDA(cudaMemsetAsync(z, 0, nall * sizeof(float), st));
+    CBCT_CUDA(cudaMemsetAsync(xold, 0, nall * sizeof(float), st));
+  }
+  std::vector<int> seg_of_bin(NB);
+  double t = 1.0, told = 1.0;
+  for (int it = 0; it < prm.iterations; ++it) {
+    for (int s = 0; s < S; ++s) {
+      t = 0.5 * (1.0 + std::sqrt(1.0 + 4.0 * t * t));
+      std::fill(seg_of_bin.begin(), seg_of_bin.end(), -1);
+      for (int k : segs[s]) {
+        seg_of_bin[bin_of(k)] = k;
+        forward_launch_ex(p, k, CBCT_F32, z + nv * bin_of(k), r + pl * p->first[k], b + pl * p->first[k], nullptr,
+                          1.f, 1, p->offcorr[k], 0, nullptr, st);
+      }
+      const double stepsz = double(prm.beta) / (1.0 + double(prm.gamma) * it) * S;
+      const double mom = (told - 1.0) / t;
+      for (int bb = 0; bb < NB; ++bb) {
+        const int k = seg_of_bin[bb];
+        if (k >= 0)
+          backproject_step_launch(p, k, r + pl * p->first[k], z + nv * bb, sbuf + nv * bb, D + nv * bb,
+                                  float(stepsz), st);
+        else
+          CBCT_CUDA(cudaMemcpyAsync(sbuf + nv * bb, z + nv * bb, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      }
+      // denoise (osMOMSolverD.h:205-231): L = 4, sigma = 1/(tau L^2), tau and
+      // sigma rescaled by theta = 1/sqrt(1 + 2 gam tau) after every step.
+      float tau = prm.tau, sigma = 1.f / (tau * 4.f * 4.f);
+      for (int rs = 0; rs < prm.reg_steps; ++rs) {
+        const float scale = (1.f * sigma) / (1.f + sigma * prm.tv_alpha);
+        for (int bb = 0; bb < NB; ++bb) {
+          tv_primal_launch(z + nv * bb, P, nx, ny, nz, scale, st);
+          tv_update_launch(P, z + nv * bb, sbuf + nv * bb, D + nv * bb, nx, ny, nz, 1.f, tau, tau / lambda, st);
+        }
+        const float theta = 1.f / std::sqrt(1.f + 2.f * gam * tau);
+        tau *= theta;
+        sigma /= theta;
+      }
+      // clamp and momentum: the update kernel with no gradient
+      osmom_update_launch(z, xold, D, nullptr, nall, 0.f, float(mom), prm.non_negativity, st);
+      told = t;
+    }
+  }
+}
+
 static void run_ossart(cbct_plan* p, const float* b, const float* x0, float* x, const cbct_solver_params& prm,
                        double* cost, float* Wp, float* r, float* V, cudaStream_t st) {
   const size_t nv = vol_elems(p);
@@ -403,6 +489,19 @@ void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const c
                  double* resid, cudaStream_t st) {
   CBCT_REQUIRE(prm.proj_storage == CBCT_F32 || prm.proj_storage == CBCT_F16 || prm.proj_storage == CBCT_BF16,
                "unknown projection storage type");
+  if (prm.tv_weight > 0.f) {
+    if (prm.storage != CBCT_F32 || prm.proj_storage != CBCT_F32 || resid)
+      throw Error(CBCT_ERR_UNSUPPORTED, "regularised OS-MOM: fp32 storage, no residual trace");
+    CBCT_REQUIRE(prm.tau > 0.f && prm.reg_steps >= 0, "regularised OS-MOM needs tau > 0 and reg_steps >= 0");
+    const size_t nv = vol_elems(p), nall = nv * p->n_bins;
+    const size_t need = 3 * nall + proj_elems(p) + 3 * nv + 4;
+    float* ws = workspace(p, need);
+    float* tail = ws + 3 * nall + proj_elems(p) + 3 * nv;
+    double* asum_dev = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(tail) + 7) & ~uintptr_t(7));
+    run_osmom_tv(p, static_cast<const float*>(b), x0, z, prm, ws, ws + nall, ws + 2 * nall,
+                 ws + 2 * nall + proj_elems(p), ws + 3 * nall + proj_elems(p), asum_dev, st);
+    return;
+  }
   if (p->n_bins > 1) {
     if (prm.storage != CBCT_F32 || prm.proj_storage != CBCT_F32 || resid)
       throw Error(CBCT_ERR_UNSUPPORTED, "binned OS-MOM: fp32 storage, no residual trace");

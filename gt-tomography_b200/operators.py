@@ -355,13 +355,17 @@ class Plan:
         return out
 
     def osmom(self, b, z_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
-              storage=L.CBCT_F32, refine_every=0, resid=None, stream=None):
+              storage=L.CBCT_F32, refine_every=0, resid=None, stream=None, tv_weight=0.0, tv_alpha=0.0,
+              tau=1e-3, reg_steps=1):
         """osMOMSolverD::solve on the device.  storage: type of the forward
         projector's volume input (16-bit shadow of z); b may be float32,
-        float16 or bfloat16 (its storage type is taken from the tensor)."""
+        float16 or bfloat16 (its storage type is taken from the tensor).
+        tv_weight > 0: TV regularisation (a cuTVPrimalDualOperator(tv_alpha) of
+        that weight, the solver's tau and reg_steps)."""
         bt = _storage_of(b, self.proj_shape(-1), "b")
         prm = L.CbctSolverParams(int(iterations), float(beta), float(gamma), int(nonneg), int(use_graph),
-                                 int(storage), int(refine_every), bt)
+                                 int(storage), int(refine_every), bt, float(tv_weight), float(tv_alpha), float(tau),
+                                 int(reg_steps))
         L.call("cbct_osmom_solve", self._h, _ptr(b), _ptr(x0), _ptr(z_out), C.byref(prm), _ptr(resid),
                _stream(stream))
         return z_out
@@ -851,8 +855,27 @@ class hoCuConebeamProjectionOperator:
 
 
 # ----------------------------------------------------------------- solvers
+class cuTVPrimalDualOperator:
+    """Total-variation regulariser of osMOMSolverD
+    (operators/cuTVPrimalDualOperator.{h,cu}): periodic forward differences
+    projected onto the unit ball; alpha as the reference's constructor
+    argument, the weight via set_weight.  Evaluated on the device inside
+    cbct_osmom_solve."""
+
+    def __init__(self, alpha: float = 0.0):
+        self.alpha = float(alpha)
+        self.weight = 1.0
+
+    def set_weight(self, w: float):
+        self.weight = float(w)
+
+    def get_weight(self) -> float:
+        return self.weight
+
+
 class osMOMSolverD:
-    """osMOMSolverD<cuNDArray<float>> without regularisers (solvers/osMOMSolverD.h:19-329).
+    """osMOMSolverD<cuNDArray<float>> (solvers/osMOMSolverD.h:19-329), unregularised
+    or with one cuTVPrimalDualOperator.
 
     solve() runs the whole loop on the device (cbct_osmom_solve).  The
     per-iteration dump files of the reference (:184-189) are not written;
@@ -869,6 +892,21 @@ class osMOMSolverD:
         self.storage = L.CBCT_F32
         self.refine_every = 0
         self.residual_norms = None
+        self.regularizers = []
+        self.tau = 1e-3          # osMOMSolverD.h:33
+        self.reg_steps = 1       # :29
+        self.huber = 0.0
+
+    def set_tau(self, tau):
+        self.tau = float(tau)
+
+    def set_reg_steps(self, n):
+        self.reg_steps = int(n)
+
+    def set_huber(self, h):
+        """denoise_alpha of the solver's linear-operator regularisers; the TV
+        operator takes its own alpha."""
+        self.huber = float(h)
 
     def set_max_iterations(self, i):
         self._iterations = int(i)
@@ -894,8 +932,14 @@ class osMOMSolverD:
     def set_encoding_operator(self, E):
         self.E = E
 
-    def add_regularization_operator(self, *a, **k):
-        raise NotImplementedError("regularised OS-MOM is outside this build's scope")
+    def add_regularization_operator(self, op):
+        """osMOMSolverD::add_regularization_operator (.h:48-54); this build
+        takes one cuTVPrimalDualOperator."""
+        if not isinstance(op, cuTVPrimalDualOperator):
+            raise NotImplementedError("only cuTVPrimalDualOperator regularisation is built")
+        if self.regularizers:
+            raise NotImplementedError("one regulariser per solver in this build")
+        self.regularizers.append(op)
 
     def solve(self, projections):
         T = torch()
@@ -907,8 +951,13 @@ class osMOMSolverD:
         z = T.empty(E.plan.vol_shape, dtype=T.float32, device=projections.device)
         S = E.get_number_of_subsets()
         self.residual_norms = T.zeros(self._iterations * S, dtype=T.float64, device=projections.device)
+        tv = self.regularizers[0] if self.regularizers else None
+        if tv is not None:
+            self.residual_norms = None   # the regularised solve keeps no residual trace
         E.plan.osmom(projections, z, self.x0, self._iterations, self._beta, self._gamma, self.non_negativity,
-                     self.use_graph, self.storage, self.refine_every, self.residual_norms)
+                     self.use_graph, self.storage, self.refine_every, self.residual_norms,
+                     tv_weight=0.0 if tv is None else tv.weight, tv_alpha=0.0 if tv is None else tv.alpha,
+                     tau=self.tau, reg_steps=self.reg_steps)
         return z
 
 

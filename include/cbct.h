@@ -310,6 +310,16 @@ typedef struct {
   cbct_dtype storage;      /* storage type of the forward projector's volume input */
   int32_t refine_every;    /* mixed precision: FP32 forward every n iterations (0 = never) */
   cbct_dtype proj_storage; /* storage type of the measured projections b (OS-MOM); the residual stays FP32 */
+  /* OS-MOM total-variation regularisation (osMOMSolverD with a cuTVPrimalDualOperator:
+   * denoise and updateG of osMOMSolverD.h:205-247, operators/cuTVPrimalDualOperator.cu;
+   * the updateG that osMOMSolverD<cuNDArray<float>> runs): tv_weight > 0 turns
+   * it on (the operator's weight), tv_alpha is its alpha, tau the solver's tau
+   * (reference default 1e-3), reg_steps its primal-dual steps per subset step
+   * (reference default 1).  Regularised solves run eagerly (use_graph ignored). */
+  float tv_weight;
+  float tv_alpha;
+  float tau;
+  int32_t reg_steps;
 } cbct_solver_params;
 
 /* osMOMSolverD<cuNDArray<float>>::solve without regularisers

@@ -571,6 +571,65 @@ static int g_solver_bins = 1;
 // Mask and projection weights used by the next oracle_osmom / oracle_ossart call (NULL = none).
 void oracle_set_solver_mask(const unsigned char* mask) { g_solver_mask = mask; }
 void oracle_set_solver_weights(const double* w) { g_solver_weights = w; }
+// Total-variation regularisation of the next oracle_osmom call (weight 0: none):
+// osMOMSolverD with one cuTVPrimalDualOperator(alpha) of this weight, the
+// solver's tau and reg_steps.
+static double g_tv_weight = 0.0, g_tv_alpha = 0.0, g_tv_tau = 1e-3;
+static int g_tv_steps = 1;
+void oracle_set_solver_tv(double weight, double alpha, double tau, int reg_steps) {
+  g_tv_weight = weight;
+  g_tv_alpha = alpha;
+  g_tv_tau = tau;
+  g_tv_steps = reg_steps;
+}
+
+// denoise of osMOMSolverD.h:205-231 with one TV operator, whose weight the
+// solver normalises to 1 (avg_lambda = the weight, :124-126): primal-dual steps
+// from x toward s.  The TV primal step (operators/cuTVPrimalDualOperator.cu:9-37)
+// takes periodic forward differences, scales them by sigma / (1 + sigma alpha)
+// and projects each gradient vector onto the unit ball; the dual step (:40-62)
+// adds the negative divergence; updateG (osMOMSolverD.h:233-247, the generic
+// version that osMOMSolverD<cuNDArray<float>> runs) resolves the
+// preconditioned data term.  Every bin is a separate 3-D image.
+static void tv_denoise(const Geom* g, int n_bins, std::vector<double>& x, const std::vector<double>& s,
+                       const std::vector<double>& D, double lambda, double alpha, double tau0, int steps, double gam) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const size_t nv = (size_t)nx * ny * nz;
+  double tau = tau0, sigma = 1.0 / (tau * 4.0 * 4.0);
+  std::vector<double> P(3 * nv);
+  auto at = [&](int i, int j, int k) { return ((size_t)k * ny + j) * nx + i; };
+  for (int it = 0; it < steps; ++it) {
+    const double scale = sigma / (1.0 + sigma * alpha);
+    for (int b = 0; b < n_bins; ++b) {
+      double* xb = x.data() + nv * b;
+      const double* sb = s.data() + nv * b;
+      const double* Db = D.data() + nv * b;
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i < nx; ++i) {
+            const size_t c = at(i, j, k);
+            const double v = xb[c];
+            double d[3] = {(xb[at((i + 1) % nx, j, k)] - v) * scale, (xb[at(i, (j + 1) % ny, k)] - v) * scale,
+                           (xb[at(i, j, (k + 1) % nz)] - v) * scale};
+            const double m = std::max(1.0, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+            for (int a = 0; a < 3; ++a) P[a * nv + c] = d[a] / m;
+          }
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i < nx; ++i) {
+            const size_t c = at(i, j, k);
+            const double gv = (P[at((i + nx - 1) % nx, j, k)] - P[c]) +
+                              (P[nv + at(i, (j + ny - 1) % ny, k)] - P[nv + c]) +
+                              (P[2 * nv + at(i, j, (k + nz - 1) % nz)] - P[2 * nv + c]);
+            xb[c] = ((xb[c] - tau * gv) + tau / lambda * (sb[c] / Db[c])) / ((1.0 / Db[c]) * (tau / lambda) + 1.0);
+          }
+    }
+    const double theta = 1.0 / std::sqrt(1.0 + 2.0 * gam * tau);
+    tau *= theta;
+    sigma /= theta;
+  }
+}
+
 // Bins (CBCT_binning) of the next oracle_osmom call: view_bin per view in
 // subset order (NULL: one bin); images then hold n_bins volumes.
 void oracle_set_solver_bins(int n_bins, const int* view_bin) {
@@ -600,6 +659,9 @@ int oracle_osmom(const Geom* g, const float* angles, const float* offs, const in
   std::vector<double> pre(nv, 0.0);
   for (int s = 0; s < S; ++s) A.MH(s, proj.data() + A.npx() * A.first(s), pre.data(), 1);
   for (size_t i = 0; i < nv; ++i) D[i] = 1.0 / std::max(pre[i], 1e-6);
+  double asum_D = 0;
+  for (size_t i = 0; i < nv; ++i) asum_D += std::fabs(D[i]);
+  const double gam = g_tv_weight > 0 ? 0.35 / g_tv_weight / (double(nv) / asum_D) : 0.0;
   double t = 1, told = 1;
   int step = 0;
   for (int it = 0; it < iters; ++it) {
@@ -614,7 +676,10 @@ int oracle_osmom(const Geom* g, const float* angles, const float* offs, const in
       A.MH(s, r, tmp_img.data(), 0);
       const double a = -beta / (1 + gamma * it) * S;
       for (size_t i = 0; i < nv; ++i) z[i] += a * (tmp_img[i] * D[i]);
-      x = z;                                            // denoise: x = z (:211-213)
+      if (g_tv_weight > 0)                              // denoise with the TV prior
+        tv_denoise(g, A.n_bins, x, z, D, g_tv_weight, g_tv_alpha, g_tv_tau, g_tv_steps, gam);
+      else
+        x = z;                                          // denoise: x = z (:211-213)
       if (nonneg) for (auto& e : x) e = std::max(e, 0.0);
       const double m = (told - 1) / t;
       for (size_t i = 0; i < nv; ++i) z[i] = x[i] * (1 + m) - m * xold[i];

@@ -114,7 +114,8 @@ _LAYOUT_PROBE = r"""
 int main(void) {
   S(cbct_geometry) S(cbct_solver_params) S(cbct_batch_item) S(cbct_server_config) S(cbct_request)
   S(cbct_request_info)
-  F(cbct_solver_params, proj_storage) F(cbct_batch_item, params) F(cbct_batch_item, resid_norm2_out)
+  F(cbct_solver_params, proj_storage) F(cbct_solver_params, reg_steps) F(cbct_batch_item, params)
+  F(cbct_batch_item, resid_norm2_out)
   F(cbct_server_config, device) F(cbct_request, geometry) F(cbct_request, angles_deg)
   F(cbct_request, proj_host) F(cbct_request, params) F(cbct_request, filter) F(cbct_request, offset_correction)
   F(cbct_request_info, t_submit) F(cbct_request_info, bytes_peak) F(cbct_request_info, message)

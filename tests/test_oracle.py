@@ -304,3 +304,62 @@ def test_binned_osmom_is_per_bin(O, gtb):
         sz = [int(keep[f:f + n].sum()) for f, n in zip(first, sizes)]
         z1, _ = O.osmom(g, bb[keep], a[keep], o[keep], sz, np.zeros(3, np.int32), iters=2, nonneg=True)
         assert np.array_equal(z2[sel], z1)
+
+
+def test_tv_osmom_vs_numpy(O):
+    """The TV-regularised osMOMSolverD (denoise and updateG, osMOMSolverD.h:205-247,
+    with cuTVPrimalDualOperator.cu:9-62) restated in numpy over the oracle's
+    projectors; the periodic differences use np.roll."""
+    case = make("cube")
+    g = case.oracle_geom(O)
+    rng = np.random.default_rng(7)
+    truth = np.zeros((case.nz, case.ny, case.nx))
+    truth[8:24, 10:22, 6:26] = 0.02
+    order, sizes = O.subset_partition(case.angles.size, 3)
+    a, o = case.angles[order], case.offsets[order]
+    b = O.forward(g, truth, a, o) + rng.normal(0, 2e-3, (a.size, case.H, case.W))
+    first = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    S, iters, lam, alpha, tau0, steps = 3, 2, 0.05, 0.1, 1e-3, 2
+
+    def M(s, x):
+        f, n = first[s], sizes[s]
+        return O.forward(g, x, a[f:f + n], o[f:f + n])
+
+    def MH(s, y):
+        f, n = first[s], sizes[s]
+        return O.backproject(g, y, a[f:f + n], o[f:f + n])
+
+    def denoise(x, sv, D, gam):
+        tau, sigma = tau0, 1.0 / (tau0 * 16.0)
+        for _ in range(steps):
+            scale = sigma / (1.0 + sigma * alpha)
+            d = np.stack([(np.roll(x, -1, axis=ax) - x) * scale for ax in (2, 1, 0)])
+            P = d / np.maximum(1.0, np.sqrt((d * d).sum(axis=0)))
+            gv = sum(np.roll(P[i], 1, axis=ax) - P[i] for i, ax in enumerate((2, 1, 0)))
+            x = ((x - tau * gv) + tau / lam * (sv / D)) / ((1.0 / D) * (tau / lam) + 1.0)
+            theta = 1.0 / math.sqrt(1.0 + 2.0 * gam * tau)
+            tau, sigma = tau * theta, sigma / theta
+        return x
+
+    ones = np.ones_like(truth)
+    pre = sum(MH(s, M(s, ones)) for s in range(S))
+    D = 1.0 / np.maximum(pre, 1e-6)
+    gam = 0.35 / lam / (D.size / np.abs(D).sum())
+    z = np.zeros_like(truth)
+    x, xold = z.copy(), z.copy()
+    t = told = 1.0
+    for it in range(iters):
+        for s in range(S):
+            t = 0.5 * (1 + math.sqrt(1 + 4 * t * t))
+            r = M(s, x) - b[first[s]:first[s] + sizes[s]]
+            z = z - S * (MH(s, r) * D)
+            x = np.maximum(denoise(x, z, D, gam), 0)
+            z = x * (1 + (told - 1) / t) - (told - 1) / t * xold
+            x, xold = xold, x
+            x = z.copy()
+            told = t
+    zo, _ = O.osmom(g, b, a, o, sizes, np.zeros(S, np.int32), iters=iters, nonneg=True, tv_weight=lam,
+                    tv_alpha=alpha, tau=tau0, reg_steps=steps)
+    assert np.max(np.abs(zo - z)) <= 1e-9 * max(1.0, np.max(np.abs(z)))
+    plain, _ = O.osmom(g, b, a, o, sizes, np.zeros(S, np.int32), iters=iters, nonneg=True)
+    assert np.max(np.abs(plain - z)) > 1e-6   # the prior does change the result

@@ -1,6 +1,6 @@
 """Benchmark of the cone-beam OS-MOM hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c4|c5]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5]
 
 Workload (default, c2): OS-MOM reconstruction (osMOMSolverD semantics,
 positivity, no regulariser) of a 256^3 seeded ellipsoid phantom from 360
@@ -565,6 +565,122 @@ def batched(args):
     print(json.dumps(line), flush=True)
 
 
+def mixed_precision(args):
+    """Mixed-precision OS-MOM (the north star's third configuration): a 512^3
+    phantom of 10 seeded ellipsoids plus 2000 small spheres (radius 0.5..2 mm,
+    density up to 0.5/mm), 0.5 mm voxels (assumed), 720 views of 1024x768 at
+    0.4 mm, Poisson noise at I0 = 5e4, 10 subsets x 20 iterations, positivity.
+    Solved with fp32, bf16 and fp16 storage (16-bit: the measured projections
+    and the forward projector's volume input; FP32 interpolation and
+    accumulation, FP64 norms; the forward reads the FP32 image every 5th
+    iteration).  Timed with CUDA events; the 16-bit results are compared with
+    the fp32 result.  The per-iteration error against FP64 is measured on the
+    same scene at a quarter of the resolution (128^3 at 2 mm, 180 views of
+    256x192 at 1.6 mm), where the FP64 oracle finishes on the host: z after
+    iteration k of the device solve (a k-iteration solve, the same
+    computation prefix) against the oracle's z after iteration k."""
+    import torch
+    gtb = _package()
+    L = gtb._lib
+    dev = torch.device("cuda", 0)
+    seed, iters, S = 4321, args.c3_iters, 10
+    half = 128.0  # mm, half the volume
+    ell = gtb.phantom.ellipsoids(seed, (2 * half,) * 3, n=10, n_spheres=2000)
+    ell_d = torch.from_numpy(ell.reshape(-1)).to(dev)
+
+    def problem(n, P, W, H, pitch, I0):
+        g = L.CbctGeometry(1000.0, 1500.0, W * pitch, H * pitch, W, H, n, n, n, 2 * half, 2 * half, 2 * half, 1.5)
+        ang = gtb.phantom.circular_orbit(P)
+        order, sizes = gtb.subset_partition(P, S)
+        a = ang[order].copy()
+        o = np.zeros((P, 2), np.float32)
+        plan = gtb.Plan(g, a, o, sizes, np.zeros(S, np.int32))
+        exact = torch.empty(plan.proj_shape(), dtype=torch.float32, device=dev)
+        plan.phantom_project(ell_d, exact)
+        b = gtb.phantom.poisson_log(exact, I0, seed + 1).contiguous()
+        return g, a, o, sizes, plan, b
+
+    storages = [("fp32", torch.float32, L.CBCT_F32), ("bf16", torch.bfloat16, L.CBCT_BF16),
+                ("fp16", torch.float16, L.CBCT_F16)]
+
+    def solve(plan, b, dt, code, k, z):
+        bt = b if dt == torch.float32 else b.to(dt).contiguous()
+        plan.osmom(bt, z, None, k, nonneg=True, use_graph=True, storage=code, refine_every=5)
+
+    # full size
+    g, a, o, sizes, plan, b = problem(512, 720, 1024, 768, 0.4, 5e4)
+    clocks = ClockSampler(0)
+    clocks.start()
+    results, times = {}, {}
+    for name, dt, code in storages:
+        z = torch.empty(plan.vol_shape, dtype=torch.float32, device=dev)
+        solve(plan, b, dt, code, 1, z)          # warm-up: kernels, graph capture
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solve(plan, b, dt, code, iters, z)
+        e1.record()
+        e1.synchronize()
+        times[name] = e0.elapsed_time(e1)
+        results[name] = z.cpu()
+    clk = clocks.stop()
+    ref = results["fp32"].double()
+    rel_vs_fp32 = {k: float((v.double() - ref).norm() / ref.norm()) for k, v in results.items() if k != "fp32"}
+    n_upd = (iters + 1) * (1024 * 768 * 720 * int(np.float32(1.5) * np.float32(512)) + 512 ** 3 * 720)
+    plan.close()
+    del results, b
+    torch.cuda.empty_cache()
+    # quarter resolution against the FP64 oracle, per iteration
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    O.set_num_threads(os.cpu_count() or 1)
+    g2, a2, o2, sizes2, plan2, b2 = problem(128, 180, 256, 192, 1.6, 5e4)
+    og = O.Geometry(128, 128, 128, 2 * half, 2 * half, 2 * half, 256, 192, 256 * 1.6, 192 * 1.6, 1000.0, 1500.0)
+    snaps = np.zeros((iters, 128, 128, 128), np.float64)
+    t0 = time.perf_counter()
+    O.osmom(og, b2.double().cpu().numpy(), a2, o2, sizes2, np.zeros(S, np.int32), iters=iters, nonneg=True,
+            snapshots=snaps)
+    oracle_s = time.perf_counter() - t0
+    per_iter = {}
+    for name, dt, code in storages:
+        errs = []
+        z = torch.empty(plan2.vol_shape, dtype=torch.float32, device=dev)
+        for k in range(1, iters + 1):
+            solve(plan2, b2, dt, code, k, z)
+            ref_k = snaps[k - 1]
+            errs.append(float(np.linalg.norm(z.cpu().numpy().astype(np.float64) - ref_k) / np.linalg.norm(ref_k)))
+        per_iter[name] = [float(f"{e:.3e}") for e in errs]
+    # the plain FP32 path (the reference's structure: texture weights, per-call copies) for context
+    import ctypes as C
+    errs = []
+    bt2 = b2.contiguous()
+    zp = torch.empty(plan2.vol_shape, dtype=torch.float32, device=dev)
+    ap2, op2 = np.ascontiguousarray(a2, np.float32), np.ascontiguousarray(o2, np.float32)
+    sz2, oc2 = np.ascontiguousarray(sizes2, np.int32), np.zeros(S, np.int32)
+    for k in range(1, iters + 1):
+        L.call("cbct_plain_osmom_solve", C.byref(g2), ap2.ctypes.data, op2.ctypes.data, ap2.size, sz2.ctypes.data, S,
+               oc2.ctypes.data, bt2.data_ptr(), zp.data_ptr(), k, 1, None)
+        ref_k = snaps[k - 1]
+        errs.append(float(np.linalg.norm(zp.cpu().numpy().astype(np.float64) - ref_k) / np.linalg.norm(ref_k)))
+    per_iter["plain_fp32_path"] = [float(f"{e:.3e}") for e in errs]
+    ms = times["bf16"]
+    line = {"metric": "mixed-precision OS-MOM recon/s (512^3, 720 views)", "value": round(1e3 / ms, 4),
+            "unit": "recon/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": round(ms, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 storage, f32 compute",
+            "data": "synthetic",
+            "config": {"workload": "osmom 512^3 (0.5 mm, assumed) from 720 views 1024x768@0.4mm, I0=5e4, "
+                                   f"10 ellipsoids + 2000 spheres, {S} subsets x {iters} iterations, positivity",
+                       "storage": "projections and forward volume input 16-bit; FP32 forward every 5th iteration",
+                       "assumed": ["voxel_mm", "SAD_mm", "SDD_mm"]},
+            "ms_per_reconstruction": {k: round(v, 1) for k, v in times.items()},
+            "gups": {k: round(n_upd / (v * 1e-3) / 1e9, 1) for k, v in times.items()},
+            "rel_l2_vs_fp32_storage": {k: float(f"{v:.3e}") for k, v in rel_vs_fp32.items()},
+            "per_iteration_rel_l2_vs_fp64_quarter_scale": per_iter,
+            "fp64_oracle_seconds": round(oracle_s, 1), "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def _scan_host(gtb, sp, dev, I0=1e5):
     """One seeded scan of the batched shapes: geometry, acquisition-order
     angles/offsets and noisy log projections (pinned float32 host tensor)."""
@@ -725,10 +841,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c4", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
     ap.add_argument("--scans", type=int, default=64, help="c4: number of scans")
     ap.add_argument("--streams", type=int, default=8, help="c4: streams of the batch executor")
     ap.add_argument("--requests", type=int, default=32, help="c5: requests in the arrival stream")
+    ap.add_argument("--c3-iters", type=int, default=20, help="c3: OS-MOM iterations")
     ap.add_argument("--rate", type=float, default=20.0, help="c5: Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=4, help="c5: request slots of the server")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="c5: HBM budget of the server")
@@ -743,6 +860,9 @@ def main():
         return
     if args.config == "c5":
         served(args)
+        return
+    if args.config == "c3":
+        mixed_precision(args)
         return
     wl = Workload(args.config)
     if args.only:

@@ -630,6 +630,11 @@ static void tv_denoise(const Geom* g, int n_bins, std::vector<double>& x, const 
   }
 }
 
+// Per-iteration copies of z from the next oracle_osmom call (iters * images
+// doubles; NULL: none).
+static double* g_solver_snapshots = nullptr;
+void oracle_set_solver_snapshots(double* buf) { g_solver_snapshots = buf; }
+
 // Bins (CBCT_binning) of the next oracle_osmom call: view_bin per view in
 // subset order (NULL: one bin); images then hold n_bins volumes.
 void oracle_set_solver_bins(int n_bins, const int* view_bin) {
@@ -687,6 +692,7 @@ int oracle_osmom(const Geom* g, const float* angles, const float* offs, const in
       x = z;
       told = t;
     }
+    if (g_solver_snapshots) std::copy(z.begin(), z.end(), g_solver_snapshots + (size_t)it * nv);
   }
   std::copy(z.begin(), z.end(), z_out);
   return 0;

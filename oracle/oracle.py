@@ -90,6 +90,7 @@ def _declare(L):
     L.oracle_set_solver_weights.argtypes = [C.c_void_p]
     L.oracle_set_solver_bins.argtypes = [C.c_int, C.c_void_p]
     L.oracle_set_solver_tv.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int]
+    L.oracle_set_solver_snapshots.argtypes = [C.c_void_p]
     L.oracle_spacecarver.argtypes = [_GP, _f32, _f32, C.c_int, _f64, C.c_double,
                                      _P(dtype=np.uint8, flags="C_CONTIGUOUS")]
 
@@ -206,14 +207,15 @@ def _solver(fn, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma, nonne
 
 def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,
           x0=None, spp=1.5, mask=None, weights=None, view_bin=None, n_bins=1, tv_weight=0.0, tv_alpha=0.0,
-          tau=1e-3, reg_steps=1):
+          tau=1e-3, reg_steps=1, snapshots=None):
     """osMOMSolverD::solve (no regulariser); returns (z, per-step ||r||^2).
     mask: optional uint8 voxel mask applied after every mult_MH; weights:
     optional projection weights of CBSubsetWeightOperator (subset order);
     view_bin: bin of every view (subset order, each subset sorted by bin) for
     n_bins volumes (z then has shape (n_bins, nz, ny, nx)); tv_weight > 0: the
     TV-regularised solver (one cuTVPrimalDualOperator(tv_alpha) of that weight,
-    the solver's tau and reg_steps)."""
+    the solver's tau and reg_steps); snapshots: float64 array of shape
+    (iters,) + z.shape that receives z after every iteration."""
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
     vb = None if view_bin is None else np.ascontiguousarray(view_bin, dtype=np.int32)
@@ -221,6 +223,9 @@ def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, 
     lib().oracle_set_solver_weights(None if w is None else w.ctypes.data)
     lib().oracle_set_solver_bins(int(n_bins), None if vb is None else vb.ctypes.data)
     lib().oracle_set_solver_tv(float(tv_weight), float(tv_alpha), float(tau), int(reg_steps))
+    if snapshots is not None:
+        assert snapshots.dtype == np.float64 and snapshots.flags["C_CONTIGUOUS"] and snapshots.shape[0] >= iters
+    lib().oracle_set_solver_snapshots(None if snapshots is None else snapshots.ctypes.data)
     try:
         return _solver(lib().oracle_osmom, g, b, angles, offsets, sizes, offcorr, iters, beta, gamma,
                        nonneg, x0, spp, iters * len(sizes), n_bins if vb is not None else 1)
@@ -229,6 +234,7 @@ def osmom(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, 
         lib().oracle_set_solver_weights(None)
         lib().oracle_set_solver_bins(1, None)
         lib().oracle_set_solver_tv(0.0, 0.0, 1e-3, 1)
+        lib().oracle_set_solver_snapshots(None)
 
 
 def ossart(g, b, angles, offsets, sizes, offcorr, iters=10, beta=1.0, gamma=0.0, nonneg=False,

@@ -481,10 +481,12 @@ def ours(args, wl: Workload):
 def kernel_only(args, wl: Workload):
     """Runs one kernel of the workload `--steps` times after `--warmup` launches
     (for profiler captures): forward = forward residual of subset 0,
-    backproject = back-projection with the OS-MOM update of subset 0."""
+    backproject = back-projection of subset 0, fdk = the FDK row filter of
+    every view, tv = one TV primal-dual step (primal + fused dual/update)."""
     import torch
     dev = torch.device("cuda", 0)
     gtb = _package()
+    L = gtb._lib
     plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev)
     n0 = int(sizes[0])
     vol = torch.full(plan.vol_shape, 0.01, dtype=torch.float32, device=dev)
@@ -492,11 +494,26 @@ def kernel_only(args, wl: Workload):
     bs = b[:n0].contiguous()
     stream = torch.cuda.current_stream()
 
+    if args.only == "fdk":
+        # FDK filter of every view (cosine + ramp + offset weight), 283 MB in and out
+        rf = torch.empty_like(b)
+        filt = gtb.hann_ramp_filter(wl.W)
+    if args.only == "tv":
+        # one TV primal-dual step on the volume (gradient field 201 MB)
+        P3 = torch.empty((3,) + plan.vol_shape, dtype=torch.float32, device=dev)
+        sv = torch.full(plan.vol_shape, 0.01, dtype=torch.float32, device=dev)
+        D = torch.full(plan.vol_shape, 0.02, dtype=torch.float32, device=dev)
+        nz_, ny_, nx_ = plan.vol_shape
+
     def one():
         if args.only == "forward":
             plan.forward_residual(vol, bs, r, 0, 1.0, bool(oc[0]), None)
-        else:
+        elif args.only == "backproject":
             plan.backproject(bs, vol, 0, 0, False, True)
+        elif args.only == "fdk":
+            plan.fdk_filter(b, rf, -1, filt, L.CBCT_FDK_RAMP | L.CBCT_FDK_COSINE | L.CBCT_FDK_OFFSET)
+        else:
+            gtb.operators.tv_step(vol, P3, sv, D, 0.5, 1e-3, 0.02)
 
     for _ in range(args.warmup):
         one()
@@ -522,6 +539,14 @@ def batched(args):
     gtb = _package()
     specs = gtb.phantom.uneven_scans(args.scans, seed0=1000)
     scans = [gtb.phantom.make_osmom_scan(sp, 8, 1e5, dev) for sp in specs]
+    variants = {}
+    if args.autotune:
+        # per-scan choice of projector variants (timed on each plan's largest subset)
+        for pl, _, _ in scans:
+            t = pl.autotune()
+            key = (t["forward_variant"], "bp-tma" if (t["backproject_tma"] or 1e9) <= (t["backproject_global"] or 1e9)
+                   else "bp-global")
+            variants["+".join(key)] = variants.get("+".join(key), 0) + 1
     zs = [torch.empty(pl.vol_shape, dtype=torch.float32, device=dev) for pl, _, _ in scans]
     jobs = [dict(plan=pl, b=b, z=z, iterations=10, nonneg=True) for (pl, b, _), z in zip(scans, zs)]
     stream = torch.cuda.current_stream()
@@ -557,7 +582,8 @@ def batched(args):
             "unit": "recon/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_b, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{len(jobs)} uneven scans, OS-MOM 8 subsets x 10 iterations, fp32",
-                       "streams": args.streams, "sizes": "multiples of 8; seeds 1000+i"},
+                       "streams": args.streams, "sizes": "multiples of 8; seeds 1000+i",
+                       "autotune": bool(args.autotune), "variants": variants or None},
             "gups": round(updates / (ms_b * 1e-3) / 1e9, 2),
             "one_at_a_time": {"ms_per_step": round(ms_s, 1), "recon_per_s": round(len(jobs) * 1e3 / ms_s, 3),
                               "gups": round(updates / (ms_s * 1e-3) / 1e9, 2)},
@@ -846,13 +872,14 @@ def main():
     ap.add_argument("--streams", type=int, default=8, help="c4: streams of the batch executor")
     ap.add_argument("--requests", type=int, default=32, help="c5: requests in the arrival stream")
     ap.add_argument("--c3-iters", type=int, default=20, help="c3: OS-MOM iterations")
+    ap.add_argument("--autotune", action="store_true", help="c4: autotune each scan's projector variants")
     ap.add_argument("--rate", type=float, default=20.0, help="c5: Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=4, help="c5: request slots of the server")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="c5: HBM budget of the server")
     ap.add_argument("--seed", type=int, default=5, help="c5: seed of kinds, storage and arrivals")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison leg")
-    ap.add_argument("--only", choices=["forward", "backproject"], default=None,
+    ap.add_argument("--only", choices=["forward", "backproject", "fdk", "tv"], default=None,
                     help="time one kernel of the workload (profiling)")
     args = ap.parse_args()
     if args.config == "c4":

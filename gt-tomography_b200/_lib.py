@@ -35,6 +35,7 @@ EXPORTED = [
     "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
     "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
     "cbct_fdk_filter_ex", "cbct_fdk_ex", "cbct_host_forward", "cbct_host_backproject", "cbct_plan_set_bins",
+    "cbct_tv_step", "cbct_plan_autotune",
     "cbct_server_create", "cbct_server_request_bytes", "cbct_server_submit", "cbct_server_wait",
     "cbct_server_now", "cbct_server_destroy",
 ]
@@ -138,6 +139,8 @@ _SIGS = {
     "cbct_fdk_ex": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _u32, _vp, _vp]),
     "cbct_host_forward": (C.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _vp]),
     "cbct_plan_set_bins": (C.c_int, [_vp, _i32, _vp]),
+    "cbct_tv_step": (C.c_int, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _f, _f, _f, _vp]),
+    "cbct_plan_autotune": (C.c_int, [_vp, _vp, _vp]),
     "cbct_host_backproject": (C.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _u32, _i32, _f, _i32, _vp]),
     "cbct_server_create": (C.c_int, [C.POINTER(CbctServerConfig), C.POINTER(_vp)]),
     "cbct_server_request_bytes": (C.c_int, [C.POINTER(CbctRequest), C.POINTER(_sz)]),

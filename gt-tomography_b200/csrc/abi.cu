@@ -423,6 +423,13 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
   });
 }
 
+cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan && times_ms_out, "NULL argument");
+    plan_autotune(plan, times_ms_out, S(stream));
+  });
+}
+
 cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t reset) {
   return guard([&] {
     CBCT_REQUIRE(plan && flags_out, "bad arguments");
@@ -742,6 +749,16 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
     if (prm.proj_storage != CBCT_F32) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART takes float projections");
     if (prm.tv_weight > 0.f) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART has no regulariser (osSARTSolver.h)");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
+  });
+}
+
+cbct_status cbct_tv_step(float* x, float* P, const float* s, const float* D, int32_t nx, int32_t ny, int32_t nz,
+                         float scale, float tau, float tau_lambda, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(x && P && s && D, "NULL array");
+    CBCT_REQUIRE(nx > 0 && ny > 0 && nz > 0, "image size must be positive");
+    tv_primal_launch(x, P, nx, ny, nz, scale, S(stream));
+    tv_update_launch(P, x, s, D, nx, ny, nz, 1.f, tau, tau_lambda, S(stream));
   });
 }
 

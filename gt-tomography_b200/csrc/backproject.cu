@@ -383,7 +383,7 @@ void backproject_choose_variant(cbct_plan* p) {
   p->bp_variant = 0;
   p->bp_box = SlabBox{0, 0, 0, 0};
   p->bp_max_views = 0;
-  if (p->force_gather || (g.width * 4) % 16 != 0) return;
+  if (p->force_gather || p->bp_pref == 1 || (g.width * 4) % 16 != 0) return;
   const double vx = double(g.lx) / g.nx, vy = double(g.ly) / g.ny, vz = double(g.lz) / g.nz;
   const double ku = g.width / double(g.fov_u), kv = g.height / double(g.fov_v);
   const double bu = g.width / 2.0 - 0.5, bv = g.height / 2.0 - 0.5;

@@ -190,6 +190,7 @@ struct cbct_plan {
   std::vector<int> subset_has_xdom;  // per subset (and all-views entry): any x-dominant view
   void* d_volT = nullptr;   // x/y-transposed volume for x-dominant views (fp32 capacity)
   int bp_variant = 0;       // 0 = global loads, 1 = TMA-staged detector boxes
+  int bp_pref = 0;          // 0: TMA-staged where it fits, 1: global loads (autotuner)
   cbct::SlabBox bp_box{};   // detector box (bx = u width, by = v rows)
   int bp_max_views = 0;     // views per launch the TMA back-projector holds
 
@@ -298,6 +299,12 @@ void host_backproject(cbct_plan* p, int s0, int ns, const float* proj_host, floa
 void tv_primal_launch(const float* x, float* P, int nx, int ny, int nz, float scale, cudaStream_t st);
 void tv_update_launch(const float* P, float* x, const float* s, const float* D, int nx, int ny, int nz, float w,
                       float tau, float tau_lambda, cudaStream_t st);
+
+// autotune.cu: times the plan's projector variants on its largest subset and
+// keeps the fastest; times[5] = forward slab, fan, gather, back-projection
+// TMA, global (ms per launch, -1 where unavailable)
+void plan_autotune(cbct_plan* p, float* times, cudaStream_t st);
+void graph_cache_free(cbct_plan* p);
 
 // mask.cu
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,

@@ -269,6 +269,16 @@ class Plan:
     def set_option(self, opt: int, value: int):
         L.call("cbct_plan_set_option", self._h, opt, int(value))
 
+    def autotune(self, stream=None) -> dict:
+        """cbct_plan_autotune: times the projector variants on the largest
+        subset, keeps the fastest; returns ms per launch (None: unavailable)."""
+        t = np.zeros(5, np.float32)
+        L.call("cbct_plan_autotune", self._h, t.ctypes.data, _stream(stream))
+        names = ["forward_slab", "forward_fan", "forward_gather", "backproject_tma", "backproject_global"]
+        out = {n: (float(v) if v >= 0 else None) for n, v in zip(names, t)}
+        out["forward_variant"] = self.forward_variant()
+        return out
+
     def read_flags(self, reset=True):
         f = (C.c_int32 * 2)()
         L.call("cbct_plan_read_flags", self._h, C.cast(f, C.c_void_p), int(reset))
@@ -415,6 +425,17 @@ def batch_osmom(jobs, n_streams=8, stream=None):
         items[i] = L.CbctBatchItem(j["plan"].handle.value, _ptr(j["b"]), _ptr(j.get("x0")), _ptr(j["z"]), prm,
                                    _ptr(j.get("resid")))
     L.call("cbct_batch_osmom", items, len(jobs), int(n_streams), _stream(stream))
+
+
+def tv_step(x, P, s, D, scale, tau, tau_lambda, stream=None):
+    """One primal-dual step of the TV regulariser (cbct_tv_step): x, s, D of
+    shape (nz, ny, nx), P of shape (3, nz, ny, nx); x is updated in place."""
+    nz, ny, nx = x.shape
+    for t, shp, what in ((x, x.shape, "x"), (s, x.shape, "s"), (D, x.shape, "D"), (P, (3,) + tuple(x.shape), "P")):
+        _need_cuda_f32(t, shp, what)
+    L.call("cbct_tv_step", _ptr(x), _ptr(P), _ptr(s), _ptr(D), nx, ny, nz, float(scale), float(tau),
+           float(tau_lambda), _stream(stream))
+    return x
 
 
 def apply_mask(vol, mask, stream=None):

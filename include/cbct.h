@@ -138,6 +138,14 @@ CBCT_API cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t*
 /* Name of the forward-projector variant the plan selected ("tma-fan", "tma-slab" or "gather"). */
 CBCT_API const char* cbct_plan_forward_variant(const cbct_plan* plan);
 
+/* Autotuner (no reference counterpart): runs every forward projector (slab,
+ * column-fan, gather) and back-projector (TMA-staged, global loads) the plan
+ * can use on its largest subset, keeps the fastest of each for the plan, and
+ * writes the timings (ms per launch; -1 where a variant is unavailable) to
+ * times_ms_out[5] = {fwd slab, fwd fan, fwd gather, bp TMA, bp global}.
+ * Synchronises `stream`; allocates and frees two scratch buffers. */
+CBCT_API cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, void* stream);
+
 /* Plan options (no reference counterpart; diagnostics of this library).
  * CBCT_OPT_DEBUG_CHECKS: kernels record index-range violations and unconsumed
  *   samples in the plan's flag word instead of only clamping.
@@ -272,6 +280,17 @@ CBCT_API cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtyp
 CBCT_API cbct_status cbct_osmom_update(float* z, float* xold, const float* precon, const float* g,
                               size_t n, float step, float mom, int32_t nonneg, void* stream);
 
+/* One primal-dual step of the TV regulariser inside the OS-MOM denoise
+ * (osMOMSolverD.h:214-224 with a cuTVPrimalDualOperator of weight 1 after the
+ * solver's normalisation): P (3*nx*ny*nz floats) receives the periodic forward
+ * differences of x times `scale` (= sigma / (1 + sigma alpha)), each gradient
+ * vector projected onto the unit ball (cuTVPrimalDualOperator.cu:9-37); then
+ * x = ((x - tau g) + tau_lambda (s / D)) / ((1 / D) tau_lambda + 1) with g the
+ * negative divergence of P (:40-62) and tau_lambda = tau / lambda
+ * (updateG, osMOMSolverD.h:233-247). */
+CBCT_API cbct_status cbct_tv_step(float* x, float* P, const float* s, const float* D, int32_t nx, int32_t ny,
+                                  int32_t nz, float scale, float tau, float tau_lambda, void* stream);
+
 /* FP64 reductions: kind 0 = dot(a,b), 1 = nrm2(a)^2 (sum of squares),
  * 2 = asum(a).  out_dev: one double in device memory. */
 CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t n,
@@ -354,8 +373,10 @@ typedef struct {
 
 /* Runs n independent osMOMSolverD reconstructions (cbct_osmom_solve semantics)
  * concurrently on up to n_streams internal streams.  Items are ordered largest
- * first and each goes to the least-loaded stream; each item replays its own
- * plan's captured CUDA graph.  Items must not share plans or output buffers.
+ * first; an item whose forward launches fill the GPU four times or more runs
+ * on the first stream after the other such items, the others go to the
+ * least-loaded of the remaining streams; each item replays its own plan's
+ * captured CUDA graph.  Items must not share plans or output buffers.
  * Every kernel of an item reads only that item's buffers, so each result is
  * bitwise identical to the item solved alone.  The work starts after all work
  * already enqueued on `stream` and the call returns once every item has

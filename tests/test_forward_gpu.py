@@ -181,3 +181,30 @@ def test_forward_16bit_full_size_offset(gtb, cuda, dtype):
     plan.forward(v16.float().contiguous(), b)
     assert plan.forward_variant() == "tma-slab"
     assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["cube", "short"])
+def test_autotune_keeps_results(gtb, O, cuda, name):
+    """The autotuner times the variants, keeps the fastest, and the plan's
+    results stay within the FP32 tolerance of the FP64 oracle."""
+    import torch
+    case = make(name)
+    _, vol = _phantom(case, O)
+    plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets, [7, case.angles.size - 7])
+    t = plan.autotune()
+    assert t["forward_slab"] is not None and t["forward_gather"] is not None and t["backproject_global"] is not None
+    fastest = min((v, k) for k, v in t.items() if k.startswith("forward_") and k != "forward_variant"
+                  and v is not None)[1]
+    assert t["forward_variant"] == {"forward_slab": "tma-slab", "forward_fan": "tma-fan",
+                                    "forward_gather": "gather"}[fastest]
+    plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
+    v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
+    out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
+    plan.forward(v, out)
+    assert plan.read_flags() == (0, 0)
+    ref = O.forward(case.oracle_geom(O), vol, case.angles, case.offsets)
+    assert O.rel_l2(out.cpu().numpy(), ref) < TOL
+    back = torch.zeros(plan.vol_shape, dtype=torch.float32, device=cuda)
+    plan.backproject(out, back)
+    refb = O.backproject(case.oracle_geom(O), out.cpu().numpy().astype(np.float64), case.angles, case.offsets)
+    assert O.rel_l2(back.cpu().numpy(), refb) < TOL

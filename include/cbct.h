@@ -298,10 +298,10 @@ CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* 
 
 /* The same FP64 reduction for callers that cannot allocate device memory.
  * No counterpart in the reference: it exists for code that must not call
- * cudaMalloc while it runs, such as a caller that records its work into a CUDA
- * graph (allocation is not allowed during stream capture) or a host whose
- * device memory is owned by another allocator (a framework's caching
- * allocator) that forbids side allocations.  cbct_reduce_f64 allocates its
+ * cudaMalloc while it runs, such as a latency-bound caller sharing the GPU
+ * with other work (cudaMalloc may wait for the whole device to go idle) or a
+ * host whose device memory is owned by another allocator (a framework's
+ * caching allocator) that forbids side allocations.  cbct_reduce_f64 allocates its
  * partial-sum buffer on its first call on each host thread; this entry point
  * allocates nothing and calls no allocating routine.
  * Scratch: the per-block partial sums live in a static device array of 1024

@@ -1,9 +1,9 @@
 """The allocation-free FP64 reduction, cbct_reduce_f64_noalloc, on the GPU.
 
 Some callers of this library cannot allocate device memory while they run:
-code that records its GPU work into a CUDA graph (cudaMalloc is not allowed
-during stream capture), or a host whose device memory belongs to another
-allocator that forbids side allocations.  cbct_reduce_f64 allocates its
+a latency-bound caller sharing the GPU with other work (cudaMalloc may wait
+for the whole device to go idle), or a host whose device memory belongs to
+another allocator that forbids side allocations.  cbct_reduce_f64 allocates its
 partial-sum buffer on first use; cbct_reduce_f64_noalloc keeps the partial
 sums in a static device array instead.  This test calls it through the C ABI
 and checks it against cbct_reduce_f64 on two calls in a row (a large call,

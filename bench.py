@@ -115,15 +115,24 @@ class Workload:
         return rays * self.Nsamp, nvox * self.P
 
     def launches_per_step(self):
+        # Every subset of this orbit holds x-dominant views, so each forward
+        # launch is preceded by the x/y transpose of the volume.
         if self.name == "c2":
-            # fill + S forward + 1 back-projection (preconditioner), then per subset
-            # step: forward-residual, norm finalise, back-projection with the update.
-            return 1 + self.S + 1 + self.iters * self.S * 3
-        return 1 + 1 + 1            # forward, FDK filter, FDK back-projection
+            # fill + S (transpose + forward) + 1 back-projection (preconditioner), then
+            # per subset step: transpose, forward-residual, norm finalise,
+            # back-projection with the update.
+            return 1 + 2 * self.S + 1 + self.iters * self.S * 4
+        return 2 + 1 + 1            # transpose + forward, FDK filter, FDK back-projection
 
 
-def make_inputs(wl: Workload, gtb, dev):
-    """Seeded phantom, exact line integrals on the device, Poisson noise, log."""
+FORWARD_KERNELS = {"auto": 0, "slab": 1, "gather": 2, "fan": 3, "pair": 4}
+FORWARD_KERNEL_NAMES = {"tma-pair": "fwd_pair_kernel", "tma-slab": "fwd_slab_kernel", "tma-fan": "fwd_fan_kernel",
+                        "gather": "fwd_gather_kernel"}
+
+
+def make_inputs(wl: Workload, gtb, dev, forward_kernel: str = "auto"):
+    """Seeded phantom, exact line integrals on the device, Poisson noise, log.
+    forward_kernel: the plan's forward projector (CBCT_OPT_FORWARD_KERNEL)."""
     import torch
     ang = gtb.phantom.circular_orbit(wl.P)
     off = np.tile(np.array([[wl.offset, 0.0]], np.float32), (wl.P, 1))
@@ -135,6 +144,8 @@ def make_inputs(wl: Workload, gtb, dev):
     oc = [int(abs(float(o[f:f + n, 0].mean())) > 0.1 * fw) if n else 0
           for f, n in zip(np.concatenate([[0], np.cumsum(sizes)[:-1]]), sizes)]
     plan = gtb.Plan(g, a, o, sizes, oc)
+    if forward_kernel != "auto":
+        plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, FORWARD_KERNELS[forward_kernel])
     ell_d = torch.from_numpy(ell.reshape(-1)).to(dev)
     exact = torch.empty(plan.proj_shape(), dtype=torch.float32, device=dev)
     plan.phantom_project(ell_d, exact)
@@ -193,10 +204,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_for(kernel: str, workload: str):
+def traffic_for(kernel: str, workload: str, variant: str | None = None):
+    """DRAM bytes per launch of `kernel` from one ncu capture (profiles/traffic.json),
+    per forward variant where the file keeps several."""
     try:
         d = json.load(open(TRAFFIC_PATH))
-        return d.get(workload, {}).get(kernel)
+        t = d.get(workload, {}).get(kernel)
+        return t.get(variant) if isinstance(t, dict) else t
     except Exception:
         return None
 
@@ -304,7 +318,7 @@ def ours(args, wl: Workload):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     gtb = _package()
-    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev)
+    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev, args.forward_kernel)
     nvox = wl.n[0] * wl.n[1] * wl.n[2]
     z = torch.empty(plan.vol_shape, dtype=torch.float32, device=dev)
     resid = torch.zeros(max(wl.iters * wl.S, 1), dtype=torch.float64, device=dev)
@@ -397,6 +411,7 @@ def ours(args, wl: Workload):
     rays0 = wl.W * wl.H * n0
     alg_bytes = 4 * nvox + 4 * rays0 * 3        # volume + b read + r write (+ per-pixel offset weight computed)
     hbm, peak_kind = peaks()
+    variant = plan.forward_variant()
     achieved = alg_bytes / t_fwd / 1e9
     samples_s = rays0 * wl.Nsamp / t_fwd
 
@@ -408,14 +423,15 @@ def ours(args, wl: Workload):
         "recon_per_s": round(world * 1e3 / ms, 4) if wl.name == "c2" else None,
         "e2e": {"value": round(gups_e2e, 3), "unit": "GUPS", "ms_per_step": round(ms_e2e, 3),
                 "h2d_bytes_per_step": int(b.numel() * 4), "d2h_bytes_per_step": int(nvox * 4)},
-        "roofline": {"bound": "hbm", "kernel": "fwd_slab_kernel (forward residual, one subset)",
+        "roofline": {"bound": "hbm", "kernel": f"{FORWARD_KERNEL_NAMES.get(variant, variant)} (forward residual, "
+                                                 "one subset)",
                      "achieved": round(achieved, 2), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 5), "traffic": traffic_for("forward_residual", wl.name),
+                     "frac": round(achieved / hbm, 5), "traffic": traffic_for("forward_residual", wl.name, variant),
                      "launch_ms": round(t_fwd * 1e3, 4), "alg_bytes_per_launch": alg_bytes,
                      "gsamples_per_s": round(samples_s / 1e9, 2),
                      "note": "gather/issue-bound kernel: HBM fraction of compulsory bytes is small by design"},
         "gpu_launches": wl.launches_per_step() * args.steps,
-        "forward_variant": plan.forward_variant(),
+        "forward_variant": variant,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and wl.name == "c2" and not args.no_plain:
@@ -487,7 +503,7 @@ def kernel_only(args, wl: Workload):
     dev = torch.device("cuda", 0)
     gtb = _package()
     L = gtb._lib
-    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev)
+    plan, b, ell_d, (a, o, sizes, oc) = make_inputs(wl, gtb, dev, args.forward_kernel)
     n0 = int(sizes[0])
     vol = torch.full(plan.vol_shape, 0.01, dtype=torch.float32, device=dev)
     r = torch.empty(plan.proj_shape(0), dtype=torch.float32, device=dev)
@@ -879,6 +895,8 @@ def main():
     ap.add_argument("--seed", type=int, default=5, help="c5: seed of kinds, storage and arrivals")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison leg")
+    ap.add_argument("--forward-kernel", choices=list(FORWARD_KERNELS), default="auto",
+                    help="c1/c2: forward projector variant of the plan (auto: the plan's choice)")
     ap.add_argument("--only", choices=["forward", "backproject", "fdk", "tv"], default=None,
                     help="time one kernel of the workload (profiling)")
     args = ap.parse_args()

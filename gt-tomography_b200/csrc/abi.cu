@@ -398,7 +398,10 @@ cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_ou
 
 const char* cbct_plan_forward_variant(const cbct_plan* plan) {
   if (!plan) return "";
-  return plan->fwd_variant == 2 ? "tma-fan" : plan->fwd_variant == 1 ? "tma-slab" : "gather";
+  return plan->fwd_variant == 3   ? "tma-pair"
+         : plan->fwd_variant == 2 ? "tma-fan"
+         : plan->fwd_variant == 1 ? "tma-slab"
+                                  : "gather";
 }
 
 cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value) {
@@ -409,7 +412,8 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
     } else if (option == CBCT_OPT_FORCE_GATHER || option == CBCT_OPT_FORWARD_KERNEL) {
       if (option == CBCT_OPT_FORCE_GATHER) plan->force_gather = value != 0;
       else {
-        CBCT_REQUIRE(value >= 0 && value <= 3, "forward kernel must be 0 (automatic), 1 (slab), 2 (gather) or 3 (fan)");
+        CBCT_REQUIRE(value >= 0 && value <= 4,
+                     "forward kernel must be 0 (automatic), 1 (slab), 2 (gather), 3 (fan) or 4 (row pairs)");
         plan->fwd_pref = value;
       }
       graph_cache_free(plan);

@@ -1,13 +1,15 @@
 // autotune.cu -- choose the projector variants of a plan by timing them.
 //
 // Which forward projector is fastest depends on the geometry: the slab kernel
-// (16x16 ray tiles, per-ray trilinear samples from TMA boxes), the fan kernel
-// (8x32 tiles, e/d interpolation shared by a detector column; larger boxes),
-// or the gather kernel (no staging); likewise the TMA-staged and the plain
-// back-projector.  The autotuner runs every candidate the plan can use on the
-// plan's largest subset (one warm-up and three timed launches each, CUDA
-// events on the caller's stream) and keeps the fastest.  All candidates give
-// results within FP32 rounding of each other (slab and fan bitwise equal).
+// (16x16 ray tiles, per-ray trilinear samples from TMA boxes), the row-pair
+// kernel (16x32 tiles, two rays of a column per thread sharing their in-plane
+// interpolation), the fan kernel (8x32 tiles, e/d interpolation shared by a
+// detector column; larger boxes), or the gather kernel (no staging); likewise
+// the TMA-staged and the plain back-projector.  The autotuner runs every
+// candidate the plan can use on the plan's largest subset (one warm-up and
+// three timed launches each, CUDA events on the caller's stream) and keeps the
+// fastest.  All candidates give
+// results within FP32 rounding of each other (slab, pair and fan bitwise equal).
 // No counterpart in the reference.
 #include <vector>
 
@@ -40,7 +42,7 @@ float time_ms(cudaStream_t st, F&& f) {
 
 void plan_autotune(cbct_plan* p, float* times, cudaStream_t st) {
   CBCT_REQUIRE(p != nullptr, "plan is NULL");
-  for (int i = 0; i < 5; ++i) times[i] = -1.f;
+  for (int i = 0; i < 6; ++i) times[i] = -1.f;
   int s = 0;
   for (int k = 1; k < p->n_subsets; ++k)
     if (p->count[k] > p->count[s]) s = k;
@@ -51,20 +53,22 @@ void plan_autotune(cbct_plan* p, float* times, cudaStream_t st) {
   try {
     fill_launch(vol, nv, 0.01f, st);
     fill_launch(proj, np, 0.01f, st);
-    // forward: slab (1), fan (3), gather (2); the variant must be the one asked for
-    const int prefs[3] = {1, 3, 2}, want[3] = {1, 2, 0};
+    // forward: slab (1), fan (3), gather (2), pairs (4); the variant must be
+    // the one asked for; slot = its entry of times[]
+    const int prefs[4] = {1, 3, 2, 4}, want[4] = {1, 2, 0, 3}, slot[4] = {0, 1, 2, 5};
     const int saved_pref = p->fwd_pref;
     int best = -1;
     float best_ms = 0.f;
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < 4; ++c) {
       p->fwd_pref = prefs[c];
       forward_choose_variant(p);
       forward_prepare(p);
       if (p->fwd_variant != want[c]) continue;
-      times[c] = time_ms(st, [&] {
+      const float ms = time_ms(st, [&] {
         forward_launch(p, s, CBCT_F32, vol, proj, nullptr, 1.f, 0, 0, 0, nullptr, st);
       });
-      if (best < 0 || times[c] < best_ms) { best = c; best_ms = times[c]; }
+      times[slot[c]] = ms;
+      if (best < 0 || ms < best_ms) { best = c; best_ms = ms; }
     }
     p->fwd_pref = best >= 0 ? prefs[best] : saved_pref;
     forward_choose_variant(p);

@@ -154,13 +154,25 @@ constexpr int kFU = 8;
 constexpr int kFV = 32;
 constexpr int kFKC = 16;
 constexpr int kFanWidths[] = {24, 40, 56, 72};
+// Row-pair forward projector: kPU detector columns x kPV rows per CTA, each
+// thread marching two vertically adjacent rays of one column.
+#ifndef CBCT_PAIR_ROWS
+#define CBCT_PAIR_ROWS 32
+#endif
+#ifndef CBCT_PAIR_COLS
+#define CBCT_PAIR_COLS 16
+#endif
+constexpr int kPU = CBCT_PAIR_COLS;
+constexpr int kPV = CBCT_PAIR_ROWS;
+constexpr int kPairThreads = kPU * kPV / 2;
 
-// Forward-projector blocks per view: the larger of the slab and fan tilings
-// (one FP64 partial sum per block).
+// Forward-projector blocks per view: the largest of the slab, pair and fan
+// tilings (one FP64 partial sum per block).
 inline size_t forward_tiles(int W, int H) {
   const size_t slab = (size_t)((W + kTU - 1) / kTU) * ((H + kTV - 1) / kTV);
+  const size_t pair = (size_t)((W + kPU - 1) / kPU) * ((H + kPV - 1) / kPV);
   const size_t fan = (size_t)((W + kFU - 1) / kFU) * ((H + kFV - 1) / kFV);
-  return std::max(slab, fan);
+  return std::max(std::max(slab, pair), fan);
 }
 
 
@@ -178,9 +190,11 @@ struct cbct_plan {
   int device = 0;
   int max_subset = 0;
 
-  // forward variant: 0 = gather (global loads), 1 = TMA slab, 2 = TMA fan
+  // forward variant: 0 = gather (global loads), 1 = TMA slab, 2 = TMA fan, 3 = TMA row pairs
   int fwd_variant = 0;
-  int fwd_pref = 0;         // CBCT_OPT_FORWARD_KERNEL: 0 automatic, 1 slab, 2 gather, 3 fan
+  int fwd_pref = 0;         // CBCT_OPT_FORWARD_KERNEL: 0 automatic, 1 slab, 2 gather, 3 fan, 4 pair
+  cbct::SlabBox pair{};     // row-pair kernel box for fp32 storage
+  cbct::SlabBox pair16{};   // row-pair kernel box for 16-bit storage
   cbct::SlabBox fan{};      // fan kernel box for fp32 storage
   cbct::SlabBox fan16{};    // fan kernel box for 16-bit storage
   int fan_lz = 0;           // line length (planes) of the fan kernel, odd

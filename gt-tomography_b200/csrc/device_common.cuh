@@ -70,6 +70,17 @@ __device__ __forceinline__ Ray make_ray(const ViewParams& vp, const GridConst& g
   return r;
 }
 
+// ------------------------------------------------------------ rounding
+// floor(x) for |x| < 2^22 on the FMA pipe instead of the conversion unit:
+// x + 1.5 * 2^23 rounded toward -infinity is floor(x) + 1.5 * 2^23 (the sum's
+// last place is 1), and subtracting the constant again is exact.  The result
+// equals floorf(x).
+constexpr float kRoundC = 12582912.f;      // 1.5 * 2^23
+constexpr int kRoundBits = 0x4B400000;     // its bit pattern
+__device__ __forceinline__ float floor_small(float x) { return __fadd_rd(x, kRoundC) - kRoundC; }
+// The integer v (|v| < 2^22) held by a float s = v + 1.5 * 2^23: its low mantissa bits.
+__device__ __forceinline__ int int_of_biased(float s) { return __float_as_int(s) - kRoundBits; }
+
 // Bounds-checked trilinear fetch from global memory at texel coordinates
 // (border texels read as 0, as cudaAddressModeBorder does).
 template <class V>

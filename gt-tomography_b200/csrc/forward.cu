@@ -84,32 +84,34 @@ __device__ __forceinline__ float march_global(const V* __restrict__ vol, const G
   return acc;
 }
 
-// Epilogue shared by both variants.  All threads of the block must call it.
-__device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& gc, const ViewParams& vp,
-                                             int p, int u, int v, bool active, float val,
-                                             double* sh_red, int tid) {
+// Output of one ray (store, reciprocal or weighted residual); returns the
+// squared residual (residual mode) for the block's partial sum.
+__device__ __forceinline__ double fwd_store(const FwdOut& o, const GridConst& gc, const ViewParams& vp, int p,
+                                            int u, int v, float val) {
   double sq = 0.0;
-  if (active) {
-    const size_t idx = ((size_t)p * gc.H + v) * gc.W + u;
-    // CBSubsetWeightOperator: mult_M multiplies the projection by w, and mult_MH
-    // of the residual weights its input by w again (CBSubsetWeightOperator.h:32-49).
-    const float wp = o.wproj ? o.wproj[idx] : 1.f;
-    val *= wp;
-    if (o.mode == kModeStore) {
-      o.out[idx] = o.accumulate ? o.out[idx] + val : val;
-    } else if (o.mode == kModeRecip) {
-      o.out[idx] = 1.f / fmaxf(val, 1e-6f);
-    } else {
-      const float d = o.b ? val - ld_any(o.b, idx, o.b_dtype) : val;
-      sq = double(d) * double(d);
-      float w = o.scale * wp;
-      if (o.pw) w *= o.pw[idx];
-      if (o.apply_offset) w *= offset_weight_full(gc.fov_u, gc.W, u, vp.ox);
-      o.out[idx] = d * w;
-    }
+  const size_t idx = ((size_t)p * gc.H + v) * gc.W + u;
+  // CBSubsetWeightOperator: mult_M multiplies the projection by w, and mult_MH
+  // of the residual weights its input by w again (CBSubsetWeightOperator.h:32-49).
+  const float wp = o.wproj ? o.wproj[idx] : 1.f;
+  val *= wp;
+  if (o.mode == kModeStore) {
+    o.out[idx] = o.accumulate ? o.out[idx] + val : val;
+  } else if (o.mode == kModeRecip) {
+    o.out[idx] = 1.f / fmaxf(val, 1e-6f);
+  } else {
+    const float d = o.b ? val - ld_any(o.b, idx, o.b_dtype) : val;
+    sq = double(d) * double(d);
+    float w = o.scale * wp;
+    if (o.pw) w *= o.pw[idx];
+    if (o.apply_offset) w *= offset_weight_full(gc.fov_u, gc.W, u, vp.ox);
+    o.out[idx] = d * w;
   }
+  return sq;
+}
+
+// Deterministic block sum of sq; one partial per block in launch order.
+__device__ __forceinline__ void fwd_block_partial(const FwdOut& o, double sq, double* sh_red, int tid) {
   if (o.partials != nullptr) {
-    // Deterministic block sum; one partial per block in launch order.
     double t = warp_sum(sq);
     const int w = tid >> 5, l = tid & 31;
     if (l == 0) sh_red[w] = t;
@@ -123,6 +125,14 @@ __device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& g
       }
     }
   }
+}
+
+// Epilogue shared by the per-ray variants.  All threads of the block must call it.
+__device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& gc, const ViewParams& vp,
+                                             int p, int u, int v, bool active, float val,
+                                             double* sh_red, int tid) {
+  const double sq = active ? fwd_store(o, gc, vp, p, u, v, val) : 0.0;
+  fwd_block_partial(o, sq, sh_red, tid);
 }
 
 // ------------------------------------------------------------------ gather
@@ -187,13 +197,13 @@ template <class V, int BX>
 struct SlabSample {
   static constexpr int BXY = BX * kBoxY;
   // Trilinear value of one sample whose frame coordinates are (ced.x, ced.y, cz)
-  // and whose floors are (fe, fd, fz).
+  // and whose floors are (fe, fd, fz).  cmo = 1.5 * 2^23 - (box origin index):
+  // the element index comes out of the mantissa of an exact sum.
   static __device__ __forceinline__ float eval(const V* __restrict__ s, float2 ced, float cz, float fe, float fd,
-                                               float fz, float orgf, unsigned maxidx, int& bad, bool check) {
+                                               float fz, float cmo, unsigned maxidx, int& bad, bool check) {
     const float2 aed = __fadd2_rn(ced, make_float2(-fe, -fd));
     const float az = cz - fz;
-    const float idxf = fmaf(fz, float(BXY), fmaf(fd, float(BX), fe)) - orgf;
-    const int idx0 = int(idxf);
+    const int idx0 = int_of_biased(fmaf(fz, float(BXY), fmaf(fd, float(BX), fe)) + cmo);
     if (check) bad |= (unsigned)idx0 > maxidx;
     const unsigned idx = min((unsigned)idx0, maxidx);
     const V* q = s + idx;
@@ -218,8 +228,8 @@ constexpr int kFwdUnroll = 2;
 
 template <class V, int BX, int SGN, bool CHECK>
 __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
-                                             float cz0, float dce, float dcd, float dcz, float lo, float hi,
-                                             float orgf, unsigned maxidx, float& acc, int& bad) {
+                                             float cz0, float dce, float dcd, float idcd, float dcz, float lo,
+                                             float hi, float cmo, unsigned maxidx, float& acc, int& bad) {
   using SS = SlabSample<V, BX>;
   const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
   // floor(x) >= hi <=> x >= hi and floor(x) < lo <=> x < lo, lo and hi being integers.
@@ -227,7 +237,8 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
     const float x = fmaf(k, dcd, cd0);
     return SGN > 0 ? (x >= hi) : (x < lo);
   };
-  float ke = ceilf(((SGN > 0 ? hi : lo) - cd0) / dcd);
+  // Estimate (idcd = 1 / dcd), then the exact boundary: out_at is monotone in k.
+  float ke = ceilf(((SGN > 0 ? hi : lo) - cd0) * idcd);
   ke = fminf(fmaxf(ke, kf), Nf);
   while (ke > kf && out_at(ke - 1.f)) ke -= 1.f;
   while (ke < Nf && !out_at(ke)) ke += 1.f;
@@ -239,7 +250,7 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
       const float kq = k + float(q);
       const float2 pq = __ffma2_rn(make_float2(kq, kq), dc, c0);
       const float czq = fmaf(kq, dcz, cz0);
-      v[q] = SS::eval(s, pq, czq, floorf(pq.x), floorf(pq.y), floorf(czq), orgf, maxidx, bad, CHECK);
+      v[q] = SS::eval(s, pq, czq, floor_small(pq.x), floor_small(pq.y), floor_small(czq), cmo, maxidx, bad, CHECK);
     }
 #pragma unroll
     for (int q = 0; q < kFwdUnroll; ++q) acc += v[q];
@@ -247,7 +258,7 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
   for (; k < ke; k += 1.f) {
     const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
     const float czq = fmaf(k, dcz, cz0);
-    acc += SS::eval(s, pq, czq, floorf(pq.x), floorf(pq.y), floorf(czq), orgf, maxidx, bad, CHECK);
+    acc += SS::eval(s, pq, czq, floor_small(pq.x), floor_small(pq.y), floor_small(czq), cmo, maxidx, bad, CHECK);
   }
   kf = ke;
 }
@@ -282,6 +293,7 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
   // Frame coordinates: e = cross axis, d = slab axis (y for dom = 1, x for dom = 0).
   const float ce0 = dom ? r.c0x : r.c0y, dce = dom ? r.dcx : r.dcy;
   const float cd0 = dom ? r.c0y : r.c0x, dcd = dom ? r.dcy : r.dcx;
+  const float idcd = 1.f / dcd;
   const float ke = dom ? gc.kx : gc.ky, be = dom ? gc.bx : gc.by;
   const float kd = dom ? gc.ky : gc.kx, bd = dom ? gc.by : gc.bx;
   const float Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
@@ -389,11 +401,13 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
     if (hit) {
       const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
       const float lo = float(od), hi = lo + float(kTS);
-      const float orgf = float(oe + od * BX + oz * BXY);
+      const float cmo = kRoundC - float(oe + od * BX + oz * BXY);
       if (vp.dsgn > 0)
-        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, idcd, r.dcz, lo, hi, cmo, maxidx, acc,
+                                        bad);
       else
-        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, idcd, r.dcz, lo, hi, cmo, maxidx, acc,
+                                         bad);
     }
     __syncthreads();
     if (tid == 0 && i + kNStage < nslab) {
@@ -419,6 +433,306 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
     if (grown_range(vp, gc, u, v, r, k0, k1)) val = march_global(vol, gc, r, k0, k1) * r.delta;
   }
   fwd_epilogue(o, gc, vp, p, u, v, active, val, sh.red, tid);
+}
+
+// ------------------------------------------------------------------ row pairs
+// Two vertically adjacent rays of one detector column lie in the column's
+// vertical plane.  When both leave the volume through its side faces their
+// clip (a1, a2) is the column's, so their k-th samples share the in-plane
+// position (e_k, d_k) and differ only in z; when in addition their z
+// coordinates differ by less than one texel at every sample (checked at both
+// ends; the difference is linear in k), the lower ray's planes fz, fz + 1 and
+// the upper ray's planes are among fz, fz + 1, fz + 2.  One thread then marches
+// the pair: one e/d position, three planes interpolated in e and d (12 shared
+// loads instead of 16), and each ray's own z lerp.  Every value is the one the
+// slab kernel computes for that ray (same texels, same operations, same
+// order), so results are bitwise equal.  Other pairs (rays clipped by the top
+// or bottom face, or far apart in z) run slab_samples for each ray.
+// One sample of a paired ray: (lower ray's value, upper ray's value).
+template <class V, int BX, bool CHECK>
+__device__ __forceinline__ float2 pair_eval(const V* __restrict__ s, float k, float2 c0, float2 dc, float zl0,
+                                            float dzl, float zu0, float dzu, float cmo, unsigned maxidx,
+                                            unsigned maxidx3, int& bad) {
+  constexpr int BXY = BX * kBoxY;
+  const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
+  const float czl = fmaf(k, dzl, zl0), czu = fmaf(k, dzu, zu0);
+  const float fe = floor_small(pq.x), fd = floor_small(pq.y), fzl = floor_small(czl), fzu = floor_small(czu);
+  const float2 aed = __fadd2_rn(pq, make_float2(-fe, -fd));
+  const int idx0 = int_of_biased(fmaf(fzl, float(BXY), fmaf(fd, float(BX), fe)) + cmo);
+  const bool up = fzu != fzl;
+  if (CHECK) bad |= ((unsigned)idx0 > maxidx) | (up && (unsigned)idx0 + 2u * BXY > maxidx3) | (fzu - fzl > 1.f);
+  const V* q = s + min((unsigned)idx0, maxidx);
+  const V* q2 = s + min((unsigned)idx0 + 2u * BXY, maxidx3);
+  const float2 te = make_float2(aed.x, aed.x);
+  const float2 e0 = lerp2(make_float2(sm_f(q[0]), sm_f(q[BX])), make_float2(sm_f(q[1]), sm_f(q[BX + 1])), te);
+  const float2 e1 = lerp2(make_float2(sm_f(q[BXY]), sm_f(q[BXY + BX])),
+                          make_float2(sm_f(q[BXY + 1]), sm_f(q[BXY + BX + 1])), te);
+  const float2 e2 = lerp2(make_float2(sm_f(q2[0]), sm_f(q2[BX])), make_float2(sm_f(q2[1]), sm_f(q2[BX + 1])), te);
+  // d lerps of planes fz, fz + 1 (packed) and fz + 2: the slab kernel's formula
+  const float2 d01 = lerp2(make_float2(e0.x, e1.x), make_float2(e0.y, e1.y), make_float2(aed.y, aed.y));
+  const float d2 = fmaf(aed.y, e2.y, fmaf(-aed.y, e2.x, e2.x));
+  const float bl = up ? d01.y : d01.x, bh = up ? d2 : d01.y;
+  return make_float2(fmaf(czl - fzl, d01.y - d01.x, d01.x), fmaf(czu - fzu, bh - bl, bl));
+}
+
+#ifndef CBCT_PAIR_UNROLL
+#define CBCT_PAIR_UNROLL 1
+#endif
+constexpr int kPairUnroll = CBCT_PAIR_UNROLL;
+
+// The pair's samples inside one slab (counted as in slab_samples), each ray's
+// values added in ray order.
+template <class V, int BX, int SGN, bool CHECK>
+__device__ __forceinline__ void pair_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
+                                             float dce, float dcd, float idcd, float zl0, float dzl, float zu0,
+                                             float dzu, float lo, float hi, float cmo, unsigned maxidx,
+                                             unsigned maxidx3, float& accl, float& accu, int& bad) {
+  const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
+  auto out_at = [&](float k) {
+    const float x = fmaf(k, dcd, cd0);
+    return SGN > 0 ? (x >= hi) : (x < lo);
+  };
+  float ke = ceilf(((SGN > 0 ? hi : lo) - cd0) * idcd);
+  ke = fminf(fmaxf(ke, kf), Nf);
+  while (ke > kf && out_at(ke - 1.f)) ke -= 1.f;
+  while (ke < Nf && !out_at(ke)) ke += 1.f;
+  float k = kf;
+  if (kPairUnroll > 1) {
+    for (; k + float(kPairUnroll - 1) < ke; k += float(kPairUnroll)) {
+      float2 v[kPairUnroll];
+#pragma unroll
+      for (int q = 0; q < kPairUnroll; ++q)
+        v[q] = pair_eval<V, BX, CHECK>(s, k + float(q), c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
+#pragma unroll
+      for (int q = 0; q < kPairUnroll; ++q) {
+        accl += v[q].x;
+        accu += v[q].y;
+      }
+    }
+  }
+  for (; k < ke; k += 1.f) {
+    const float2 v = pair_eval<V, BX, CHECK>(s, k, c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
+    accl += v.x;
+    accu += v.y;
+  }
+  kf = ke;
+}
+
+// CTAs per SM the register budget is sized for (shared memory allows two fp32
+// or three 16-bit boxes of a 256-thread tile).
+template <class V>
+constexpr int pair_min_blocks() {
+  return kPairThreads >= 256 ? (sizeof(V) == 4 ? 2 : 3) : (sizeof(V) == 4 ? 3 : 5);
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
+    fwd_pair_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
+                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ, FwdOut o,
+                    int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ SlabShared sh;
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  constexpr int BXY = BX * kBoxY;
+  const ViewParams vp = views[blockIdx.z];
+  const int dom = vp.dom;
+  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const int tid = threadIdx.x;
+  const int p = blockIdx.z;
+  const int u0 = blockIdx.x * kPU, v0 = blockIdx.y * kPV;
+  const int u = u0 + (tid % kPU), va = v0 + 2 * (tid / kPU), vb = va + 1;
+  const bool act_a = (u < gc.W) && (va < gc.H), act_b = (u < gc.W) && (vb < gc.H);
+  const int uc = min(u, gc.W - 1);
+  const Ray ra = make_ray(vp, gc, uc, min(va, gc.H - 1));
+  const Ray rb = make_ray(vp, gc, uc, min(vb, gc.H - 1));
+  const bool hit_a = act_a && (ra.a2 > ra.a1), hit_b = act_b && (rb.a2 > rb.a1);
+  const float ke_ = dom ? gc.kx : gc.ky, be = dom ? gc.bx : gc.by;
+  const float kd = dom ? gc.ky : gc.kx, bd = dom ? gc.by : gc.bx;
+  const float Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
+  // Frame coordinates (e = cross axis, d = slab axis) of both rays.
+  const float ce0a = dom ? ra.c0x : ra.c0y, dcea = dom ? ra.dcx : ra.dcy;
+  const float cd0a = dom ? ra.c0y : ra.c0x, dcda = dom ? ra.dcy : ra.dcx;
+  const float ce0b = dom ? rb.c0x : rb.c0y, dceb = dom ? rb.dcx : rb.dcy;
+  const float cd0b = dom ? rb.c0y : rb.c0x, dcdb = dom ? rb.dcy : rb.dcx;
+  const float idcda = 1.f / dcda, idcdb = 1.f / dcdb;
+  const float Nf = float(gc.N);
+  // Pairing: same clip, z difference in (0, 1) texel at both ends (the lower
+  // ray first).  The margins cover the rounding of the sample coordinates.
+  bool paired = false, a_low = true;
+  if (hit_a && hit_b && ra.a1 == rb.a1 && ra.a2 == rb.a2) {
+    const float d0 = rb.c0z - ra.c0z;
+    const float d1 = fmaf(Nf - 1.f, rb.dcz, rb.c0z) - fmaf(Nf - 1.f, ra.dcz, ra.c0z);
+    const bool ab = d0 >= 2e-3f && d0 <= 0.998f && d1 >= 2e-3f && d1 <= 0.998f;
+    const bool ba = d0 <= -2e-3f && d0 >= -0.998f && d1 <= -2e-3f && d1 >= -0.998f;
+    paired = ab || ba;
+    a_low = ab;
+  }
+  const float zl0 = a_low ? ra.c0z : rb.c0z, dzl = a_low ? ra.dcz : rb.dcz;
+  const float zu0 = a_low ? rb.c0z : ra.c0z, dzu = a_low ? rb.dcz : ra.dcz;
+
+  if (tid == 0) {
+    sh.mlo = INT_MAX;
+    sh.mhi = INT_MIN;
+    sh.abort_flag = 0;
+    for (int s = 0; s < kNStage; ++s) mbar_init(&sh.bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  {
+    int mn = INT_MAX, mx = INT_MIN;
+    if (hit_a) {
+      const int m0 = (max(int(floorf(cd0a)), kSlabBase) - kSlabBase) / kTS;
+      const int m1 = (max(int(floorf(fmaf(Nf - 1.f, dcda, cd0a))), kSlabBase) - kSlabBase) / kTS;
+      mn = min(m0, m1);
+      mx = max(m0, m1);
+    }
+    if (hit_b) {
+      const int m0 = (max(int(floorf(cd0b)), kSlabBase) - kSlabBase) / kTS;
+      const int m1 = (max(int(floorf(fmaf(Nf - 1.f, dcdb, cd0b))), kSlabBase) - kSlabBase) / kTS;
+      mn = min(mn, min(m0, m1));
+      mx = max(mx, max(m0, m1));
+    }
+    if (mn <= mx) {
+      atomicMin(&sh.mlo, mn);
+      atomicMax(&sh.mhi, mx);
+    }
+  }
+  __syncthreads();
+  const int mlo = sh.mlo, mhi = sh.mhi;
+  int nslab = (mhi >= mlo) ? (mhi - mlo + 1) : 0;
+  if (nslab > kMaxSlabs) {
+    if (tid == 0) atomicAdd(&flags[0], 1);
+    nslab = 0;
+  }
+  for (int i = tid; i < nslab; i += blockDim.x) {
+    sh.emin[i] = INT_MAX; sh.emax[i] = INT_MIN;
+    sh.zmin[i] = INT_MAX; sh.zmax[i] = INT_MIN;
+  }
+  __syncthreads();
+  // Footprint of every slab: the tile's four corner rays at the slab's two
+  // bounding planes, clamped to the volume's texel range.
+  const int ue = min(u0 + kPU, gc.W) - 1, ve = min(v0 + kPV, gc.H) - 1;
+  const int ne = dom ? gc.nx : gc.ny;
+  for (int q = tid; q < nslab * 8; q += blockDim.x) {
+    const int i = q >> 3, c = q & 7;
+    const int m = mlo + i;
+    const float plane = float(kSlabBase + m * kTS + ((c & 4) ? kTS : 0));
+    const int ucc = (c & 1) ? ue : u0, vcc = (c & 2) ? ve : v0;
+    const float dx = fmaf(float(ucc), vp.Eux, vp.D0x);
+    const float dy = fmaf(float(ucc), vp.Euy, vp.D0y);
+    const float dz = fmaf(float(vcc), vp.Evz, vp.D0z);
+    const float de = dom ? dx : dy, dd = dom ? dy : dx;
+    const float t = ((plane - bd) / kd - Sd) / dd;
+    const float ce = fmaf(fmaf(t, de, Se), ke_, be);
+    const float cz = fmaf(t * dz, gc.kz, gc.bz);
+    const int fe = min(max(int(floorf(fminf(fmaxf(ce, -1.0e5f), 1.0e5f))), -1), ne - 1);
+    const int fz = min(max(int(floorf(fminf(fmaxf(cz, -1.0e5f), 1.0e5f))), -1), gc.nz - 1);
+    atomicMin(&sh.emin[i], fe);
+    atomicMax(&sh.emax[i], fe);
+    atomicMin(&sh.zmin[i], fz);
+    atomicMax(&sh.zmax[i], fz);
+  }
+  __syncthreads();
+
+  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
+  const unsigned maxidx = unsigned(BXY * (BZ - 1) - BX - 2);   // two-plane loads stay in the box
+  const unsigned maxidx3 = unsigned(BXY * BZ - BX - 2);        // the third plane's loads
+  auto origin = [&](int i, int& oe, int& od, int& oz, int& m) {
+    m = (vp.dsgn > 0) ? mlo + i : mhi - i;
+    const int ii = m - mlo;
+    oe = (sh.emin[ii] - 1) & ~(int(16 / sizeof(V)) - 1);   // 16-byte aligned x start
+    od = kSlabBase + m * kTS;
+    oz = sh.zmin[ii] - 1;
+  };
+  auto issue = [&](int i) {
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    uint64_t* bar = &sh.bars[i % kNStage];
+    mbar_arrive_expect_tx(bar, box_bytes);
+    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, oe, od, oz, bar);
+  };
+  if (tid == 0) {
+    for (int i = 0; i < min(kNStage, nslab); ++i) issue(i);
+  }
+
+  float acca = 0.f, accb = 0.f;   // paired: lower / upper ray
+  float kfa = 0.f, kfb = 0.f;     // paired: kfa is the pair's next sample
+  int bad = 0;
+  int done = 0;
+  for (int i = 0; i < nslab; ++i) {
+    const int slot = i % kNStage;
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
+      break;
+    }
+    done = i + 1;
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    if (CHECK && tid == 0) {
+      const int ii = m - mlo;
+      if (sh.emax[ii] + 2 - oe >= BX || sh.zmax[ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
+    }
+    const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
+    const float lo = float(od), hi = lo + float(kTS);
+    const float cmo = kRoundC - float(oe + od * BX + oz * BXY);
+    if (paired) {
+      if (vp.dsgn > 0)
+        pair_samples<V, BX, 1, CHECK>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi, cmo,
+                                      maxidx, maxidx3, acca, accb, bad);
+      else
+        pair_samples<V, BX, -1, CHECK>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi, cmo,
+                                       maxidx, maxidx3, acca, accb, bad);
+    } else {
+      if (hit_a) {
+        if (vp.dsgn > 0)
+          slab_samples<V, BX, 1, CHECK>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
+                                        maxidx, acca, bad);
+        else
+          slab_samples<V, BX, -1, CHECK>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
+                                         maxidx, acca, bad);
+      }
+      if (hit_b) {
+        if (vp.dsgn > 0)
+          slab_samples<V, BX, 1, CHECK>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
+                                        maxidx, accb, bad);
+        else
+          slab_samples<V, BX, -1, CHECK>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
+                                         maxidx, accb, bad);
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && i + kNStage < nslab) {
+      fence_proxy_async();
+      issue(i + kNStage);
+    }
+  }
+  if (sh.abort_flag && tid == 0) {
+    for (int i = done; i < min(done + kNStage, nslab); ++i)
+      (void)mbar_wait_bounded(&sh.bars[i % kNStage], (i / kNStage) & 1, kWaitLimit);
+  }
+  if (CHECK) {
+    // every sample of a hit ray must be consumed
+    if (paired ? kfa != Nf : ((hit_a && kfa != Nf) || (hit_b && kfb != Nf))) bad = 1;
+    if (bad) atomicAdd(&flags[0], 1);
+  }
+  float vala = 0.f, valb = 0.f;
+  if (paired) {
+    vala = (a_low ? acca : accb) * ra.delta;
+    valb = (a_low ? accb : acca) * rb.delta;
+  } else {
+    int k0, k1;
+    if (hit_a) vala = acca * ra.delta;
+    else if (act_a && grown_range(vp, gc, u, va, ra, k0, k1)) vala = march_global(vol, gc, ra, k0, k1) * ra.delta;
+    if (hit_b) valb = accb * rb.delta;
+    else if (act_b && grown_range(vp, gc, u, vb, rb, k0, k1)) valb = march_global(vol, gc, rb, k0, k1) * rb.delta;
+  }
+  double sq = 0.0;
+  if (act_a) sq += fwd_store(o, gc, vp, p, u, va, vala);
+  if (act_b) sq += fwd_store(o, gc, vp, p, u, vb, valb);
+  fwd_block_partial(o, sq, sh.red, tid);
 }
 
 // ------------------------------------------------------------------ fan
@@ -482,7 +796,7 @@ __device__ __forceinline__ void fan_slab(const V* __restrict__ s, float* __restr
     if (g < G) {
       const float kfj = float(kcol + j);
       const float2 pa = __ffma2_rn(make_float2(kfj, kfj), dc, c0);
-      const float fe = floorf(pa.x), fd = floorf(pa.y);
+      const float fe = floor_small(pa.x), fd = floor_small(pa.y);
       const float2 aed = __fadd2_rn(pa, make_float2(-fe, -fd));
       const float2 te = make_float2(aed.x, aed.x);
       const float td = aed.y;
@@ -502,7 +816,7 @@ __device__ __forceinline__ void fan_slab(const V* __restrict__ s, float* __restr
       const float* L = lines;
       for (int jj = 0; jj < nk; ++jj, L += LZ) {
         const float cz = fmaf(float(kcol + jj), dcz, c0z);
-        const float fz = floorf(cz);
+        const float fz = floor_small(cz);
         const float az = cz - fz;
         int iz = int(fz) - zl;
         if (CHECK) bad |= (unsigned)iz > (unsigned)(nz - 2);
@@ -552,6 +866,7 @@ __global__ void __launch_bounds__(256, 3) fwd_fan_kernel(const __grid_constant__
   // shared rays they are the column's.
   const float ce0 = dom ? r.c0x : r.c0y, dce = dom ? r.dcx : r.dcy;
   const float cd0 = dom ? r.c0y : r.c0x, dcd = dom ? r.dcy : r.dcx;
+  const float idcd = 1.f / dcd;
   // The column's frame coordinates, from the first shared lane.
   const int src = any_shared ? __ffs(__ballot_sync(0xffffffffu, shared)) - 1 : 0;
   const float2 cc0 = make_float2(__shfl_sync(0xffffffffu, ce0, src), __shfl_sync(0xffffffffu, cd0, src));
@@ -671,10 +986,13 @@ __global__ void __launch_bounds__(256, 3) fwd_fan_kernel(const __grid_constant__
                                    orgf, acc, bad);
     }
     if (own) {
+      const float cmo = kRoundC - orgf;
       if (vp.dsgn > 0)
-        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+        slab_samples<V, BX, 1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, idcd, r.dcz, lo, hi, cmo, maxidx, acc,
+                                        bad);
       else
-        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, r.dcz, lo, hi, orgf, maxidx, acc, bad);
+        slab_samples<V, BX, -1, CHECK>(s, kf, Nf, ce0, cd0, r.c0z, dce, dcd, idcd, r.dcz, lo, hi, cmo, maxidx, acc,
+                                         bad);
     }
     __syncthreads();
     if (tid == 0 && i + kNStage < nslab) {
@@ -767,6 +1085,30 @@ void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim
 }
 
 template <class V>
+const SlabBox& pair_box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->pair : p->pair16; }
+
+template <class V, int BX>
+void launch_pair(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, int first, int cnt, cudaStream_t st,
+                 cbct_dtype dt) {
+  const SlabBox& b = pair_box_for<V>(p);
+  const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
+  const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
+                                  volT ? p->g.nx : p->g.ny, p->g.nz, b);
+  const size_t smem = forward_smem(b, sizeof(V), 0);
+  const dim3 grid((p->g.width + kPU - 1) / kPU, (p->g.height + kPV - 1) / kPV, cnt);
+  if (p->debug_checks) {
+    auto k = fwd_pair_kernel<V, BX, true>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+  } else {
+    auto k = fwd_pair_kernel<V, BX, false>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+  }
+  check_launch("fwd_pair_kernel");
+}
+
+template <class V>
 const SlabBox& fan_box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->fan : p->fan16; }
 
 template <class V, int BX>
@@ -810,6 +1152,17 @@ void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaS
     check_launch("transpose_xy_kernel");
     volT = t;
   }
+  if (p->fwd_variant == 3) {
+    switch (pair_box_for<V>(p).bx) {
+      case 40: launch_pair<V, 40>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 56: launch_pair<V, 56>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 72: launch_pair<V, 72>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 104: launch_pair<V, 104>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 136: launch_pair<V, 136>(p, vol, volT, o, first, cnt, st, dt); break;
+      default: throw Error(CBCT_ERR_INTERNAL, "unsupported pair box width");
+    }
+    return;
+  }
   if (p->fwd_variant == 2) {
     switch (fan_box_for<V>(p).bx) {
       case 24: launch_fan<V, 24>(p, vol, volT, o, first, cnt, st, dt); break;
@@ -837,6 +1190,12 @@ void prepare_width(size_t smem) {
 }
 
 template <class V, int BX>
+void prepare_pair_width(size_t smem) {
+  ensure_smem_attr((const void*)fwd_pair_kernel<V, BX, false>, smem);
+  ensure_smem_attr((const void*)fwd_pair_kernel<V, BX, true>, smem);
+}
+
+template <class V, int BX>
 void prepare_fan_width(size_t smem) {
   ensure_smem_attr((const void*)fwd_fan_kernel<V, BX, false>, smem);
   ensure_smem_attr((const void*)fwd_fan_kernel<V, BX, true>, smem);
@@ -844,6 +1203,18 @@ void prepare_fan_width(size_t smem) {
 
 template <class V>
 void prepare_typed(const cbct_plan* p) {
+  if (p->fwd_variant == 3) {
+    const SlabBox& b = pair_box_for<V>(p);
+    const size_t ps = forward_smem(b, sizeof(V), 0);
+    switch (b.bx) {
+      case 40: prepare_pair_width<V, 40>(ps); break;
+      case 56: prepare_pair_width<V, 56>(ps); break;
+      case 72: prepare_pair_width<V, 72>(ps); break;
+      case 104: prepare_pair_width<V, 104>(ps); break;
+      case 136: prepare_pair_width<V, 136>(ps); break;
+      default: break;
+    }
+  }
   if (p->fwd_variant == 2) {
     const SlabBox& f = fan_box_for<V>(p);
     const size_t fs = forward_smem(f, sizeof(V), p->fan_lz, slabs_max(p->g));
@@ -873,12 +1244,12 @@ void prepare_typed(const cbct_plan* p) {
 // (corner-ray bounding box in the view's frame, computed in FP64): e extent
 // and z extent in elements, including margins.  False when some view cannot
 // use slabs (a ray not dominated by its view's slab axis, or too many slabs).
-static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ext_z) {
+static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ext_z, double* row_dz = nullptr) {
   const cbct_geometry& g = p->g;
   const double kx = g.nx / (double)g.lx, ky = g.ny / (double)g.ly, kz = g.nz / (double)g.lz;
   const double bx = g.nx / 2.0 - 0.5, by = g.ny / 2.0 - 0.5, bz = g.nz / 2.0 - 0.5;
   const int tiles_u = (g.width + TU - 1) / TU, tiles_v = (g.height + TV - 1) / TV;
-  struct Acc { int e = 0, z = 0, ok = 1; };
+  struct Acc { int e = 0, z = 0, ok = 1; double dz = 0; };
   std::vector<Acc> acc(host_threads());
   // The in-plane coordinate of a ray does not depend on the detector row, so the
   // e extent is a function of (view, tile column, slab); the z extent comes from
@@ -919,6 +1290,8 @@ static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ex
             emn = std::min(emn, ce); emx = std::max(emx, ce);
             tmn = std::min(tmn, t); tmx = std::max(tmx, t);
           }
+          // z distance (texels) between the rays of adjacent detector rows
+          a.dz = std::max(a.dz, std::max(std::fabs(tmn), std::fabs(tmx)) * std::fabs((double)vp.Evz) * kz);
           // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin; the
           // kernels clamp footprints to the volume, whose extent bounds the box
           const int Ne = dom ? g.nx : g.ny;
@@ -936,21 +1309,27 @@ static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ex
   });
   ext_e = ext_z = 0;
   bool ok = true;
+  double dz = 0;
   for (const Acc& a : acc) {
     ext_e = std::max(ext_e, a.e);
     ext_z = std::max(ext_z, a.z);
+    dz = std::max(dz, a.dz);
     ok = ok && a.ok;
   }
+  if (row_dz) *row_dz = dz;
   return ok;
 }
 
 // Chooses the forward variant and its TMA boxes from the plan geometry: the
-// per-ray slab kernel where its boxes fit, else the gather kernel; the fan
-// kernel on request (CBCT_OPT_FORWARD_KERNEL = 3).
+// row-pair kernel where adjacent detector rows are less than one z texel
+// apart over the whole volume (so pairs share their planes) and its boxes fit,
+// else the per-ray slab kernel where its boxes fit, else the gather kernel.
+// CBCT_OPT_FORWARD_KERNEL forces slab (1), gather (2), fan (3) or pairs (4).
 void forward_choose_variant(cbct_plan* p) {
   p->fwd_variant = 0;
   p->slab = SlabBox{0, 0, 0, 0};
   p->fan = SlabBox{0, 0, 0, 0};
+  p->pair = p->pair16 = SlabBox{0, 0, 0, 0};
   // Per view range (subsets, the all-views entry and bin segments).
   p->subset_has_xdom.assign(p->first.size(), 0);
   for (size_t s = 0; s < p->first.size(); ++s)
@@ -975,6 +1354,19 @@ void forward_choose_variant(cbct_plan* p) {
       p->slab16 = b16;
       p->slab_smem = forward_smem(b32, 4, 0);
       p->fwd_variant = 1;
+    }
+  }
+  double row_dz = 0;
+  if ((p->fwd_pref == 4 || (p->fwd_pref == 0 && p->fwd_variant == 1)) && slab_extents(p, kPU, kPV, e, z, &row_dz) &&
+      (p->fwd_pref == 4 || row_dz < 0.99)) {
+    const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
+    const int boxz = std::max(z, 3);
+    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    if (w32 && w16 && boxz <= 256 && forward_smem(b32, 4, 0) <= (size_t)kSmemBudget &&
+        forward_smem(b16, 2, 0) <= (size_t)kSmemBudget) {
+      p->pair = b32;
+      p->pair16 = b16;
+      p->fwd_variant = 3;
     }
   }
   if (p->fwd_pref == 3 && slab_extents(p, kFU, kFV, e, z)) {
@@ -1031,8 +1423,8 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
                         ((size_t)p->g.ny * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(vol) % 16 == 0) &&
                         (!p->subset_has_xdom[s] || p->d_volT != nullptr);
   // One partial sum per block of the kernel that will run.
-  const bool fan = use_slab && p->fwd_variant == 2;
-  const int TU = fan ? kFU : kTU, TV = fan ? kFV : kTV;
+  const bool fan = use_slab && p->fwd_variant == 2, pair = use_slab && p->fwd_variant == 3;
+  const int TU = fan ? kFU : pair ? kPU : kTU, TV = fan ? kFV : pair ? kPV : kTV;
   const size_t nblocks = (size_t)((p->g.width + TU - 1) / TU) * ((p->g.height + TV - 1) / TV) * cnt;
   if (norm2_out) {
     if (nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");

@@ -142,7 +142,10 @@ constexpr int kTU = 16;
 constexpr int kTV = 16;
 constexpr int kTS = 8;
 constexpr int kBoxY = 10;
-constexpr int kNStage = 2;
+#ifndef CBCT_NSTAGE
+#define CBCT_NSTAGE 2
+#endif
+constexpr int kNStage = CBCT_NSTAGE;
 constexpr int kSlabBase = -1;      // slab m covers texel rows [kSlabBase + m*kTS, +kTS)
 constexpr int kMaxSlabs = 260;
 constexpr int kSmemBudget = 200 * 1024;
@@ -157,7 +160,7 @@ constexpr int kFanWidths[] = {24, 40, 56, 72};
 // Row-pair forward projector: kPU detector columns x kPV rows per CTA, each
 // thread marching two vertically adjacent rays of one column.
 #ifndef CBCT_PAIR_ROWS
-#define CBCT_PAIR_ROWS 32
+#define CBCT_PAIR_ROWS 16
 #endif
 #ifndef CBCT_PAIR_COLS
 #define CBCT_PAIR_COLS 16

@@ -448,6 +448,20 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
 // slab kernel computes for that ray (same texels, same operations, same
 // order), so results are bitwise equal.  Other pairs (rays clipped by the top
 // or bottom face, or far apart in z) run slab_samples for each ray.
+// The row-pair kernel keeps one TMA stage: with 16x16 tiles its box is small
+// enough for six CTAs per SM, and the other CTAs' work covers each CTA's wait
+// for its next slab (two stages would halve the CTAs per SM).
+#ifndef CBCT_PAIR_STAGES
+#define CBCT_PAIR_STAGES 1
+#endif
+constexpr int kPairStages = CBCT_PAIR_STAGES;
+
+struct PairShared {
+  uint64_t bars[kPairStages];
+  int mlo, mhi, abort_flag;
+  double red[8];
+};
+
 // One sample of a paired ray: (lower ray's value, upper ray's value).
 template <class V, int BX, bool CHECK>
 __device__ __forceinline__ float2 pair_eval(const V* __restrict__ s, float k, float2 c0, float2 dc, float zl0,
@@ -518,20 +532,24 @@ __device__ __forceinline__ void pair_samples(const V* __restrict__ s, float& kf,
   kf = ke;
 }
 
-// CTAs per SM the register budget is sized for (shared memory allows two fp32
-// or three 16-bit boxes of a 256-thread tile).
+// CTAs per SM the register budget is sized for: 80 registers (no spills) at
+// six 128-thread CTAs, as many as the fp32 boxes of 16x16 tiles leave room for.
 template <class V>
 constexpr int pair_min_blocks() {
-  return kPairThreads >= 256 ? (sizeof(V) == 4 ? 2 : 3) : (sizeof(V) == 4 ? 3 : 5);
+#ifdef CBCT_PAIR_MINB
+  return CBCT_PAIR_MINB;
+#else
+  return kPairThreads >= 256 ? 3 : 6;
+#endif
 }
 
 template <class V, int BX, bool CHECK>
 __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     fwd_pair_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
-                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ, FwdOut o,
-                    int* flags) {
+                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
+                    int nsl_max, FwdOut o, int* flags) {
   extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ SlabShared sh;
+  __shared__ PairShared sh;
   unsigned char* smem_raw =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
   constexpr int BXY = BX * kBoxY;
@@ -575,7 +593,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     sh.mlo = INT_MAX;
     sh.mhi = INT_MIN;
     sh.abort_flag = 0;
-    for (int s = 0; s < kNStage; ++s) mbar_init(&sh.bars[s], 1);
+    for (int s = 0; s < kPairStages; ++s) mbar_init(&sh.bars[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -601,13 +619,20 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   __syncthreads();
   const int mlo = sh.mlo, mhi = sh.mhi;
   int nslab = (mhi >= mlo) ? (mhi - mlo + 1) : 0;
-  if (nslab > kMaxSlabs) {
+  if (nslab > nsl_max) {
     if (tid == 0) atomicAdd(&flags[0], 1);
     nslab = 0;
   }
+  // Per-slab footprints (e min, e max, z min, z max) after the boxes.
+  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
+  int* const emin = reinterpret_cast<int*>(smem_raw + kPairStages * stage_stride);
+  int* const emax = emin + nsl_max;
+  int* const zmin = emax + nsl_max;
+  int* const zmax = zmin + nsl_max;
   for (int i = tid; i < nslab; i += blockDim.x) {
-    sh.emin[i] = INT_MAX; sh.emax[i] = INT_MIN;
-    sh.zmin[i] = INT_MAX; sh.zmax[i] = INT_MIN;
+    emin[i] = INT_MAX; emax[i] = INT_MIN;
+    zmin[i] = INT_MAX; zmax[i] = INT_MIN;
   }
   __syncthreads();
   // Footprint of every slab: the tile's four corner rays at the slab's two
@@ -628,33 +653,31 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     const float cz = fmaf(t * dz, gc.kz, gc.bz);
     const int fe = min(max(int(floorf(fminf(fmaxf(ce, -1.0e5f), 1.0e5f))), -1), ne - 1);
     const int fz = min(max(int(floorf(fminf(fmaxf(cz, -1.0e5f), 1.0e5f))), -1), gc.nz - 1);
-    atomicMin(&sh.emin[i], fe);
-    atomicMax(&sh.emax[i], fe);
-    atomicMin(&sh.zmin[i], fz);
-    atomicMax(&sh.zmax[i], fz);
+    atomicMin(&emin[i], fe);
+    atomicMax(&emax[i], fe);
+    atomicMin(&zmin[i], fz);
+    atomicMax(&zmax[i], fz);
   }
   __syncthreads();
 
-  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
-  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
   const unsigned maxidx = unsigned(BXY * (BZ - 1) - BX - 2);   // two-plane loads stay in the box
   const unsigned maxidx3 = unsigned(BXY * BZ - BX - 2);        // the third plane's loads
   auto origin = [&](int i, int& oe, int& od, int& oz, int& m) {
     m = (vp.dsgn > 0) ? mlo + i : mhi - i;
     const int ii = m - mlo;
-    oe = (sh.emin[ii] - 1) & ~(int(16 / sizeof(V)) - 1);   // 16-byte aligned x start
+    oe = (emin[ii] - 1) & ~(int(16 / sizeof(V)) - 1);   // 16-byte aligned x start
     od = kSlabBase + m * kTS;
-    oz = sh.zmin[ii] - 1;
+    oz = zmin[ii] - 1;
   };
   auto issue = [&](int i) {
     int oe, od, oz, m;
     origin(i, oe, od, oz, m);
-    uint64_t* bar = &sh.bars[i % kNStage];
+    uint64_t* bar = &sh.bars[i % kPairStages];
     mbar_arrive_expect_tx(bar, box_bytes);
-    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, oe, od, oz, bar);
+    tma_load_3d(smem_raw + (i % kPairStages) * stage_stride, map, oe, od, oz, bar);
   };
   if (tid == 0) {
-    for (int i = 0; i < min(kNStage, nslab); ++i) issue(i);
+    for (int i = 0; i < min(kPairStages, nslab); ++i) issue(i);
   }
 
   float acca = 0.f, accb = 0.f;   // paired: lower / upper ray
@@ -662,8 +685,8 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   int bad = 0;
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
-    const int slot = i % kNStage;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
+    const int slot = i % kPairStages;
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, kWaitLimit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;
@@ -673,7 +696,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     origin(i, oe, od, oz, m);
     if (CHECK && tid == 0) {
       const int ii = m - mlo;
-      if (sh.emax[ii] + 2 - oe >= BX || sh.zmax[ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
+      if (emax[ii] + 2 - oe >= BX || zmax[ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
     }
     const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
     const float lo = float(od), hi = lo + float(kTS);
@@ -704,14 +727,14 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
       }
     }
     __syncthreads();
-    if (tid == 0 && i + kNStage < nslab) {
+    if (tid == 0 && i + kPairStages < nslab) {
       fence_proxy_async();
-      issue(i + kNStage);
+      issue(i + kPairStages);
     }
   }
   if (sh.abort_flag && tid == 0) {
-    for (int i = done; i < min(done + kNStage, nslab); ++i)
-      (void)mbar_wait_bounded(&sh.bars[i % kNStage], (i / kNStage) & 1, kWaitLimit);
+    for (int i = done; i < min(done + kPairStages, nslab); ++i)
+      (void)mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit);
   }
   if (CHECK) {
     // every sample of a hit ray must be consumed
@@ -1061,6 +1084,12 @@ static int slabs_max(const cbct_geometry& g) {
   return (std::max(g.nx, g.ny) + 1 - kSlabBase + kTS - 1) / kTS + 1;
 }
 
+// Dynamic shared memory of a row-pair launch: kPairStages boxes (128-byte
+// aligned), the per-slab footprints, alignment slack.
+static size_t pair_smem(const SlabBox& b, size_t es, int nsl) {
+  return kPairStages * ((b.bx * b.by * b.bz * es + 127) & ~size_t(127)) + 4 * sizeof(int) * (size_t)nsl + 128;
+}
+
 template <class V>
 const SlabBox& box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->slab : p->slab16; }
 
@@ -1094,16 +1123,17 @@ void launch_pair(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, int
   const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
   const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
                                   volT ? p->g.nx : p->g.ny, p->g.nz, b);
-  const size_t smem = forward_smem(b, sizeof(V), 0);
+  const int nsl = slabs_max(p->g);
+  const size_t smem = pair_smem(b, sizeof(V), nsl);
   const dim3 grid((p->g.width + kPU - 1) / kPU, (p->g.height + kPV - 1) / kPV, cnt);
   if (p->debug_checks) {
     auto k = fwd_pair_kernel<V, BX, true>;
     ensure_smem_attr((const void*)k, smem);
-    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, nsl, o, p->d_flags);
   } else {
     auto k = fwd_pair_kernel<V, BX, false>;
     ensure_smem_attr((const void*)k, smem);
-    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
+    k<<<grid, kPairThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, nsl, o, p->d_flags);
   }
   check_launch("fwd_pair_kernel");
 }
@@ -1205,7 +1235,7 @@ template <class V>
 void prepare_typed(const cbct_plan* p) {
   if (p->fwd_variant == 3) {
     const SlabBox& b = pair_box_for<V>(p);
-    const size_t ps = forward_smem(b, sizeof(V), 0);
+    const size_t ps = pair_smem(b, sizeof(V), slabs_max(p->g));
     switch (b.bx) {
       case 40: prepare_pair_width<V, 40>(ps); break;
       case 56: prepare_pair_width<V, 56>(ps); break;
@@ -1362,8 +1392,9 @@ void forward_choose_variant(cbct_plan* p) {
     const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
     const int boxz = std::max(z, 3);
     const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
-    if (w32 && w16 && boxz <= 256 && forward_smem(b32, 4, 0) <= (size_t)kSmemBudget &&
-        forward_smem(b16, 2, 0) <= (size_t)kSmemBudget) {
+    const int nsl = slabs_max(p->g);
+    if (w32 && w16 && boxz <= 256 && pair_smem(b32, 4, nsl) <= (size_t)kSmemBudget &&
+        pair_smem(b16, 2, nsl) <= (size_t)kSmemBudget) {
       p->pair = b32;
       p->pair16 = b16;
       p->fwd_variant = 3;

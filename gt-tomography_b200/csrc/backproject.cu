@@ -266,15 +266,17 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
       const float U = 1.f - yr / gc.SAD;
       wt = 1.f / (U * U);
     }
-    const float fu = floorf(cu);
+    // Floors and the box index on the FMA pipe (exact for |cv| < 2^22; the
+    // index is clamped into the box below whatever it is).
+    const float fu = floor_small(cu);
     const float au = cu - fu;
     const float2 tu = make_float2(au, au);
-    const float fub = fu;
+    const float fubc = fu + kRoundC;
 #pragma unroll
     for (int q = 0; q < kZT; ++q) {
-      const float fv = floorf(cv);
+      const float fv = floor_small(cv);
       const float av = cv - fv;
-      const int idx0 = int(fmaf(fv, float(BU), fub));
+      const int idx0 = int_of_biased(fmaf(fv, float(BU), fubc));
       const unsigned idx = min((unsigned)idx0, maxidx);
       const float* t = sp + idx;
       const float2 r0 = make_float2(t[0], t[BU]);        // (u0,v0) (u0,v1)

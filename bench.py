@@ -125,9 +125,9 @@ class Workload:
         return 2 + 1 + 1            # transpose + forward, FDK filter, FDK back-projection
 
 
-FORWARD_KERNELS = {"auto": 0, "slab": 1, "gather": 2, "fan": 3, "pair": 4}
-FORWARD_KERNEL_NAMES = {"tma-pair": "fwd_pair_kernel", "tma-slab": "fwd_slab_kernel", "tma-fan": "fwd_fan_kernel",
-                        "gather": "fwd_gather_kernel"}
+FORWARD_KERNELS = {"auto": 0, "slab": 1, "gather": 2, "fan": 3, "pair": 4, "quad": 5}
+FORWARD_KERNEL_NAMES = {"tma-quad": "fwd_quad_kernel", "tma-pair": "fwd_pair_kernel", "tma-slab": "fwd_slab_kernel",
+                        "tma-fan": "fwd_fan_kernel", "gather": "fwd_gather_kernel"}
 
 
 def make_inputs(wl: Workload, gtb, dev, forward_kernel: str = "auto"):

@@ -398,7 +398,8 @@ cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_ou
 
 const char* cbct_plan_forward_variant(const cbct_plan* plan) {
   if (!plan) return "";
-  return plan->fwd_variant == 3   ? "tma-pair"
+  return plan->fwd_variant == 4   ? "tma-quad"
+         : plan->fwd_variant == 3 ? "tma-pair"
          : plan->fwd_variant == 2 ? "tma-fan"
          : plan->fwd_variant == 1 ? "tma-slab"
                                   : "gather";
@@ -412,8 +413,8 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
     } else if (option == CBCT_OPT_FORCE_GATHER || option == CBCT_OPT_FORWARD_KERNEL) {
       if (option == CBCT_OPT_FORCE_GATHER) plan->force_gather = value != 0;
       else {
-        CBCT_REQUIRE(value >= 0 && value <= 4,
-                     "forward kernel must be 0 (automatic), 1 (slab), 2 (gather), 3 (fan) or 4 (row pairs)");
+        CBCT_REQUIRE(value >= 0 && value <= 5, "forward kernel must be 0 (automatic), 1 (slab), 2 (gather), 3 (fan), "
+                                              "4 (row pairs) or 5 (row quads)");
         plan->fwd_pref = value;
       }
       graph_cache_free(plan);

@@ -2,14 +2,15 @@
 //
 // Which forward projector is fastest depends on the geometry: the slab kernel
 // (16x16 ray tiles, per-ray trilinear samples from TMA boxes), the row-pair
-// kernel (16x32 tiles, two rays of a column per thread sharing their in-plane
-// interpolation), the fan kernel (8x32 tiles, e/d interpolation shared by a
+// and row-quad kernels (two or four rays of a column per thread sharing their
+// in-plane interpolation), the fan kernel (8x32 tiles, e/d interpolation shared by a
 // detector column; larger boxes), or the gather kernel (no staging); likewise
 // the TMA-staged and the plain back-projector.  The autotuner runs every
 // candidate the plan can use on the plan's largest subset (one warm-up and
 // three timed launches each, CUDA events on the caller's stream) and keeps the
 // fastest.  All candidates give
-// results within FP32 rounding of each other (slab, pair and fan bitwise equal).
+// results within FP32 rounding of each other (slab, pair, quad and fan bitwise
+// equal).
 // No counterpart in the reference.
 #include <vector>
 
@@ -42,7 +43,7 @@ float time_ms(cudaStream_t st, F&& f) {
 
 void plan_autotune(cbct_plan* p, float* times, cudaStream_t st) {
   CBCT_REQUIRE(p != nullptr, "plan is NULL");
-  for (int i = 0; i < 6; ++i) times[i] = -1.f;
+  for (int i = 0; i < 7; ++i) times[i] = -1.f;
   int s = 0;
   for (int k = 1; k < p->n_subsets; ++k)
     if (p->count[k] > p->count[s]) s = k;
@@ -53,13 +54,13 @@ void plan_autotune(cbct_plan* p, float* times, cudaStream_t st) {
   try {
     fill_launch(vol, nv, 0.01f, st);
     fill_launch(proj, np, 0.01f, st);
-    // forward: slab (1), fan (3), gather (2), pairs (4); the variant must be
-    // the one asked for; slot = its entry of times[]
-    const int prefs[4] = {1, 3, 2, 4}, want[4] = {1, 2, 0, 3}, slot[4] = {0, 1, 2, 5};
+    // forward: slab (1), fan (3), gather (2), pairs (4), quads (5); the variant
+    // must be the one asked for; slot = its entry of times[]
+    const int prefs[5] = {1, 3, 2, 4, 5}, want[5] = {1, 2, 0, 3, 4}, slot[5] = {0, 1, 2, 5, 6};
     const int saved_pref = p->fwd_pref;
     int best = -1;
     float best_ms = 0.f;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 5; ++c) {
       p->fwd_pref = prefs[c];
       forward_choose_variant(p);
       forward_prepare(p);

@@ -168,14 +168,23 @@ constexpr int kFanWidths[] = {24, 40, 56, 72};
 constexpr int kPU = CBCT_PAIR_COLS;
 constexpr int kPV = CBCT_PAIR_ROWS;
 constexpr int kPairThreads = kPU * kPV / 2;
+// Row-quad forward projector: kQU columns x kQV rows per CTA, four adjacent
+// rows of a column per thread.
+#ifndef CBCT_QUAD_ROWS
+#define CBCT_QUAD_ROWS 32
+#endif
+constexpr int kQU = 16;
+constexpr int kQV = CBCT_QUAD_ROWS;
+constexpr int kQuadThreads = kQU * kQV / 4;
 
-// Forward-projector blocks per view: the largest of the slab, pair and fan
+// Forward-projector blocks per view: the largest of the slab, pair, quad and fan
 // tilings (one FP64 partial sum per block).
 inline size_t forward_tiles(int W, int H) {
   const size_t slab = (size_t)((W + kTU - 1) / kTU) * ((H + kTV - 1) / kTV);
   const size_t pair = (size_t)((W + kPU - 1) / kPU) * ((H + kPV - 1) / kPV);
+  const size_t quad = (size_t)((W + kQU - 1) / kQU) * ((H + kQV - 1) / kQV);
   const size_t fan = (size_t)((W + kFU - 1) / kFU) * ((H + kFV - 1) / kFV);
-  return std::max(std::max(slab, pair), fan);
+  return std::max(std::max(slab, pair), std::max(quad, fan));
 }
 
 
@@ -193,11 +202,14 @@ struct cbct_plan {
   int device = 0;
   int max_subset = 0;
 
-  // forward variant: 0 = gather (global loads), 1 = TMA slab, 2 = TMA fan, 3 = TMA row pairs
+  // forward variant: 0 = gather (global loads), 1 = TMA slab, 2 = TMA fan, 3 = TMA row pairs,
+  // 4 = TMA row quads
   int fwd_variant = 0;
-  int fwd_pref = 0;         // CBCT_OPT_FORWARD_KERNEL: 0 automatic, 1 slab, 2 gather, 3 fan, 4 pair
+  int fwd_pref = 0;         // CBCT_OPT_FORWARD_KERNEL: 0 automatic, 1 slab, 2 gather, 3 fan, 4 pair, 5 quad
   cbct::SlabBox pair{};     // row-pair kernel box for fp32 storage
   cbct::SlabBox pair16{};   // row-pair kernel box for 16-bit storage
+  cbct::SlabBox quad{};     // row-quad kernel box for fp32 storage
+  cbct::SlabBox quad16{};   // row-quad kernel box for 16-bit storage
   cbct::SlabBox fan{};      // fan kernel box for fp32 storage
   cbct::SlabBox fan16{};    // fan kernel box for 16-bit storage
   int fan_lz = 0;           // line length (planes) of the fan kernel, odd

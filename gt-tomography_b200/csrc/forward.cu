@@ -758,6 +758,362 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   fwd_block_partial(o, sq, sh.red, tid);
 }
 
+// ------------------------------------------------------------------ row quads
+// The row-pair argument for four adjacent rows of a column: when all four rays
+// leave through the side faces (one clip) and, sorted by z, each lies less
+// than two texels above the lowest at both ends of the ray, their planes are
+// among the lowest ray's fz .. fz + 3.  One thread marches the quad: one e/d
+// position, four planes interpolated in e and d (16 shared loads for four
+// samples), each ray's own z lerp on its two planes.  Values are the slab
+// kernel's for every ray, so results are bitwise equal.  Quads that do not
+// qualify run as two pairs (or single rays) exactly as the row-pair kernel.
+
+// One sample of a quad (rays sorted by z; z0/dz hold their z start and step).
+template <class V, int BX, bool CHECK>
+__device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, float2 c0, float2 dc, float4 z0,
+                                            float4 dz, float cmo, unsigned maxidx, int& bad) {
+  constexpr int BXY = BX * kBoxY;
+  const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
+  const float fe = floor_small(pq.x), fd = floor_small(pq.y);
+  const float2 aed = __fadd2_rn(pq, make_float2(-fe, -fd));
+  const float c0z = fmaf(k, dz.x, z0.x), c1z = fmaf(k, dz.y, z0.y);
+  const float c2z = fmaf(k, dz.z, z0.z), c3z = fmaf(k, dz.w, z0.w);
+  const float f0 = floor_small(c0z), f1 = floor_small(c1z), f2 = floor_small(c2z), f3 = floor_small(c3z);
+  const float s1 = f1 - f0, s2 = f2 - f0, s3 = f3 - f0;   // 0, 1 or 2
+  const int idx0 = int_of_biased(fmaf(f0, float(BXY), fmaf(fd, float(BX), fe)) + cmo);
+  if (CHECK) {
+    const float smax = fmaxf(s1, fmaxf(s2, s3)), smin = fminf(s1, fminf(s2, s3));
+    bad |= ((unsigned)idx0 > maxidx) | (smax >= 1.f && (unsigned)idx0 + 2u * BXY > maxidx) | (smax > 2.f) |
+           (smin < 0.f);
+  }
+  // planes fz, fz + 1 from q; fz + 2, fz + 3 from q2 (in the box whenever a ray
+  // needs them; clamped otherwise)
+  const V* q = s + min((unsigned)idx0, maxidx);
+  const V* q2 = s + min((unsigned)idx0 + 2u * BXY, maxidx);
+  const float2 te = make_float2(aed.x, aed.x);
+  const float2 e0 = lerp2(make_float2(sm_f(q[0]), sm_f(q[BX])), make_float2(sm_f(q[1]), sm_f(q[BX + 1])), te);
+  const float2 e1 = lerp2(make_float2(sm_f(q[BXY]), sm_f(q[BXY + BX])),
+                          make_float2(sm_f(q[BXY + 1]), sm_f(q[BXY + BX + 1])), te);
+  const float2 e2 = lerp2(make_float2(sm_f(q2[0]), sm_f(q2[BX])), make_float2(sm_f(q2[1]), sm_f(q2[BX + 1])), te);
+  const float2 e3 = lerp2(make_float2(sm_f(q2[BXY]), sm_f(q2[BXY + BX])),
+                          make_float2(sm_f(q2[BXY + 1]), sm_f(q2[BXY + BX + 1])), te);
+  const float2 td = make_float2(aed.y, aed.y);
+  const float2 d01 = lerp2(make_float2(e0.x, e1.x), make_float2(e0.y, e1.y), td);   // planes fz, fz + 1
+  const float2 d23 = lerp2(make_float2(e2.x, e3.x), make_float2(e2.y, e3.y), td);   // planes fz + 2, fz + 3
+  auto ray = [&](float sk, float cz, float fz) {
+    const float lo = sk < 0.5f ? d01.x : (sk < 1.5f ? d01.y : d23.x);
+    const float hi = sk < 0.5f ? d01.y : (sk < 1.5f ? d23.x : d23.y);
+    return fmaf(cz - fz, hi - lo, lo);
+  };
+  return make_float4(fmaf(c0z - f0, d01.y - d01.x, d01.x), ray(s1, c1z, f1), ray(s2, c2z, f2), ray(s3, c3z, f3));
+}
+
+// The quad's samples inside one slab, each ray's values added in ray order.
+template <class V, int BX, int SGN, bool CHECK>
+__device__ __forceinline__ void quad_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
+                                             float dce, float dcd, float idcd, float4 z0, float4 dz, float lo,
+                                             float hi, float cmo, unsigned maxidx, float4& acc, int& bad) {
+  const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
+  auto out_at = [&](float k) {
+    const float x = fmaf(k, dcd, cd0);
+    return SGN > 0 ? (x >= hi) : (x < lo);
+  };
+  float ke = ceilf(((SGN > 0 ? hi : lo) - cd0) * idcd);
+  ke = fminf(fmaxf(ke, kf), Nf);
+  while (ke > kf && out_at(ke - 1.f)) ke -= 1.f;
+  while (ke < Nf && !out_at(ke)) ke += 1.f;
+  for (float k = kf; k < ke; k += 1.f) {
+    const float4 v = quad_eval<V, BX, CHECK>(s, k, c0, dc, z0, dz, cmo, maxidx, bad);
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+    acc.w += v.w;
+  }
+  kf = ke;
+}
+
+// Two rays of one column (rows a, b) outside a quad: a pair when they qualify,
+// else each on its own.  Frame coordinates: (ce0, cd0, dce, dcd, idcd) per ray.
+struct RayFrame {
+  float ce0, cd0, dce, dcd, idcd, c0z, dcz;
+};
+
+__device__ __forceinline__ RayFrame ray_frame(const Ray& r, int dom) {
+  RayFrame f;
+  f.ce0 = dom ? r.c0x : r.c0y;
+  f.dce = dom ? r.dcx : r.dcy;
+  f.cd0 = dom ? r.c0y : r.c0x;
+  f.dcd = dom ? r.dcy : r.dcx;
+  f.idcd = 1.f / f.dcd;
+  f.c0z = r.c0z;
+  f.dcz = r.dcz;
+  return f;
+}
+
+// Pair test of the row-pair kernel: 1 = pair with a lower, -1 = pair with b
+// lower, 0 = no pair.
+__device__ __forceinline__ int pair_kind(const Ray& ra, const Ray& rb, bool hit_a, bool hit_b, float Nf) {
+  if (!(hit_a && hit_b && ra.a1 == rb.a1 && ra.a2 == rb.a2)) return 0;
+  const float d0 = rb.c0z - ra.c0z;
+  const float d1 = fmaf(Nf - 1.f, rb.dcz, rb.c0z) - fmaf(Nf - 1.f, ra.dcz, ra.c0z);
+  if (d0 >= 2e-3f && d0 <= 0.998f && d1 >= 2e-3f && d1 <= 0.998f) return 1;
+  if (d0 <= -2e-3f && d0 >= -0.998f && d1 <= -2e-3f && d1 >= -0.998f) return -1;
+  return 0;
+}
+
+template <class V, int BX, int SGN, bool CHECK>
+__device__ __forceinline__ void half_samples(const V* __restrict__ s, int kind, bool hit_a, bool hit_b,
+                                             const RayFrame& fa, const RayFrame& fb, float& kfa, float& kfb,
+                                             float Nf, float lo, float hi, float cmo, unsigned maxidx,
+                                             unsigned maxidx3, float& acca, float& accb, int& bad) {
+  if (kind != 0) {
+    const bool al = kind > 0;
+    float accl = al ? acca : accb, accu = al ? accb : acca;
+    pair_samples<V, BX, SGN, CHECK>(s, kfa, Nf, fa.ce0, fa.cd0, fa.dce, fa.dcd, fa.idcd, al ? fa.c0z : fb.c0z,
+                                    al ? fa.dcz : fb.dcz, al ? fb.c0z : fa.c0z, al ? fb.dcz : fa.dcz, lo, hi, cmo,
+                                    maxidx, maxidx3, accl, accu, bad);
+    acca = al ? accl : accu;
+    accb = al ? accu : accl;
+    return;
+  }
+  if (hit_a)
+    slab_samples<V, BX, SGN, CHECK>(s, kfa, Nf, fa.ce0, fa.cd0, fa.c0z, fa.dce, fa.dcd, fa.idcd, fa.dcz, lo, hi,
+                                    cmo, maxidx, acca, bad);
+  if (hit_b)
+    slab_samples<V, BX, SGN, CHECK>(s, kfb, Nf, fb.ce0, fb.cd0, fb.c0z, fb.dce, fb.dcd, fb.idcd, fb.dcz, lo, hi,
+                                    cmo, maxidx, accb, bad);
+}
+
+// CTAs per SM the register budget is sized for: four 128-thread CTAs (124
+// registers, no spills), as many as the fp32 boxes of 16x32 tiles leave room for.
+template <class V>
+constexpr int quad_min_blocks() {
+#ifdef CBCT_QUAD_MINB
+  return CBCT_QUAD_MINB;
+#else
+  return kQuadThreads >= 256 ? 2 : kQuadThreads >= 128 ? 4 : 6;
+#endif
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
+    fwd_quad_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
+                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
+                    int nsl_max, FwdOut o, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ PairShared sh;
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  constexpr int BXY = BX * kBoxY;
+  const ViewParams vp = views[blockIdx.z];
+  const int dom = vp.dom;
+  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const int tid = threadIdx.x;
+  const int p = blockIdx.z;
+  const int u0 = blockIdx.x * kQU, v0 = blockIdx.y * kQV;
+  const int u = u0 + (tid % kQU), vq = v0 + 4 * (tid / kQU);
+  const int uc = min(u, gc.W - 1);
+  const float Nf = float(gc.N);
+  Ray r[4];
+  bool act[4], hit[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    act[i] = (u < gc.W) && (vq + i < gc.H);
+    r[i] = make_ray(vp, gc, uc, min(vq + i, gc.H - 1));
+    hit[i] = act[i] && (r[i].a2 > r[i].a1);
+  }
+  RayFrame f[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) f[i] = ray_frame(r[i], dom);
+  // Quad test: one clip; sorted by z (rows run one way), every ray within
+  // [0.002, 1.998] texels above the lowest at both ends.
+  bool quad = hit[0] && hit[1] && hit[2] && hit[3];
+#pragma unroll
+  for (int i = 1; i < 4; ++i) quad = quad && r[i].a1 == r[0].a1 && r[i].a2 == r[0].a2;
+  const bool up = r[1].c0z > r[0].c0z;   // z grows with the row
+  if (quad) {
+    const int lo_i = up ? 0 : 3;
+    const float zs = r[lo_i].c0z, ze = fmaf(Nf - 1.f, r[lo_i].dcz, r[lo_i].c0z);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (i == lo_i) continue;
+      const float d0 = r[i].c0z - zs, d1 = fmaf(Nf - 1.f, r[i].dcz, r[i].c0z) - ze;
+      quad = quad && d0 >= 2e-3f && d0 <= 1.998f && d1 >= 2e-3f && d1 <= 1.998f;
+    }
+  }
+  // Sorted z parameters of the quad (lowest first).
+  const float4 qz0 = up ? make_float4(f[0].c0z, f[1].c0z, f[2].c0z, f[3].c0z)
+                        : make_float4(f[3].c0z, f[2].c0z, f[1].c0z, f[0].c0z);
+  const float4 qdz = up ? make_float4(f[0].dcz, f[1].dcz, f[2].dcz, f[3].dcz)
+                        : make_float4(f[3].dcz, f[2].dcz, f[1].dcz, f[0].dcz);
+  const int kind01 = quad ? 0 : pair_kind(r[0], r[1], hit[0], hit[1], Nf);
+  const int kind23 = quad ? 0 : pair_kind(r[2], r[3], hit[2], hit[3], Nf);
+  const float ke_ = dom ? gc.kx : gc.ky, be = dom ? gc.bx : gc.by;
+  const float kd = dom ? gc.ky : gc.kx, bd = dom ? gc.by : gc.bx;
+  const float Se = dom ? vp.Sx : vp.Sy, Sd = dom ? vp.Sy : vp.Sx;
+
+  if (tid == 0) {
+    sh.mlo = INT_MAX;
+    sh.mhi = INT_MIN;
+    sh.abort_flag = 0;
+    for (int st = 0; st < kPairStages; ++st) mbar_init(&sh.bars[st], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  {
+    int mn = INT_MAX, mx = INT_MIN;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (!hit[i]) continue;
+      const int m0 = (max(int(floorf(f[i].cd0)), kSlabBase) - kSlabBase) / kTS;
+      const int m1 = (max(int(floorf(fmaf(Nf - 1.f, f[i].dcd, f[i].cd0))), kSlabBase) - kSlabBase) / kTS;
+      mn = min(mn, min(m0, m1));
+      mx = max(mx, max(m0, m1));
+    }
+    if (mn <= mx) {
+      atomicMin(&sh.mlo, mn);
+      atomicMax(&sh.mhi, mx);
+    }
+  }
+  __syncthreads();
+  const int mlo = sh.mlo, mhi = sh.mhi;
+  int nslab = (mhi >= mlo) ? (mhi - mlo + 1) : 0;
+  if (nslab > nsl_max) {
+    if (tid == 0) atomicAdd(&flags[0], 1);
+    nslab = 0;
+  }
+  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
+  int* const emin = reinterpret_cast<int*>(smem_raw + kPairStages * stage_stride);
+  int* const emax = emin + nsl_max;
+  int* const zmin = emax + nsl_max;
+  int* const zmax = zmin + nsl_max;
+  for (int i = tid; i < nslab; i += blockDim.x) {
+    emin[i] = INT_MAX; emax[i] = INT_MIN;
+    zmin[i] = INT_MAX; zmax[i] = INT_MIN;
+  }
+  __syncthreads();
+  const int ue = min(u0 + kQU, gc.W) - 1, ve = min(v0 + kQV, gc.H) - 1;
+  const int ne = dom ? gc.nx : gc.ny;
+  for (int qq = tid; qq < nslab * 8; qq += blockDim.x) {
+    const int i = qq >> 3, c = qq & 7;
+    const int m = mlo + i;
+    const float plane = float(kSlabBase + m * kTS + ((c & 4) ? kTS : 0));
+    const int ucc = (c & 1) ? ue : u0, vcc = (c & 2) ? ve : v0;
+    const float dx = fmaf(float(ucc), vp.Eux, vp.D0x);
+    const float dy = fmaf(float(ucc), vp.Euy, vp.D0y);
+    const float dzz = fmaf(float(vcc), vp.Evz, vp.D0z);
+    const float de = dom ? dx : dy, dd = dom ? dy : dx;
+    const float t = ((plane - bd) / kd - Sd) / dd;
+    const float ce = fmaf(fmaf(t, de, Se), ke_, be);
+    const float cz = fmaf(t * dzz, gc.kz, gc.bz);
+    const int fe = min(max(int(floorf(fminf(fmaxf(ce, -1.0e5f), 1.0e5f))), -1), ne - 1);
+    const int fz = min(max(int(floorf(fminf(fmaxf(cz, -1.0e5f), 1.0e5f))), -1), gc.nz - 1);
+    atomicMin(&emin[i], fe);
+    atomicMax(&emax[i], fe);
+    atomicMin(&zmin[i], fz);
+    atomicMax(&zmax[i], fz);
+  }
+  __syncthreads();
+
+  const unsigned maxidx = unsigned(BXY * (BZ - 1) - BX - 2);   // two-plane loads stay in the box
+  const unsigned maxidx3 = unsigned(BXY * BZ - BX - 2);        // the pair's third plane
+  auto origin = [&](int i, int& oe, int& od, int& oz, int& m) {
+    m = (vp.dsgn > 0) ? mlo + i : mhi - i;
+    const int ii = m - mlo;
+    oe = (emin[ii] - 1) & ~(int(16 / sizeof(V)) - 1);   // 16-byte aligned x start
+    od = kSlabBase + m * kTS;
+    oz = zmin[ii] - 1;
+  };
+  auto issue = [&](int i) {
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    uint64_t* bar = &sh.bars[i % kPairStages];
+    mbar_arrive_expect_tx(bar, box_bytes);
+    tma_load_3d(smem_raw + (i % kPairStages) * stage_stride, map, oe, od, oz, bar);
+  };
+  if (tid == 0) {
+    for (int i = 0; i < min(kPairStages, nslab); ++i) issue(i);
+  }
+
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);   // quad: sorted by z; else per row
+  float kf[4] = {0.f, 0.f, 0.f, 0.f};            // quad / pairs: kf[0], kf[2] lead
+  int bad = 0;
+  int done = 0;
+  for (int i = 0; i < nslab; ++i) {
+    const int slot = i % kPairStages;
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, kWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
+      break;
+    }
+    done = i + 1;
+    int oe, od, oz, m;
+    origin(i, oe, od, oz, m);
+    if (CHECK && tid == 0) {
+      const int ii = m - mlo;
+      if (emax[ii] + 2 - oe >= BX || zmax[ii] + 2 - oz >= BZ) atomicAdd(&flags[0], 1);
+    }
+    const V* sm = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
+    const float lo = float(od), hi = lo + float(kTS);
+    const float cmo = kRoundC - float(oe + od * BX + oz * BXY);
+    if (quad) {
+      if (vp.dsgn > 0)
+        quad_samples<V, BX, 1, CHECK>(sm, kf[0], Nf, f[0].ce0, f[0].cd0, f[0].dce, f[0].dcd, f[0].idcd, qz0, qdz, lo,
+                                      hi, cmo, maxidx, acc, bad);
+      else
+        quad_samples<V, BX, -1, CHECK>(sm, kf[0], Nf, f[0].ce0, f[0].cd0, f[0].dce, f[0].dcd, f[0].idcd, qz0, qdz,
+                                       lo, hi, cmo, maxidx, acc, bad);
+    } else if (vp.dsgn > 0) {
+      half_samples<V, BX, 1, CHECK>(sm, kind01, hit[0], hit[1], f[0], f[1], kf[0], kf[1], Nf, lo, hi, cmo, maxidx,
+                                    maxidx3, acc.x, acc.y, bad);
+      half_samples<V, BX, 1, CHECK>(sm, kind23, hit[2], hit[3], f[2], f[3], kf[2], kf[3], Nf, lo, hi, cmo, maxidx,
+                                    maxidx3, acc.z, acc.w, bad);
+    } else {
+      half_samples<V, BX, -1, CHECK>(sm, kind01, hit[0], hit[1], f[0], f[1], kf[0], kf[1], Nf, lo, hi, cmo, maxidx,
+                                     maxidx3, acc.x, acc.y, bad);
+      half_samples<V, BX, -1, CHECK>(sm, kind23, hit[2], hit[3], f[2], f[3], kf[2], kf[3], Nf, lo, hi, cmo, maxidx,
+                                     maxidx3, acc.z, acc.w, bad);
+    }
+    __syncthreads();
+    if (tid == 0 && i + kPairStages < nslab) {
+      fence_proxy_async();
+      issue(i + kPairStages);
+    }
+  }
+  if (sh.abort_flag && tid == 0) {
+    for (int i = done; i < min(done + kPairStages, nslab); ++i)
+      (void)mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit);
+  }
+  if (CHECK) {
+    // every sample of a hit ray must be consumed
+    if (quad) {
+      if (kf[0] != Nf) bad = 1;
+    } else {
+      if (kind01 != 0 ? kf[0] != Nf : ((hit[0] && kf[0] != Nf) || (hit[1] && kf[1] != Nf))) bad = 1;
+      if (kind23 != 0 ? kf[2] != Nf : ((hit[2] && kf[2] != Nf) || (hit[3] && kf[3] != Nf))) bad = 1;
+    }
+    if (bad) atomicAdd(&flags[0], 1);
+  }
+  // Per-row sums (the quad's are sorted by z).
+  float sum[4];
+  if (quad && !up) {
+    sum[0] = acc.w; sum[1] = acc.z; sum[2] = acc.y; sum[3] = acc.x;
+  } else {
+    sum[0] = acc.x; sum[1] = acc.y; sum[2] = acc.z; sum[3] = acc.w;
+  }
+  double sq = 0.0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float val = 0.f;
+    int k0, k1;
+    if (hit[i]) val = sum[i] * r[i].delta;
+    else if (act[i] && grown_range(vp, gc, u, vq + i, r[i], k0, k1)) val = march_global(vol, gc, r[i], k0, k1) * r[i].delta;
+    if (act[i]) sq += fwd_store(o, gc, vp, p, u, vq + i, val);
+  }
+  fwd_block_partial(o, sq, sh.red, tid);
+}
+
 // ------------------------------------------------------------------ fan
 // The rays of one detector column lie in one vertical plane (the detector's
 // v axis is the world z axis).  A ray that enters and leaves the volume
@@ -1139,6 +1495,31 @@ void launch_pair(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, int
 }
 
 template <class V>
+const SlabBox& quad_box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->quad : p->quad16; }
+
+template <class V, int BX>
+void launch_quad(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, int first, int cnt, cudaStream_t st,
+                 cbct_dtype dt) {
+  const SlabBox& b = quad_box_for<V>(p);
+  const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
+  const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
+                                  volT ? p->g.nx : p->g.ny, p->g.nz, b);
+  const int nsl = slabs_max(p->g);
+  const size_t smem = pair_smem(b, sizeof(V), nsl);
+  const dim3 grid((p->g.width + kQU - 1) / kQU, (p->g.height + kQV - 1) / kQV, cnt);
+  if (p->debug_checks) {
+    auto k = fwd_quad_kernel<V, BX, true>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kQuadThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, nsl, o, p->d_flags);
+  } else {
+    auto k = fwd_quad_kernel<V, BX, false>;
+    ensure_smem_attr((const void*)k, smem);
+    k<<<grid, kQuadThreads, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, nsl, o, p->d_flags);
+  }
+  check_launch("fwd_quad_kernel");
+}
+
+template <class V>
 const SlabBox& fan_box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->fan : p->fan16; }
 
 template <class V, int BX>
@@ -1182,6 +1563,17 @@ void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaS
     check_launch("transpose_xy_kernel");
     volT = t;
   }
+  if (p->fwd_variant == 4) {
+    switch (quad_box_for<V>(p).bx) {
+      case 40: launch_quad<V, 40>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 56: launch_quad<V, 56>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 72: launch_quad<V, 72>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 104: launch_quad<V, 104>(p, vol, volT, o, first, cnt, st, dt); break;
+      case 136: launch_quad<V, 136>(p, vol, volT, o, first, cnt, st, dt); break;
+      default: throw Error(CBCT_ERR_INTERNAL, "unsupported quad box width");
+    }
+    return;
+  }
   if (p->fwd_variant == 3) {
     switch (pair_box_for<V>(p).bx) {
       case 40: launch_pair<V, 40>(p, vol, volT, o, first, cnt, st, dt); break;
@@ -1220,6 +1612,12 @@ void prepare_width(size_t smem) {
 }
 
 template <class V, int BX>
+void prepare_quad_width(size_t smem) {
+  ensure_smem_attr((const void*)fwd_quad_kernel<V, BX, false>, smem);
+  ensure_smem_attr((const void*)fwd_quad_kernel<V, BX, true>, smem);
+}
+
+template <class V, int BX>
 void prepare_pair_width(size_t smem) {
   ensure_smem_attr((const void*)fwd_pair_kernel<V, BX, false>, smem);
   ensure_smem_attr((const void*)fwd_pair_kernel<V, BX, true>, smem);
@@ -1233,6 +1631,18 @@ void prepare_fan_width(size_t smem) {
 
 template <class V>
 void prepare_typed(const cbct_plan* p) {
+  if (p->fwd_variant == 4) {
+    const SlabBox& b = quad_box_for<V>(p);
+    const size_t qs = pair_smem(b, sizeof(V), slabs_max(p->g));
+    switch (b.bx) {
+      case 40: prepare_quad_width<V, 40>(qs); break;
+      case 56: prepare_quad_width<V, 56>(qs); break;
+      case 72: prepare_quad_width<V, 72>(qs); break;
+      case 104: prepare_quad_width<V, 104>(qs); break;
+      case 136: prepare_quad_width<V, 136>(qs); break;
+      default: break;
+    }
+  }
   if (p->fwd_variant == 3) {
     const SlabBox& b = pair_box_for<V>(p);
     const size_t ps = pair_smem(b, sizeof(V), slabs_max(p->g));
@@ -1274,12 +1684,12 @@ void prepare_typed(const cbct_plan* p) {
 // (corner-ray bounding box in the view's frame, computed in FP64): e extent
 // and z extent in elements, including margins.  False when some view cannot
 // use slabs (a ray not dominated by its view's slab axis, or too many slabs).
-static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ext_z, double* row_dz = nullptr) {
+static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ext_z) {
   const cbct_geometry& g = p->g;
   const double kx = g.nx / (double)g.lx, ky = g.ny / (double)g.ly, kz = g.nz / (double)g.lz;
   const double bx = g.nx / 2.0 - 0.5, by = g.ny / 2.0 - 0.5, bz = g.nz / 2.0 - 0.5;
   const int tiles_u = (g.width + TU - 1) / TU, tiles_v = (g.height + TV - 1) / TV;
-  struct Acc { int e = 0, z = 0, ok = 1; double dz = 0; };
+  struct Acc { int e = 0, z = 0, ok = 1; };
   std::vector<Acc> acc(host_threads());
   // The in-plane coordinate of a ray does not depend on the detector row, so the
   // e extent is a function of (view, tile column, slab); the z extent comes from
@@ -1320,8 +1730,6 @@ static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ex
             emn = std::min(emn, ce); emx = std::max(emx, ce);
             tmn = std::min(tmn, t); tmx = std::max(tmx, t);
           }
-          // z distance (texels) between the rays of adjacent detector rows
-          a.dz = std::max(a.dz, std::max(std::fabs(tmn), std::fabs(tmx)) * std::fabs((double)vp.Evz) * kz);
           // elements from floor(min)-1 to floor(max)+1 inclusive, +2 margin; the
           // kernels clamp footprints to the volume, whose extent bounds the box
           const int Ne = dom ? g.nx : g.ny;
@@ -1339,15 +1747,28 @@ static bool slab_extents(const cbct_plan* p, int TU, int TV, int& ext_e, int& ex
   });
   ext_e = ext_z = 0;
   bool ok = true;
-  double dz = 0;
   for (const Acc& a : acc) {
     ext_e = std::max(ext_e, a.e);
     ext_z = std::max(ext_z, a.z);
-    dz = std::max(dz, a.dz);
     ok = ok && a.ok;
   }
-  if (row_dz) *row_dz = dz;
   return ok;
+}
+
+// Largest z distance (texels) between the rays of adjacent detector rows at a
+// point of the volume.  A point P lies at ray parameter t = (P - S).n / SDD,
+// n the unit vector from the source towards the detector centre, so over the
+// volume t <= (SAD + hx |sin| + hy |cos|) / SDD; rows are dv apart at t = 1.
+static double row_dz_max(const cbct_plan* p) {
+  const cbct_geometry& g = p->g;
+  const double kz = g.nz / (double)g.lz, dv = double(g.fov_v) / g.height;
+  double m = 0;
+  for (int iv = 0; iv < p->n_views; ++iv) {
+    const double th = double(p->angles[iv]) * (3.14159265358979323846 / 180.0);
+    const double tmax = (g.SAD + 0.5 * g.lx * std::fabs(std::sin(th)) + 0.5 * g.ly * std::fabs(std::cos(th))) / g.SDD;
+    m = std::max(m, tmax * dv * kz);
+  }
+  return m;
 }
 
 // Chooses the forward variant and its TMA boxes from the plan geometry: the
@@ -1360,6 +1781,7 @@ void forward_choose_variant(cbct_plan* p) {
   p->slab = SlabBox{0, 0, 0, 0};
   p->fan = SlabBox{0, 0, 0, 0};
   p->pair = p->pair16 = SlabBox{0, 0, 0, 0};
+  p->quad = p->quad16 = SlabBox{0, 0, 0, 0};
   // Per view range (subsets, the all-views entry and bin segments).
   p->subset_has_xdom.assign(p->first.size(), 0);
   for (size_t s = 0; s < p->first.size(); ++s)
@@ -1386,9 +1808,9 @@ void forward_choose_variant(cbct_plan* p) {
       p->fwd_variant = 1;
     }
   }
-  double row_dz = 0;
-  if ((p->fwd_pref == 4 || (p->fwd_pref == 0 && p->fwd_variant == 1)) && slab_extents(p, kPU, kPV, e, z, &row_dz) &&
-      (p->fwd_pref == 4 || row_dz < 0.99)) {
+  const double row_dz = row_dz_max(p);
+  if ((p->fwd_pref == 4 || (p->fwd_pref == 0 && p->fwd_variant == 1 && row_dz < 0.99)) &&
+      slab_extents(p, kPU, kPV, e, z)) {
     const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
     const int boxz = std::max(z, 3);
     const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
@@ -1398,6 +1820,21 @@ void forward_choose_variant(cbct_plan* p) {
       p->pair = b32;
       p->pair16 = b16;
       p->fwd_variant = 3;
+    }
+  }
+  // Row quads where four adjacent rows stay within two z texels (3 row steps
+  // under 0.66 texel each, margin included).
+  if ((p->fwd_pref == 5 || (p->fwd_pref == 0 && p->fwd_variant == 3 && row_dz < 0.66)) &&
+      slab_extents(p, kQU, kQV, e, z)) {
+    const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
+    const int boxz = std::max(z, 4);
+    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    const int nsl = slabs_max(p->g);
+    if (w32 && w16 && boxz <= 256 && pair_smem(b32, 4, nsl) <= (size_t)kSmemBudget &&
+        pair_smem(b16, 2, nsl) <= (size_t)kSmemBudget) {
+      p->quad = b32;
+      p->quad16 = b16;
+      p->fwd_variant = 4;
     }
   }
   if (p->fwd_pref == 3 && slab_extents(p, kFU, kFV, e, z)) {
@@ -1455,7 +1892,8 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
                         (!p->subset_has_xdom[s] || p->d_volT != nullptr);
   // One partial sum per block of the kernel that will run.
   const bool fan = use_slab && p->fwd_variant == 2, pair = use_slab && p->fwd_variant == 3;
-  const int TU = fan ? kFU : pair ? kPU : kTU, TV = fan ? kFV : pair ? kPV : kTV;
+  const bool quad = use_slab && p->fwd_variant == 4;
+  const int TU = fan ? kFU : pair ? kPU : quad ? kQU : kTU, TV = fan ? kFV : pair ? kPV : quad ? kQV : kTV;
   const size_t nblocks = (size_t)((p->g.width + TU - 1) / TU) * ((p->g.height + TV - 1) / TV) * cnt;
   if (norm2_out) {
     if (nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");

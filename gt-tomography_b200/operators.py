@@ -272,10 +272,10 @@ class Plan:
     def autotune(self, stream=None) -> dict:
         """cbct_plan_autotune: times the projector variants on the largest
         subset, keeps the fastest; returns ms per launch (None: unavailable)."""
-        t = np.zeros(6, np.float32)
+        t = np.zeros(7, np.float32)
         L.call("cbct_plan_autotune", self._h, t.ctypes.data, _stream(stream))
         names = ["forward_slab", "forward_fan", "forward_gather", "backproject_tma", "backproject_global",
-                 "forward_pair"]
+                 "forward_pair", "forward_quad"]
         out = {n: (float(v) if v >= 0 else None) for n, v in zip(names, t)}
         out["forward_variant"] = self.forward_variant()
         return out

@@ -135,17 +135,17 @@ CBCT_API cbct_status cbct_plan_destroy(cbct_plan* plan);
 CBCT_API cbct_status cbct_plan_subset(const cbct_plan* plan, int32_t s, int32_t* first_out,
                              int32_t* count_out);
 
-/* Name of the forward-projector variant the plan selected ("tma-pair", "tma-slab", "tma-fan" or
- * "gather"). */
+/* Name of the forward-projector variant the plan selected ("tma-quad", "tma-pair", "tma-slab",
+ * "tma-fan" or "gather"). */
 CBCT_API const char* cbct_plan_forward_variant(const cbct_plan* plan);
 
 /* Autotuner (no reference counterpart): runs every forward projector (slab,
- * column-fan, gather, row-pair) and back-projector (TMA-staged, global loads)
- * the plan can use on its largest subset, keeps the fastest of each for the
- * plan, and writes the timings (ms per launch; -1 where a variant is
- * unavailable) to times_ms_out[6] = {fwd slab, fwd fan, fwd gather, bp TMA,
- * bp global, fwd row-pair}.  Synchronises `stream`; allocates and frees two
- * scratch buffers. */
+ * column-fan, gather, row-pair, row-quad) and back-projector (TMA-staged,
+ * global loads) the plan can use on its largest subset, keeps the fastest of
+ * each for the plan, and writes the timings (ms per launch; -1 where a variant
+ * is unavailable) to times_ms_out[7] = {fwd slab, fwd fan, fwd gather, bp TMA,
+ * bp global, fwd row-pair, fwd row-quad}.  Synchronises `stream`; allocates
+ * and frees two scratch buffers. */
 CBCT_API cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, void* stream);
 
 /* Plan options (no reference counterpart; diagnostics of this library).
@@ -154,14 +154,15 @@ CBCT_API cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, vo
  * CBCT_OPT_FORCE_GATHER: use the global-gather forward projector. */
 #define CBCT_OPT_DEBUG_CHECKS 1
 #define CBCT_OPT_FORCE_GATHER 2
-/* CBCT_OPT_FORWARD_KERNEL: 0 = automatic (the row-pair kernel where adjacent
- * detector rows stay within one z texel of each other and its boxes fit, else
- * the per-ray slab kernel where its boxes fit, else gather), 1 = slab,
- * 2 = gather, 3 = the column-fan kernel (e/d interpolation shared by the rays
- * of a detector column; slower on B200 at the sizes measured so far), 4 = the
- * row-pair kernel (one thread marches two vertically adjacent rays of a
- * column and shares their in-plane interpolation).  Slab, fan and row-pair
- * results are bitwise equal. */
+/* CBCT_OPT_FORWARD_KERNEL: 0 = automatic (the row-quad kernel where adjacent
+ * detector rows stay within 0.66 z texel of each other, else the row-pair
+ * kernel where they stay within one texel, else the per-ray slab kernel, each
+ * where its boxes fit, else gather), 1 = slab, 2 = gather, 3 = the column-fan
+ * kernel (e/d interpolation shared by the rays of a detector column; slower on
+ * B200 at the sizes measured so far), 4 = the row-pair kernel (one thread
+ * marches two vertically adjacent rays of a column and shares their in-plane
+ * interpolation), 5 = the row-quad kernel (four rows per thread).  Slab, fan,
+ * row-pair and row-quad results are bitwise equal. */
 #define CBCT_OPT_FORWARD_KERNEL 3
 CBCT_API cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value);
 

@@ -19,7 +19,7 @@ def _phantom(case, O, seed=3):
 
 
 @pytest.mark.parametrize("name", ALL)
-@pytest.mark.parametrize("variant", ["auto", "gather", "fan", "pair"])
+@pytest.mark.parametrize("variant", ["auto", "gather", "fan", "pair", "quad"])
 def test_forward_matches_oracle(gtb, O, cuda, name, variant):
     import torch
     case = make(name)
@@ -32,6 +32,8 @@ def test_forward_matches_oracle(gtb, O, cuda, name, variant):
         plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 3)
     elif variant == "pair":
         plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 4)
+    elif variant == "quad":
+        plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 5)
     plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
     v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
     out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
@@ -55,14 +57,16 @@ def test_variant_selection(gtb, cuda):
     assert plan.forward_variant() == "tma-fan"
     plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 4)
     assert plan.forward_variant() == "tma-pair"
+    plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 5)
+    assert plan.forward_variant() == "tma-quad"
     plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, 2)
     assert plan.forward_variant() == "gather"
 
 
 @pytest.mark.parametrize("name", ["short", "cube", "offset", "aniso"])
 def test_kernels_bitwise_equal(gtb, O, cuda, name):
-    """Slab, row-pair, fan and gather kernels evaluate the same samples in the
-    same order."""
+    """Slab, row-pair, row-quad, fan and gather kernels evaluate the same
+    samples in the same order."""
     import torch
     case = make(name)
     _, vol = _phantom(case, O, seed=9)
@@ -70,15 +74,16 @@ def test_kernels_bitwise_equal(gtb, O, cuda, name):
     plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
     v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
     outs = {}
-    for k in (1, 4, 3, 2):
+    for k in (1, 4, 5, 3, 2):
         plan.set_option(gtb._lib.CBCT_OPT_FORWARD_KERNEL, k)
         out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)
         plan.forward(v, out)
         outs[plan.forward_variant()] = out
         assert plan.read_flags() == (0, 0)
-    assert set(outs) == {"tma-slab", "tma-pair", "tma-fan", "gather"}
+    assert set(outs) == {"tma-slab", "tma-pair", "tma-quad", "tma-fan", "gather"}
     assert torch.equal(outs["tma-slab"], outs["tma-fan"])
     assert torch.equal(outs["tma-slab"], outs["tma-pair"])
+    assert torch.equal(outs["tma-slab"], outs["tma-quad"])
     # the gather kernel interpolates with another FMA arrangement: equal to rounding
     a, b = outs["tma-slab"].double(), outs["gather"].double()
     assert float((a - b).norm() / b.norm()) < 1e-6
@@ -190,12 +195,13 @@ def test_forward_16bit_full_size_offset(gtb, cuda, dtype):
     b = torch.empty_like(a)
     plan.forward(v16, a, vol_dtype=gtb.CBCT_F16 if dtype == "f16" else gtb.CBCT_BF16)
     plan.forward(v16.float().contiguous(), b)
-    assert plan.forward_variant() == "tma-pair"
+    assert plan.forward_variant() == "tma-quad"
     assert torch.equal(a, b)
-    plan.set_option(L.CBCT_OPT_FORWARD_KERNEL, 1)
-    plan.forward(v16, b, vol_dtype=gtb.CBCT_F16 if dtype == "f16" else gtb.CBCT_BF16)
-    assert plan.forward_variant() == "tma-slab"
-    assert torch.equal(a, b)
+    for k, name in ((1, "tma-slab"), (4, "tma-pair")):
+        plan.set_option(L.CBCT_OPT_FORWARD_KERNEL, k)
+        plan.forward(v16, b, vol_dtype=gtb.CBCT_F16 if dtype == "f16" else gtb.CBCT_BF16)
+        assert plan.forward_variant() == name
+        assert torch.equal(a, b)
 
 
 @pytest.mark.parametrize("name", ["cube", "short"])
@@ -211,7 +217,8 @@ def test_autotune_keeps_results(gtb, O, cuda, name):
     fastest = min((v, k) for k, v in t.items() if k.startswith("forward_") and k != "forward_variant"
                   and v is not None)[1]
     assert t["forward_variant"] == {"forward_slab": "tma-slab", "forward_fan": "tma-fan",
-                                    "forward_gather": "gather", "forward_pair": "tma-pair"}[fastest]
+                                    "forward_gather": "gather", "forward_pair": "tma-pair",
+                                    "forward_quad": "tma-quad"}[fastest]
     plan.set_option(gtb._lib.CBCT_OPT_DEBUG_CHECKS, 1)
     v = torch.from_numpy(vol.astype(np.float32)).to(cuda)
     out = torch.zeros(plan.proj_shape(), dtype=torch.float32, device=cuda)

@@ -191,11 +191,11 @@ __device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
 }
 
 // Samples of one ray inside one slab.  (ce, cd, cz) are frame texel
-// coordinates; the box origin is (oe, od, oz); BX and kBoxY are the box
+// coordinates; the box origin is (oe, od, oz); BX and BY are the box
 // strides.  Consumes samples while floor(cd) stays inside the slab.
-template <class V, int BX>
+template <class V, int BX, int BY = kBoxY>
 struct SlabSample {
-  static constexpr int BXY = BX * kBoxY;
+  static constexpr int BXY = BX * BY;
   // Trilinear value of one sample whose frame coordinates are (ced.x, ced.y, cz)
   // and whose floors are (fe, fd, fz).  cmo = 1.5 * 2^23 - (box origin index):
   // the element index comes out of the mantissa of an exact sum.
@@ -226,11 +226,11 @@ struct SlabSample {
 // (ce, cd, cz) are frame texel coordinates.
 constexpr int kFwdUnroll = 2;
 
-template <class V, int BX, int SGN, bool CHECK>
+template <class V, int BX, int SGN, bool CHECK, int BY = kBoxY>
 __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
                                              float cz0, float dce, float dcd, float idcd, float dcz, float lo,
                                              float hi, float cmo, unsigned maxidx, float& acc, int& bad) {
-  using SS = SlabSample<V, BX>;
+  using SS = SlabSample<V, BX, BY>;
   const float2 c0 = make_float2(ce0, cd0), dc = make_float2(dce, dcd);
   // floor(x) >= hi <=> x >= hi and floor(x) < lo <=> x < lo, lo and hi being integers.
   auto out_at = [&](float k) {
@@ -463,11 +463,11 @@ struct PairShared {
 };
 
 // One sample of a paired ray: (lower ray's value, upper ray's value).
-template <class V, int BX, bool CHECK>
+template <class V, int BX, bool CHECK, int BY = kBoxY>
 __device__ __forceinline__ float2 pair_eval(const V* __restrict__ s, float k, float2 c0, float2 dc, float zl0,
                                             float dzl, float zu0, float dzu, float cmo, unsigned maxidx,
                                             unsigned maxidx3, int& bad) {
-  constexpr int BXY = BX * kBoxY;
+  constexpr int BXY = BX * BY;
   const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
   const float czl = fmaf(k, dzl, zl0), czu = fmaf(k, dzu, zu0);
   const float fe = floor_small(pq.x), fd = floor_small(pq.y), fzl = floor_small(czl), fzu = floor_small(czu);
@@ -496,7 +496,7 @@ constexpr int kPairUnroll = CBCT_PAIR_UNROLL;
 
 // The pair's samples inside one slab (counted as in slab_samples), each ray's
 // values added in ray order.
-template <class V, int BX, int SGN, bool CHECK>
+template <class V, int BX, int SGN, bool CHECK, int BY = kBoxY>
 __device__ __forceinline__ void pair_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
                                              float dce, float dcd, float idcd, float zl0, float dzl, float zu0,
                                              float dzu, float lo, float hi, float cmo, unsigned maxidx,
@@ -516,7 +516,7 @@ __device__ __forceinline__ void pair_samples(const V* __restrict__ s, float& kf,
       float2 v[kPairUnroll];
 #pragma unroll
       for (int q = 0; q < kPairUnroll; ++q)
-        v[q] = pair_eval<V, BX, CHECK>(s, k + float(q), c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
+        v[q] = pair_eval<V, BX, CHECK, BY>(s, k + float(q), c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
 #pragma unroll
       for (int q = 0; q < kPairUnroll; ++q) {
         accl += v[q].x;
@@ -525,7 +525,7 @@ __device__ __forceinline__ void pair_samples(const V* __restrict__ s, float& kf,
     }
   }
   for (; k < ke; k += 1.f) {
-    const float2 v = pair_eval<V, BX, CHECK>(s, k, c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
+    const float2 v = pair_eval<V, BX, CHECK, BY>(s, k, c0, dc, zl0, dzl, zu0, dzu, cmo, maxidx, maxidx3, bad);
     accl += v.x;
     accu += v.y;
   }
@@ -768,11 +768,21 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
 // kernel's for every ray, so results are bitwise equal.  Quads that do not
 // qualify run as two pairs (or single rays) exactly as the row-pair kernel.
 
+// Rows of a quad box: the slab's kTS + 1 rows and no padding.  The two quads
+// of a warp read planes two or three apart; with a plane stride of BX * 9
+// words (8 mod 32 banks for BX = 8 mod 16) those fall 16 or 24 banks apart,
+// where the padded stride (16 mod 32) puts planes two apart on the same banks.
+#ifndef CBCT_QUAD_BOXY
+#define CBCT_QUAD_BOXY 9
+#endif
+constexpr int kQuadBoxY = CBCT_QUAD_BOXY;
+static_assert(kQuadBoxY >= kTS + 1, "a quad box holds the slab's rows and the next one");
+
 // One sample of a quad (rays sorted by z; z0/dz hold their z start and step).
 template <class V, int BX, bool CHECK>
 __device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, float2 c0, float2 dc, float4 z0,
                                             float4 dz, float cmo, unsigned maxidx, int& bad) {
-  constexpr int BXY = BX * kBoxY;
+  constexpr int BXY = BX * kQuadBoxY;
   const float2 pq = __ffma2_rn(make_float2(k, k), dc, c0);
   const float fe = floor_small(pq.x), fd = floor_small(pq.y);
   const float2 aed = __fadd2_rn(pq, make_float2(-fe, -fd));
@@ -869,7 +879,7 @@ __device__ __forceinline__ void half_samples(const V* __restrict__ s, int kind, 
   if (kind != 0) {
     const bool al = kind > 0;
     float accl = al ? acca : accb, accu = al ? accb : acca;
-    pair_samples<V, BX, SGN, CHECK>(s, kfa, Nf, fa.ce0, fa.cd0, fa.dce, fa.dcd, fa.idcd, al ? fa.c0z : fb.c0z,
+    pair_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.dce, fa.dcd, fa.idcd, al ? fa.c0z : fb.c0z,
                                     al ? fa.dcz : fb.dcz, al ? fb.c0z : fa.c0z, al ? fb.dcz : fa.dcz, lo, hi, cmo,
                                     maxidx, maxidx3, accl, accu, bad);
     acca = al ? accl : accu;
@@ -877,10 +887,10 @@ __device__ __forceinline__ void half_samples(const V* __restrict__ s, int kind, 
     return;
   }
   if (hit_a)
-    slab_samples<V, BX, SGN, CHECK>(s, kfa, Nf, fa.ce0, fa.cd0, fa.c0z, fa.dce, fa.dcd, fa.idcd, fa.dcz, lo, hi,
+    slab_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.c0z, fa.dce, fa.dcd, fa.idcd, fa.dcz, lo, hi,
                                     cmo, maxidx, acca, bad);
   if (hit_b)
-    slab_samples<V, BX, SGN, CHECK>(s, kfb, Nf, fb.ce0, fb.cd0, fb.c0z, fb.dce, fb.dcd, fb.idcd, fb.dcz, lo, hi,
+    slab_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfb, Nf, fb.ce0, fb.cd0, fb.c0z, fb.dce, fb.dcd, fb.idcd, fb.dcz, lo, hi,
                                     cmo, maxidx, accb, bad);
 }
 
@@ -904,7 +914,7 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
   __shared__ PairShared sh;
   unsigned char* smem_raw =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
-  constexpr int BXY = BX * kBoxY;
+  constexpr int BXY = BX * kQuadBoxY;
   const ViewParams vp = views[blockIdx.z];
   const int dom = vp.dom;
   const CUtensorMap* map = dom ? &map_v : &map_t;
@@ -982,7 +992,7 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
     if (tid == 0) atomicAdd(&flags[0], 1);
     nslab = 0;
   }
-  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t box_bytes = uint32_t(BX * kQuadBoxY * BZ * sizeof(V));
   const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
   int* const emin = reinterpret_cast<int*>(smem_raw + kPairStages * stage_stride);
   int* const emax = emin + nsl_max;
@@ -1828,7 +1838,7 @@ void forward_choose_variant(cbct_plan* p) {
       slab_extents(p, kQU, kQV, e, z)) {
     const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
     const int boxz = std::max(z, 4);
-    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    const SlabBox b32{w32, kQuadBoxY, boxz, 1}, b16{w16, kQuadBoxY, boxz, 1};
     const int nsl = slabs_max(p->g);
     if (w32 && w16 && boxz <= 256 && pair_smem(b32, 4, nsl) <= (size_t)kSmemBudget &&
         pair_smem(b16, 2, nsl) <= (size_t)kSmemBudget) {

@@ -895,13 +895,17 @@ __device__ __forceinline__ void half_samples(const V* __restrict__ s, int kind, 
 }
 
 // CTAs per SM the register budget is sized for: four 128-thread CTAs (124
-// registers, no spills), as many as the fp32 boxes of 16x32 tiles leave room for.
+// registers, no spills), as many as the fp32 boxes of 16x32 tiles leave room
+// for; the half-size 16-bit boxes leave room for five (96 registers).
+#ifndef CBCT_QUAD_MINB16
+#define CBCT_QUAD_MINB16 5
+#endif
 template <class V>
 constexpr int quad_min_blocks() {
 #ifdef CBCT_QUAD_MINB
   return CBCT_QUAD_MINB;
 #else
-  return kQuadThreads >= 256 ? 2 : kQuadThreads >= 128 ? 4 : 6;
+  return kQuadThreads >= 256 ? 2 : kQuadThreads >= 128 ? (sizeof(V) == 4 ? 4 : CBCT_QUAD_MINB16) : 6;
 #endif
 }
 

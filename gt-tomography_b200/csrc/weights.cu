@@ -133,6 +133,159 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(
   }
 }
 
+// ------------------------------------------------------------ register FFT filter
+// The same convolution for L = 32 TL (TL = 16 or 32 lanes per transform, so
+// detectors up to 512 wide) as a four-step FFT held in registers: with
+// n = TL n1 + n2 and k = k1 + 32 k2, each lane (n2) takes a 32-point DFT over
+// n1, multiplies by W_L^(n2 k1), the transform is transposed through shared
+// memory, and each lane takes TL-point DFTs over n2 for its k1 (one for TL =
+// 32, two for TL = 16); the inverse runs the same steps backwards.  One warp
+// filters one pair of rows (TL = 32) or two pairs (TL = 16), with one
+// shared-memory transpose per direction instead of log2(L) barrier-separated
+// radix-2 passes.
+struct Tw32 {
+  float2 w[16];  // exp(-2 pi i m / 32), m = 0..15
+};
+
+constexpr int kRegFftThreads = 128;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+constexpr int brev_bits(int i, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+
+// In-register N-point DFT (N = 16 or 32) of v[off .. off+N), natural order in
+// and out; INV takes exp(+2 pi i / N).  Radix-2, decimation in time, all
+// indices compile-time.
+template <int N, bool INV, int OFF, int NV>
+__device__ __forceinline__ void fft_reg(float2 (&v)[NV], const Tw32& tw) {
+  constexpr int bits = N == 16 ? 4 : 5;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = brev_bits(i, bits);
+    if (j > i) {
+      const float2 t = v[OFF + i];
+      v[OFF + i] = v[OFF + j];
+      v[OFF + j] = t;
+    }
+  }
+#pragma unroll
+  for (int len = 2; len <= N; len <<= 1) {
+#pragma unroll
+    for (int i = 0; i < N; i += len) {
+#pragma unroll
+      for (int k = 0; k < len / 2; ++k) {
+        float2 w = tw.w[k * (32 / len)];
+        if (INV) w.y = -w.y;
+        const float2 a = v[OFF + i + k];
+        const float2 b = cmul(v[OFF + i + k + len / 2], w);
+        v[OFF + i + k] = make_float2(a.x + b.x, a.y + b.y);
+        v[OFF + i + k + len / 2] = make_float2(a.x - b.x, a.y - b.y);
+      }
+    }
+  }
+}
+
+#ifndef CBCT_FDK_MINB
+#define CBCT_FDK_MINB 4
+#endif
+
+template <class T, int TL>
+__global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_kernel(
+    const T* in, float* out, int W, int H, long rows, const float* __restrict__ spec,
+    const float2* __restrict__ twL, const __grid_constant__ Tw32 tw, const float* __restrict__ pre,
+    const float* __restrict__ parker, const float* __restrict__ post) {
+  constexpr int G = 32 / TL;          // transforms per warp
+  constexpr int S = TL + 1;           // padded row of the transpose buffer
+  extern __shared__ float2 xs[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane / TL, j = lane % TL;
+  float2* buf = xs + (size_t)(warp * G + g) * 32 * S;
+  const long npairs = (rows + 1) / 2;
+  const long nwarps = (long)gridDim.x * (kRegFftThreads / 32);
+  for (long base = ((long)blockIdx.x * (kRegFftThreads / 32) + warp) * G; base < npairs; base += nwarps * G) {
+    const long pr = base + g;
+    const bool valid = pr < npairs;
+    const long ra = 2 * pr, rb = 2 * pr + 1;
+    const bool hasb = valid && rb < rows;
+    const int pa = int(ra / H), va = int(ra % H);
+    const int pb = int(rb / H), vb = int(rb % H);
+    float2 v[32];
+    // Load x[TL n1 + j] (row a real, row b imaginary) with the pre-weights.
+#pragma unroll
+    for (int n1 = 0; n1 < 32; ++n1) {
+      const int n = TL * n1 + j;
+      float xa = 0.f, xb = 0.f;
+      if (valid && n < W) {
+        xa = sm_f(in[ra * W + n]);
+        if (pre) xa *= pre[(size_t)va * W + n];
+        if (parker) xa *= parker[(size_t)pa * W + n];
+        if (hasb) {
+          xb = sm_f(in[rb * W + n]);
+          if (pre) xb *= pre[(size_t)vb * W + n];
+          if (parker) xb *= parker[(size_t)pb * W + n];
+        }
+      }
+      v[n1] = make_float2(xa, xb);
+    }
+    fft_reg<32, false, 0>(v, tw);                       // v[k1]
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul(v[k1], twL[k1 * TL + j]);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) buf[k1 * S + j] = v[k1];
+    __syncwarp();
+    // Lane j now takes k1 = j + c TL, c < G: TL-point DFTs over n2.
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int n2 = 0; n2 < TL; ++n2) v[c * TL + n2] = buf[(j + c * TL) * S + n2];
+    fft_reg<TL, false, 0>(v, tw);
+    if (G > 1) fft_reg<TL, false, (G > 1 ? TL : 0)>(v, tw);
+    // Spectrum (real, with the 1/L scale): X[k1 + 32 k2] at v[c TL + k2].
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int k2 = 0; k2 < TL; ++k2) {
+        const float h = spec[(j + c * TL) + 32 * k2];
+        v[c * TL + k2] = make_float2(v[c * TL + k2].x * h, v[c * TL + k2].y * h);
+      }
+    fft_reg<TL, true, 0>(v, tw);
+    if (G > 1) fft_reg<TL, true, (G > 1 ? TL : 0)>(v, tw);
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int n2 = 0; n2 < TL; ++n2) buf[(j + c * TL) * S + n2] = v[c * TL + n2];
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) {
+      const float2 w = twL[k1 * TL + j];
+      v[k1] = cmul(buf[k1 * S + j], make_float2(w.x, -w.y));
+    }
+    fft_reg<32, true, 0>(v, tw);                        // y[TL n1 + j] at v[n1]
+#pragma unroll
+    for (int n1 = 0; n1 < 32; ++n1) {
+      const int n = TL * n1 + j;
+      if (valid && n < W) {
+        float ya = v[n1].x;
+        if (post) ya *= post[(size_t)pa * W + n];
+        out[ra * W + n] = ya;
+        if (hasb) {
+          float yb = v[n1].y;
+          if (post) yb *= post[(size_t)pb * W + n];
+          out[rb * W + n] = yb;
+        }
+      }
+    }
+  }
+}
+
 // FP64 spectrum of the row filter on an L-point grid, scaled by 1/L.
 std::vector<float> filter_spectrum(const float* H, int W, int L) {
   std::vector<double> h(W);
@@ -154,6 +307,7 @@ std::vector<float> filter_spectrum(const float* H, int W, int L) {
 struct FdkTables {
   float* spec = nullptr;
   float2* tw = nullptr;
+  float2* twL = nullptr;    // register FFT: W_L^(n2 k1) at [k1 * TL + n2]
   float* cosw = nullptr;
   float* parker = nullptr;  // per view of the plan
   float* post = nullptr;    // per view of the plan
@@ -167,6 +321,7 @@ struct FdkState {
   FdkTables t;
   std::vector<float> filter;
   int L = 0, logL = 0;
+  Tw32 tw32{};
 };
 
 void fdk_state_free(cbct_plan* p) {
@@ -174,6 +329,7 @@ void fdk_state_free(cbct_plan* p) {
   if (!f) return;
   plan_dealloc(p, f->t.spec);
   plan_dealloc(p, f->t.tw);
+  plan_dealloc(p, f->t.twL);
   plan_dealloc(p, f->t.cosw);
   plan_dealloc(p, f->t.parker);
   plan_dealloc(p, f->t.post);
@@ -198,6 +354,19 @@ static FdkState* fdk_state(cbct_plan* p, const float* filter) {
       tw[k] = make_float2(float(std::cos(2 * pi * k / L)), float(-std::sin(2 * pi * k / L)));
     f->t.tw = plan_alloc_n<float2>(p, tw.size());
     plan_upload(p, f->t.tw, tw.data(), sizeof(float2) * tw.size());
+    for (int m = 0; m < 16; ++m)
+      f->tw32.w[m] = make_float2(float(std::cos(2 * pi * m / 32)), float(-std::sin(2 * pi * m / 32)));
+    if (L == 512 || L == 1024) {
+      const int TL = L / 32;
+      std::vector<float2> twl((size_t)32 * TL);
+      for (int k1 = 0; k1 < 32; ++k1)
+        for (int n2 = 0; n2 < TL; ++n2) {
+          const long e = (long)k1 * n2 % L;
+          twl[(size_t)k1 * TL + n2] = make_float2(float(std::cos(2 * pi * e / L)), float(-std::sin(2 * pi * e / L)));
+        }
+      f->t.twL = plan_alloc_n<float2>(p, twl.size());
+      plan_upload(p, f->t.twL, twl.data(), sizeof(float2) * twl.size());
+    }
     f->t.spec = plan_alloc_n<float>(p, L);
     // Cosine weights (hoCuConebeamProjectionOperator.cpp:84-97): double, stored float.
     std::vector<float> cw((size_t)W * H);
@@ -267,10 +436,28 @@ void offset_weight_launch(cbct_plan* p, int s, const float* in, float* out, int 
 
 void fdk_prepare(cbct_plan* p, const float* filter) { fdk_state(p, filter); }
 
+template <class T, int TL>
+static void fdk_filter_reg(const void* in, float* out, int W, int H, long rows, const FdkState* f, const float* pre,
+                           const float* pk, const float* post, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * (size_t)(kRegFftThreads / 32) * 32 * 32 * (TL + 1) / TL;
+  auto k = fdk_filter_reg_kernel<T, TL>;
+  ensure_smem_attr((const void*)k, smem);
+  const long npairs = (rows + 1) / 2;
+  const long per_block = (kRegFftThreads / 32) * (32 / TL);
+  const int blocks = (int)std::min<long>((npairs + per_block - 1) / per_block, 148L * 16);
+  k<<<blocks, kRegFftThreads, smem, st>>>(static_cast<const T*>(in), out, W, H, rows, f->t.spec, f->t.twL, f->tw32,
+                                          pre, pk, post);
+  check_launch("fdk_filter_reg_kernel");
+}
+
 template <class T>
 static void fdk_filter_typed(const void* in, float* out, int W, int H, long rows, const FdkState* f,
                              const float* pre, const float* pk, const float* post, cudaStream_t st) {
   const int L = f->L;
+#ifndef CBCT_FDK_RADIX2_ONLY
+  if (L == 1024) return fdk_filter_reg<T, 32>(in, out, W, H, rows, f, pre, pk, post, st);
+  if (L == 512) return fdk_filter_reg<T, 16>(in, out, W, H, rows, f, pre, pk, post, st);
+#endif
   const size_t smem = sizeof(float2) * (L + L / 2) + sizeof(float) * L;
   if (smem > 200 * 1024) throw Error(CBCT_ERR_UNSUPPORTED, "detector too wide for the FDK filter");
   ensure_smem_attr((const void*)fdk_filter_kernel<T>, smem);

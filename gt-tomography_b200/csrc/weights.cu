@@ -202,10 +202,18 @@ __global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_
     const float* __restrict__ parker, const float* __restrict__ post) {
   constexpr int G = 32 / TL;          // transforms per warp
   constexpr int S = TL + 1;           // padded row of the transpose buffer
+  constexpr int L = 32 * TL;
   extern __shared__ float2 xs[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane / TL, j = lane % TL;
   float2* buf = xs + (size_t)(warp * G + g) * 32 * S;
+  // The CTA's copies of the inter-pass twiddles and the spectrum, after the
+  // transpose buffers.
+  float2* stw = xs + (size_t)(kRegFftThreads / 32) * G * 32 * S;
+  float* sspec = reinterpret_cast<float*>(stw + 32 * TL);
+  for (int i = threadIdx.x; i < 32 * TL; i += kRegFftThreads) stw[i] = twL[i];
+  for (int i = threadIdx.x; i < L; i += kRegFftThreads) sspec[i] = spec[i];
+  __syncthreads();
   const long npairs = (rows + 1) / 2;
   const long nwarps = (long)gridDim.x * (kRegFftThreads / 32);
   for (long base = ((long)blockIdx.x * (kRegFftThreads / 32) + warp) * G; base < npairs; base += nwarps * G) {
@@ -235,7 +243,7 @@ __global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_
     }
     fft_reg<32, false, 0>(v, tw);                       // v[k1]
 #pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul(v[k1], twL[k1 * TL + j]);
+    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul(v[k1], stw[k1 * TL + j]);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 32; ++k1) buf[k1 * S + j] = v[k1];
@@ -252,7 +260,7 @@ __global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_
     for (int c = 0; c < G; ++c)
 #pragma unroll
       for (int k2 = 0; k2 < TL; ++k2) {
-        const float h = spec[(j + c * TL) + 32 * k2];
+        const float h = sspec[(j + c * TL) + 32 * k2];
         v[c * TL + k2] = make_float2(v[c * TL + k2].x * h, v[c * TL + k2].y * h);
       }
     fft_reg<TL, true, 0>(v, tw);
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 32; ++k1) {
-      const float2 w = twL[k1 * TL + j];
+      const float2 w = stw[k1 * TL + j];
       v[k1] = cmul(buf[k1 * S + j], make_float2(w.x, -w.y));
     }
     fft_reg<32, true, 0>(v, tw);                        // y[TL n1 + j] at v[n1]
@@ -439,7 +447,10 @@ void fdk_prepare(cbct_plan* p, const float* filter) { fdk_state(p, filter); }
 template <class T, int TL>
 static void fdk_filter_reg(const void* in, float* out, int W, int H, long rows, const FdkState* f, const float* pre,
                            const float* pk, const float* post, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (size_t)(kRegFftThreads / 32) * 32 * 32 * (TL + 1) / TL;
+  // transpose buffers (32 x (TL + 1) per transform, 32 / TL transforms per
+  // warp), twiddles (32 TL) and spectrum (32 TL floats)
+  const size_t smem = sizeof(float2) * ((size_t)(kRegFftThreads / 32) * 32 * 32 * (TL + 1) / TL + 32 * TL) +
+                      sizeof(float) * 32 * TL;
   auto k = fdk_filter_reg_kernel<T, TL>;
   ensure_smem_attr((const void*)k, smem);
   const long npairs = (rows + 1) / 2;

@@ -6,16 +6,23 @@
 // trilinear interpolation with border 0, result scaled by the sample spacing.
 // Interpolation here is FP32 in software (not 9-bit texture weights).
 //
-// Two variants:
-//  * fwd_slab_kernel (default): a CTA marches a 16x16 tile of rays of one view
-//    through the volume in slabs of kTS voxels along the view's dominant
-//    in-plane axis.  Each slab's footprint (the box around the tile's ray
-//    pyramid) is staged into shared memory by a 3-D TMA load; out-of-volume
-//    texels arrive as zeros (the border rule for free).  Views whose rays run
-//    mostly along x read an x/y-transposed copy of the volume, so every slab is
-//    a range of memory rows and the box is never padded along its slab axis.
-//    Samples are taken in ray order, so each ray's sum has the reference's
-//    summation order.  Pairs of lerps run as packed FP32 (FFMA2).
+// Variants (all but the gather kernel give bitwise equal results):
+//  * fwd_slab_kernel: a CTA marches a 16x16 tile of rays of one view through
+//    the volume in slabs of kTS voxels along the view's dominant in-plane
+//    axis.  Each slab's footprint (the box around the tile's ray pyramid) is
+//    staged into shared memory by a 3-D TMA load; out-of-volume texels arrive
+//    as zeros (the border rule for free).  Views whose rays run mostly along x
+//    read an x/y-transposed copy of the volume, so every slab is a range of
+//    memory rows and the box is never padded along its slab axis.  Samples are
+//    taken in ray order, so each ray's sum has the reference's summation
+//    order.  Pairs of lerps run as packed FP32 (FFMA2).
+//  * fwd_pair_kernel / fwd_quad_kernel: the same slabs, but one thread marches
+//    two or four vertically adjacent rays of a detector column that share
+//    their in-plane sample positions, interpolating them in e and d once.  A
+//    plan takes the quad kernel where adjacent rows stay under 0.66 z texel
+//    apart, the pair kernel under 0.99, else the slab kernel.
+//  * fwd_fan_kernel (opt-in): the in-plane sharing across a whole column,
+//    through shared-memory lines.
 //  * fwd_gather_kernel: the same arithmetic with bounds-checked global loads,
 //    used when the geometry does not fit the slab boxes or the volume pitch is
 //    not TMA-aligned.

@@ -156,7 +156,10 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__
 // image of a convex block) is staged into shared memory by a 3-D TMA load
 // whose out-of-detector texels arrive as zeros, so the bilinear taps need no
 // bounds checks.  Views are pipelined over two stages.
-constexpr int kZT = 16;
+#ifndef CBCT_BP_ZRUN
+#define CBCT_BP_ZRUN 16
+#endif
+constexpr int kZT = CBCT_BP_ZRUN;
 constexpr int kTX = 16, kTY = 8;     // columns per CTA of the TMA back-projector
 constexpr uint32_t kBpWaitLimit = 1u << 22;
 

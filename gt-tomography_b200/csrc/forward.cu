@@ -462,6 +462,11 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
 #define CBCT_PAIR_STAGES 1
 #endif
 constexpr int kPairStages = CBCT_PAIR_STAGES;
+// Rows of a row-pair box (the slab's kTS + 1 rows, padded to kBoxY by default).
+#ifndef CBCT_PAIR_BOXY
+#define CBCT_PAIR_BOXY 10
+#endif
+constexpr int kPairBoxY = CBCT_PAIR_BOXY;
 
 struct PairShared {
   uint64_t bars[kPairStages];
@@ -559,7 +564,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   __shared__ PairShared sh;
   unsigned char* smem_raw =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
-  constexpr int BXY = BX * kBoxY;
+  constexpr int BXY = BX * kPairBoxY;
   const ViewParams vp = views[blockIdx.z];
   const int dom = vp.dom;
   const CUtensorMap* map = dom ? &map_v : &map_t;
@@ -631,7 +636,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     nslab = 0;
   }
   // Per-slab footprints (e min, e max, z min, z max) after the boxes.
-  const uint32_t box_bytes = uint32_t(BX * kBoxY * BZ * sizeof(V));
+  const uint32_t box_bytes = uint32_t(BX * kPairBoxY * BZ * sizeof(V));
   const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
   int* const emin = reinterpret_cast<int*>(smem_raw + kPairStages * stage_stride);
   int* const emax = emin + nsl_max;
@@ -708,29 +713,30 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
     const V* s = reinterpret_cast<const V*>(smem_raw + slot * stage_stride);
     const float lo = float(od), hi = lo + float(kTS);
     const float cmo = kRoundC - float(oe + od * BX + oz * BXY);
+    constexpr int PY = kPairBoxY;
     if (paired) {
       if (vp.dsgn > 0)
-        pair_samples<V, BX, 1, CHECK>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi, cmo,
-                                      maxidx, maxidx3, acca, accb, bad);
+        pair_samples<V, BX, 1, CHECK, PY>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi,
+                                          cmo, maxidx, maxidx3, acca, accb, bad);
       else
-        pair_samples<V, BX, -1, CHECK>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi, cmo,
-                                       maxidx, maxidx3, acca, accb, bad);
+        pair_samples<V, BX, -1, CHECK, PY>(s, kfa, Nf, ce0a, cd0a, dcea, dcda, idcda, zl0, dzl, zu0, dzu, lo, hi,
+                                           cmo, maxidx, maxidx3, acca, accb, bad);
     } else {
       if (hit_a) {
         if (vp.dsgn > 0)
-          slab_samples<V, BX, 1, CHECK>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
-                                        maxidx, acca, bad);
+          slab_samples<V, BX, 1, CHECK, PY>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
+                                            maxidx, acca, bad);
         else
-          slab_samples<V, BX, -1, CHECK>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
-                                         maxidx, acca, bad);
+          slab_samples<V, BX, -1, CHECK, PY>(s, kfa, Nf, ce0a, cd0a, ra.c0z, dcea, dcda, idcda, ra.dcz, lo, hi, cmo,
+                                             maxidx, acca, bad);
       }
       if (hit_b) {
         if (vp.dsgn > 0)
-          slab_samples<V, BX, 1, CHECK>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
-                                        maxidx, accb, bad);
+          slab_samples<V, BX, 1, CHECK, PY>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
+                                            maxidx, accb, bad);
         else
-          slab_samples<V, BX, -1, CHECK>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
-                                         maxidx, accb, bad);
+          slab_samples<V, BX, -1, CHECK, PY>(s, kfb, Nf, ce0b, cd0b, rb.c0z, dceb, dcdb, idcdb, rb.dcz, lo, hi, cmo,
+                                             maxidx, accb, bad);
       }
     }
     __syncthreads();
@@ -886,19 +892,21 @@ __device__ __forceinline__ void half_samples(const V* __restrict__ s, int kind, 
   if (kind != 0) {
     const bool al = kind > 0;
     float accl = al ? acca : accb, accu = al ? accb : acca;
-    pair_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.dce, fa.dcd, fa.idcd, al ? fa.c0z : fb.c0z,
-                                    al ? fa.dcz : fb.dcz, al ? fb.c0z : fa.c0z, al ? fb.dcz : fa.dcz, lo, hi, cmo,
-                                    maxidx, maxidx3, accl, accu, bad);
+    constexpr int QY = kQuadBoxY;
+    pair_samples<V, BX, SGN, CHECK, QY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.dce, fa.dcd, fa.idcd, al ? fa.c0z : fb.c0z,
+                                        al ? fa.dcz : fb.dcz, al ? fb.c0z : fa.c0z, al ? fb.dcz : fa.dcz, lo, hi,
+                                        cmo, maxidx, maxidx3, accl, accu, bad);
     acca = al ? accl : accu;
     accb = al ? accu : accl;
     return;
   }
+  constexpr int QY = kQuadBoxY;
   if (hit_a)
-    slab_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.c0z, fa.dce, fa.dcd, fa.idcd, fa.dcz, lo, hi,
-                                    cmo, maxidx, acca, bad);
+    slab_samples<V, BX, SGN, CHECK, QY>(s, kfa, Nf, fa.ce0, fa.cd0, fa.c0z, fa.dce, fa.dcd, fa.idcd, fa.dcz, lo, hi,
+                                        cmo, maxidx, acca, bad);
   if (hit_b)
-    slab_samples<V, BX, SGN, CHECK, kQuadBoxY>(s, kfb, Nf, fb.ce0, fb.cd0, fb.c0z, fb.dce, fb.dcd, fb.idcd, fb.dcz, lo, hi,
-                                    cmo, maxidx, accb, bad);
+    slab_samples<V, BX, SGN, CHECK, QY>(s, kfb, Nf, fb.ce0, fb.cd0, fb.c0z, fb.dce, fb.dcd, fb.idcd, fb.dcz, lo, hi,
+                                        cmo, maxidx, accb, bad);
 }
 
 // CTAs per SM the register budget is sized for: four 128-thread CTAs (124
@@ -1128,8 +1136,10 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
   for (int i = 0; i < 4; ++i) {
     float val = 0.f;
     int k0, k1;
-    if (hit[i]) val = sum[i] * r[i].delta;
-    else if (act[i] && grown_range(vp, gc, u, vq + i, r[i], k0, k1)) val = march_global(vol, gc, r[i], k0, k1) * r[i].delta;
+    if (hit[i])
+      val = sum[i] * r[i].delta;
+    else if (act[i] && grown_range(vp, gc, u, vq + i, r[i], k0, k1))
+      val = march_global(vol, gc, r[i], k0, k1) * r[i].delta;
     if (act[i]) sq += fwd_store(o, gc, vp, p, u, vq + i, val);
   }
   fwd_block_partial(o, sq, sh.red, tid);
@@ -1834,7 +1844,7 @@ void forward_choose_variant(cbct_plan* p) {
       slab_extents(p, kPU, kPV, e, z)) {
     const int w32 = width(kBoxWidths, e, 3), w16 = width(kBoxWidths, e, 7);
     const int boxz = std::max(z, 3);
-    const SlabBox b32{w32, kBoxY, boxz, 1}, b16{w16, kBoxY, boxz, 1};
+    const SlabBox b32{w32, kPairBoxY, boxz, 1}, b16{w16, kPairBoxY, boxz, 1};
     const int nsl = slabs_max(p->g);
     if (w32 && w16 && boxz <= 256 && pair_smem(b32, 4, nsl) <= (size_t)kSmemBudget &&
         pair_smem(b16, 2, nsl) <= (size_t)kSmemBudget) {

@@ -205,14 +205,28 @@ def peaks():
 
 
 def traffic_for(kernel: str, workload: str, variant: str | None = None):
-    """DRAM bytes per launch of `kernel` from one ncu capture (profiles/traffic.json),
-    per forward variant where the file keeps several."""
+    """A per-launch ncu counter of `kernel` (DRAM bytes, or warp instructions for
+    the `_warp_instr` entries) from one capture (profiles/traffic.json), per
+    forward variant where the file keeps several."""
     try:
         d = json.load(open(TRAFFIC_PATH))
         t = d.get(workload, {}).get(kernel)
         return t.get(variant) if isinstance(t, dict) else t
     except Exception:
         return None
+
+
+def issue_roofline(warp_instr, samples, seconds, sm_mhz, n_sm=148, issue_per_clk=4):
+    """The forward projector's own ceiling: warp instructions per launch (ncu)
+    over the SMs' issue slots (4 per SM per clock) at the sampled SM clock."""
+    if not warp_instr or not sm_mhz:
+        return None
+    peak = n_sm * issue_per_clk * sm_mhz * 1e6            # warp instructions per second
+    ceiling = samples / (warp_instr / peak)               # samples per second at 100 % issue
+    achieved = samples / seconds
+    return {"warp_instr_per_launch": warp_instr, "ceiling_gsamples_per_s": round(ceiling / 1e9, 1),
+            "achieved_gsamples_per_s": round(achieved / 1e9, 1), "frac": round(achieved / ceiling, 3),
+            "source": "ncu smsp__inst_executed.sum of one launch (profiles/), 148 SMs x 4 issue slots"}
 
 
 def flush_l2(buf):
@@ -429,6 +443,8 @@ def ours(args, wl: Workload):
                      "frac": round(achieved / hbm, 5), "traffic": traffic_for("forward_residual", wl.name, variant),
                      "launch_ms": round(t_fwd * 1e3, 4), "alg_bytes_per_launch": alg_bytes,
                      "gsamples_per_s": round(samples_s / 1e9, 2),
+                     "issue": issue_roofline(traffic_for("forward_residual_warp_instr", wl.name, variant),
+                                             rays0 * wl.Nsamp, t_fwd, clk.get("sm_mhz") if clk else None),
                      "note": "gather/issue-bound kernel: HBM fraction of compulsory bytes is small by design"},
         "gpu_launches": wl.launches_per_step() * args.steps,
         "forward_variant": variant,

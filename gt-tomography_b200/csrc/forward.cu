@@ -807,7 +807,7 @@ __device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, fl
   if (CHECK) {
     const float smax = fmaxf(s1, fmaxf(s2, s3)), smin = fminf(s1, fminf(s2, s3));
     bad |= ((unsigned)idx0 > maxidx) | (smax >= 1.f && (unsigned)idx0 + 2u * BXY > maxidx) | (smax > 2.f) |
-           (smin < 0.f);
+           (smin < 0.f) | (s1 > 1.f);
   }
   // planes fz, fz + 1 from q; fz + 2, fz + 3 from q2 (in the box whenever a ray
   // needs them; clamped otherwise)
@@ -828,7 +828,10 @@ __device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, fl
     const float hi = sk < 0.5f ? d01.y : (sk < 1.5f ? d23.x : d23.y);
     return fmaf(cz - fz, hi - lo, lo);
   };
-  return make_float4(fmaf(c0z - f0, d01.y - d01.x, d01.x), ray(s1, c1z, f1), ray(s2, c2z, f2), ray(s3, c3z, f3));
+  // the second-lowest ray is under one texel above the lowest: planes fz, fz + 1 or fz + 1, fz + 2
+  const float lo1 = s1 < 0.5f ? d01.x : d01.y, hi1 = s1 < 0.5f ? d01.y : d23.x;
+  return make_float4(fmaf(c0z - f0, d01.y - d01.x, d01.x), fmaf(c1z - f1, hi1 - lo1, lo1), ray(s2, c2z, f2),
+                     ray(s3, c3z, f3));
 }
 
 // The quad's samples inside one slab, each ray's values added in ray order.
@@ -955,7 +958,8 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
 #pragma unroll
   for (int i = 0; i < 4; ++i) f[i] = ray_frame(r[i], dom);
   // Quad test: one clip; sorted by z (rows run one way), every ray within
-  // [0.002, 1.998] texels above the lowest at both ends.
+  // [0.002, 1.998] texels above the lowest at both ends, the second-lowest
+  // within [0.002, 0.998].
   bool quad = hit[0] && hit[1] && hit[2] && hit[3];
 #pragma unroll
   for (int i = 1; i < 4; ++i) quad = quad && r[i].a1 == r[0].a1 && r[i].a2 == r[0].a2;
@@ -967,7 +971,8 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
     for (int i = 0; i < 4; ++i) {
       if (i == lo_i) continue;
       const float d0 = r[i].c0z - zs, d1 = fmaf(Nf - 1.f, r[i].dcz, r[i].c0z) - ze;
-      quad = quad && d0 >= 2e-3f && d0 <= 1.998f && d1 >= 2e-3f && d1 <= 1.998f;
+      const float dmax = (up ? i == 1 : i == 2) ? 0.998f : 1.998f;
+      quad = quad && d0 >= 2e-3f && d0 <= dmax && d1 >= 2e-3f && d1 <= dmax;
     }
   }
   // Sorted z parameters of the quad (lowest first).

@@ -774,8 +774,8 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
 // ------------------------------------------------------------------ row quads
 // The row-pair argument for four adjacent rows of a column: when all four rays
 // leave through the side faces (one clip) and, sorted by z, each lies less
-// than two texels above the lowest at both ends of the ray, their planes are
-// among the lowest ray's fz .. fz + 3.  One thread marches the quad: one e/d
+// than two texels above the lowest at both ends of the ray (the second-lowest
+// less than one), their planes are among the lowest ray's fz .. fz + 3.  One thread marches the quad: one e/d
 // position, four planes interpolated in e and d (16 shared loads for four
 // samples), each ray's own z lerp on its two planes.  Values are the slab
 // kernel's for every ray, so results are bitwise equal.  Quads that do not

@@ -402,6 +402,10 @@ def ours(args, wl: Workload):
         e1.synchronize()
         e2e_times.append(e0.elapsed_time(e1))
     barrier(world)
+    # Device-side status of everything above: raises CBCT_ERR_TIMEOUT or
+    # CBCT_ERR_DEVICE_CHECK if any kernel gave up a bounded wait or overflowed
+    # a shared-memory box (the solve reports it on return as well).
+    plan.check()
     ms_e2e = max_over_ranks(sum(e2e_times) / len(e2e_times), world)
     gups_e2e = whole_job_rate(fs + bv, world, ms_e2e)
 
@@ -448,6 +452,7 @@ def ours(args, wl: Workload):
                      "note": "gather/issue-bound kernel: HBM fraction of compulsory bytes is small by design"},
         "gpu_launches": wl.launches_per_step() * args.steps,
         "forward_variant": variant,
+        "device_flags": "clear",
         "clocks": clk,
     }
     if rank == 0 and world == 1 and wl.name == "c2" and not args.no_plain:

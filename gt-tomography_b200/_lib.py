@@ -22,15 +22,19 @@ CBCT_FDK_RAMP = 0x8
 CBCT_OPT_DEBUG_CHECKS = 1
 CBCT_OPT_FORCE_GATHER = 2
 CBCT_OPT_FORWARD_KERNEL = 3
+CBCT_OPT_WAIT_LIMIT = 4
+CBCT_OPT_STATUS_CHECK = 5
+CBCT_ERR_DEVICE_CHECK = 5
+CBCT_ERR_TIMEOUT = 6
 
 # Every symbol the header declares (checked by the CPU tests).
 EXPORTED = [
     "cbct_status_string", "cbct_last_error", "cbct_version", "cbct_subset_partition",
     "cbct_default_frequency_filter", "cbct_cosine_weights", "cbct_is_short_scan",
     "cbct_offset_override", "cbct_plan_create", "cbct_plan_destroy", "cbct_plan_subset",
-    "cbct_plan_forward_variant", "cbct_plan_set_option", "cbct_plan_read_flags", "cbct_forward",
+    "cbct_plan_forward_variant", "cbct_plan_set_option", "cbct_plan_read_flags", "cbct_plan_check", "cbct_forward",
     "cbct_backproject", "cbct_offset_correct", "cbct_fdk_filter", "cbct_fdk",
-    "cbct_forward_residual", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
+    "cbct_forward_residual", "cbct_osmom_precon", "cbct_osmom_step", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
     "cbct_osmom_solve",
     "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
     "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
@@ -40,7 +44,8 @@ EXPORTED = [
     "cbct_server_now", "cbct_server_destroy",
 ]
 # The plain reference-replica path (include/cbct_plain.h), a measurement baseline.
-EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve", "cbct_plain_fdk"]
+EXPORTED_PLAIN = ["cbct_plain_forward", "cbct_plain_backproject", "cbct_plain_osmom_solve", "cbct_plain_fdk",
+                  "cbct_plain_kernel_times"]
 
 
 class CbctGeometry(C.Structure):
@@ -116,12 +121,15 @@ _SIGS = {
     "cbct_plan_forward_variant": (C.c_char_p, [_vp]),
     "cbct_plan_set_option": (C.c_int, [_vp, _i32, _i32]),
     "cbct_plan_read_flags": (C.c_int, [_vp, _vp, _i32]),
+    "cbct_plan_check": (C.c_int, [_vp, _vp]),
     "cbct_forward": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _i32, _vp]),
     "cbct_backproject": (C.c_int, [_vp, _i32, _vp, _vp, _u32, _i32, _i32, _vp]),
     "cbct_offset_correct": (C.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "cbct_fdk_filter": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _u32, _vp]),
     "cbct_fdk": (C.c_int, [_vp, _vp, _vp, _vp, _u32, _vp, _vp]),
     "cbct_forward_residual": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _vp, _f, _i32, _vp, _vp]),
+    "cbct_osmom_precon": (C.c_int, [_vp, _vp, _vp]),
+    "cbct_osmom_step": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _vp, _vp, _vp, _f, _f, _i32, _vp, _vp]),
     "cbct_osmom_update": (C.c_int, [_vp, _vp, _vp, _vp, _sz, _f, _f, _i32, _vp]),
     "cbct_reduce_f64": (C.c_int, [_i32, _vp, _vp, _sz, _vp, _vp]),
     "cbct_reduce_f64_noalloc": (C.c_int, [_i32, _vp, _vp, _sz, _vp, _vp]),
@@ -152,6 +160,7 @@ _SIGS = {
     "cbct_plain_backproject": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _i32, _i32]),
     "cbct_plain_osmom_solve": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp]),
     "cbct_plain_fdk": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _vp, _i32, _i32]),
+    "cbct_plain_kernel_times": (C.c_int, [_gp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _i32, _vp]),
 }
 
 

@@ -186,6 +186,7 @@ static GridConst make_grid(const cbct_geometry& g) {
   c.ku = float(double(g.width) / g.fov_u); c.kv = float(double(g.height) / g.fov_v);
   c.bu = g.width * 0.5f - 0.5f; c.bv = g.height * 0.5f - 0.5f;
   c.invN = 1.f / float(c.N);
+  c.wait_limit = kWaitLimit;
   return c;
 }
 
@@ -279,6 +280,38 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   backproject_choose_variant(p.get());
   backproject_prepare(p.get());
   return p.release();
+}
+
+bool stream_capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    // Querying the legacy stream while another stream captures in global mode
+    // is itself refused: treat that as capturing (no synchronisation allowed).
+    (void)cudaGetLastError();
+    return true;
+  }
+  return cs != cudaStreamCaptureStatusNone;
+}
+
+void plan_check_flags(cbct_plan* p, cudaStream_t st) {
+  int h[4] = {0, 0, 0, 0};
+  CBCT_CUDA(cudaMemcpyAsync(h, p->d_flags, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CBCT_CUDA(cudaStreamSynchronize(st));
+  if (h[0] == 0 && h[1] == 0) return;
+  CBCT_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(h), st));
+  CBCT_CUDA(cudaStreamSynchronize(st));
+  if (h[1] != 0)
+    throw Error(CBCT_ERR_TIMEOUT, std::to_string(h[1]) + " thread block(s) gave up a bounded wait for a TMA stage "
+                                  "(their rays or voxels are incomplete); " + std::to_string(h[0]) +
+                                  " range-check event(s)");
+  throw Error(CBCT_ERR_DEVICE_CHECK, std::to_string(h[0]) + " device range-check event(s): a footprint did not fit "
+                                     "its shared-memory box or an index left its range; results are incomplete");
+}
+
+// The solve and FDK entry points report the device flags on return unless the
+// caller turned that off or is capturing the stream.
+static void check_on_return(cbct_plan* p, cudaStream_t st) {
+  if (p->status_check && !stream_capturing(st)) plan_check_flags(p, st);
 }
 
 static int subset_index(const cbct_plan* p, int s) {
@@ -410,6 +443,12 @@ cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value)
     CBCT_REQUIRE(plan, "plan is NULL");
     if (option == CBCT_OPT_DEBUG_CHECKS) {
       plan->debug_checks = value != 0;
+    } else if (option == CBCT_OPT_WAIT_LIMIT) {
+      CBCT_REQUIRE(value >= 0, "the wait limit must be >= 0 polls");
+      plan->gc.wait_limit = (unsigned)value;
+      graph_cache_free(plan);   // captured graphs hold the kernels' old constants
+    } else if (option == CBCT_OPT_STATUS_CHECK) {
+      plan->status_check = value != 0;
     } else if (option == CBCT_OPT_FORCE_GATHER || option == CBCT_OPT_FORWARD_KERNEL) {
       if (option == CBCT_OPT_FORCE_GATHER) plan->force_gather = value != 0;
       else {
@@ -432,6 +471,13 @@ cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, void* strea
   return guard([&] {
     CBCT_REQUIRE(plan && times_ms_out, "NULL argument");
     plan_autotune(plan, times_ms_out, S(stream));
+  });
+}
+
+cbct_status cbct_plan_check(cbct_plan* plan, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(plan, "plan is NULL");
+    plan_check_flags(plan, S(stream));
   });
 }
 
@@ -616,6 +662,7 @@ cbct_status cbct_fdk(cbct_plan* plan, const float* proj, float* vol, const float
     if (plan) require_one_bin(plan, "cbct_fdk");
     CBCT_REQUIRE(plan && proj && vol, "NULL argument");
     fdk_run(plan, proj, vol, filter, flags, work, S(stream), CBCT_F32);
+    check_on_return(plan, S(stream));
   });
 }
 
@@ -644,6 +691,7 @@ cbct_status cbct_fdk_ex(cbct_plan* plan, cbct_dtype proj_dtype, const void* proj
     require_dtype(proj_dtype);
     CBCT_REQUIRE(proj_dtype == CBCT_F32 || (const void*)work != proj, "a 16-bit input cannot be filtered in place");
     fdk_run(plan, proj, vol, filter, flags, work, S(stream), proj_dtype);
+    check_on_return(plan, S(stream));
   });
 }
 
@@ -683,6 +731,26 @@ cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtype vol_dty
   });
 }
 
+cbct_status cbct_osmom_precon(cbct_plan* plan, float* precon_out, void* stream) {
+  return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_osmom_precon");
+    CBCT_REQUIRE(plan && precon_out, "NULL argument");
+    osmom_precon(plan, precon_out, S(stream));
+  });
+}
+
+cbct_status cbct_osmom_step(cbct_plan* plan, int32_t s, cbct_dtype b_dtype, const void* b_s, float* z, float* xold,
+                            const float* precon, float* r_work, float step, float mom, int32_t nonneg,
+                            double* norm2_out, void* stream) {
+  return guard([&] {
+    if (plan) require_one_bin(plan, "cbct_osmom_step");
+    CBCT_REQUIRE(plan && s >= 0 && s < plan->n_subsets, "subset index out of range (one subset per step)");
+    require_dtype(b_dtype);
+    CBCT_REQUIRE(b_s && z && xold && precon && r_work, "NULL array");
+    osmom_step(plan, s, b_dtype, b_s, z, xold, precon, r_work, step, mom, nonneg, norm2_out, S(stream));
+  });
+}
+
 cbct_status cbct_osmom_update(float* z, float* xold, const float* precon, const float* g, size_t n, float step,
                               float mom, int32_t nonneg, void* stream) {
   return guard([&] {
@@ -695,16 +763,18 @@ cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t
   return guard([&] {
     CBCT_REQUIRE(kind >= 0 && kind <= 2, "kind must be 0, 1 or 2");
     CBCT_REQUIRE(a && out_dev && (kind != 0 || b), "NULL array");
-    // A small per-call partials buffer; reductions are rare outside the solvers.
-    static thread_local double* partials = nullptr;
-    static thread_local int dev = -1;
-    int cur;
-    CBCT_CUDA(cudaGetDevice(&cur));
-    if (!partials || dev != cur) {
-      CBCT_CUDA(cudaMalloc(&partials, sizeof(double) * 148 * 4));
-      dev = cur;
+    // The partial sums take a buffer from the device's stream-ordered pool on
+    // the caller's stream and give it back in stream order: calls on
+    // different streams or threads never share it, and nothing outlives the call.
+    double* partials = nullptr;
+    CBCT_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&partials), sizeof(double) * 148 * 4, S(stream)));
+    try {
+      reduce_launch(kind, a, b, n, partials, 148 * 4, out_dev, S(stream));
+    } catch (...) {
+      cudaFreeAsync(partials, S(stream));
+      throw;
     }
-    reduce_launch(kind, a, b, n, partials, 148 * 4, out_dev, S(stream));
+    CBCT_CUDA(cudaFreeAsync(partials, S(stream)));
   });
 }
 
@@ -741,6 +811,7 @@ cbct_status cbct_osmom_solve(cbct_plan* plan, const void* b, const float* x0, fl
     const cbct_solver_params prm = solver_defaults(params);
     CBCT_REQUIRE(prm.iterations >= 0, "iterations must be >= 0");
     osmom_solve(plan, b, x0, z_out, prm, resid_norm2_out, S(stream));
+    check_on_return(plan, S(stream));
   });
 }
 
@@ -754,6 +825,7 @@ cbct_status cbct_ossart_solve(cbct_plan* plan, const float* b, const float* x0, 
     if (prm.proj_storage != CBCT_F32) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART takes float projections");
     if (prm.tv_weight > 0.f) throw Error(CBCT_ERR_UNSUPPORTED, "OS-SART has no regulariser (osSARTSolver.h)");
     ossart_solve(plan, b, x0, x_out, prm, cost_out, S(stream));
+    check_on_return(plan, S(stream));
   });
 }
 

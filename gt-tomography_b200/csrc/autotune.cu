@@ -98,6 +98,7 @@ void plan_autotune(cbct_plan* p, float* times, cudaStream_t st) {
   plan_dealloc(p, vol);
   plan_dealloc(p, proj);
   graph_cache_free(p);
+  plan_check_flags(p, st);   // a variant that failed on the device must not pass as a timing
 }
 
 }  // namespace cbct

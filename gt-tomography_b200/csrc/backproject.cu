@@ -161,7 +161,6 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__
 #endif
 constexpr int kZT = CBCT_BP_ZRUN;
 constexpr int kTX = 16, kTY = 8;     // columns per CTA of the TMA back-projector
-constexpr uint32_t kBpWaitLimit = 1u << 22;
 
 struct BpView {
   float cs, sn, ox, oy;
@@ -248,7 +247,7 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
   for (int q = 0; q < kZT; ++q) acc[q] = 0.f;
   int done = 0;
   for (int pv = 0; pv < n_views; ++pv) {
-    const bool ok = mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kBpWaitLimit);
+    const bool ok = mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); abort_flag = 1; }
       break;
@@ -297,7 +296,7 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
   }
   if (abort_flag && tid == 0) {
     for (int pv = done; pv < min(done + 2, n_views); ++pv)
-      (void)mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kBpWaitLimit);
+      (void)mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kWaitLimit);
   }
   if (i >= gc.nx || j >= gc.ny) return;
   const size_t base = ((size_t)k0 * gc.ny + j) * gc.nx + i;

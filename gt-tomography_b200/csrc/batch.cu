@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <mutex>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "cbct_internal.h"
@@ -101,6 +102,21 @@ void batch_osmom(const cbct_batch_item* items, int n, int n_streams, cudaStream_
     osmom_solve(items[i].plan, items[i].b, items[i].x0, items[i].z_out, prm, items[i].resid_norm2_out, pool[s]);
   }
   for (int s = 0; s < S; ++s) CBCT_CUDA(cudaStreamSynchronize(pool[s]));
+  // Device-side status of every item (each plan's flag words are read and
+  // cleared); the first failing item's status is returned.
+  std::string first_msg;
+  cbct_status first = CBCT_OK;
+  for (int i = 0; i < n; ++i) {
+    try {
+      plan_check_flags(items[i].plan, pool[0]);
+    } catch (const Error& e) {
+      if (first == CBCT_OK) {
+        first = e.status;
+        first_msg = "batch item " + std::to_string(i) + ": " + e.what();
+      }
+    }
+  }
+  if (first != CBCT_OK) throw Error(first, first_msg);
 }
 
 }  // namespace cbct

@@ -125,7 +125,14 @@ struct GridConst {
   float ku, kv;           // pixels per mm on the detector
   float bu, bv;           // W/2 - 0.5, H/2 - 0.5
   float invN;
+  unsigned wait_limit;    // polls of a kernel's bounded wait for its next TMA stage
 };
+
+// Default poll limit of the bounded mbarrier waits (CBCT_OPT_WAIT_LIMIT).  A
+// CTA whose wait gives up still drains the loads it has in flight with this
+// default limit before it exits, so a shortened limit never leaves a copy
+// writing into shared memory after its CTA is gone.
+constexpr uint32_t kWaitLimit = 1u << 22;
 
 // Box of the TMA slab forward projector, in the view's frame (e, d, z):
 // e = in-plane cross axis (memory x), d = slab axis (memory y), z.
@@ -243,6 +250,7 @@ struct cbct_plan {
 
   int debug_checks = 0;
   int force_gather = 0;
+  int status_check = 1;     // CBCT_OPT_STATUS_CHECK: solve/FDK entry points read the flag words on return
   const unsigned char* d_mask = nullptr;  // voxel mask applied after back-projection (caller-owned)
   const float* d_pweights = nullptr;      // projection weights, all views in subset order (caller-owned)
 
@@ -343,6 +351,13 @@ void mul_launch(float* out, const float* in, const float* w, size_t n, cudaStrea
 
 // plans and set-up rules (abi.cu)
 void validate_geometry(const cbct_geometry* g);
+// Reads the plan's device flag words after the work enqueued on `st` (a
+// stream synchronisation), clears them, and throws CBCT_ERR_TIMEOUT (an
+// expired bounded wait) or CBCT_ERR_DEVICE_CHECK (a range-check violation or
+// a footprint that did not fit its box) when any is set.
+void plan_check_flags(cbct_plan* p, cudaStream_t st);
+// True while `st` is being captured into a CUDA graph.
+bool stream_capturing(cudaStream_t st);
 // forward_buffers = false leaves out the forward projector's transposed-volume
 // buffer (plans that only back-project; their forward calls take the gather path).
 cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float* offsets, int n_views,
@@ -356,6 +371,9 @@ void osmom_solve(cbct_plan* p, const void* b, const float* x0, float* z, const c
                  double* resid, cudaStream_t st);
 void fdk_run(cbct_plan* p, const void* proj, float* vol, const float* filter, uint32_t flags, float* work,
              cudaStream_t st, cbct_dtype proj_dtype);
+void osmom_precon(cbct_plan* p, float* D, cudaStream_t st);
+void osmom_step(cbct_plan* p, int s, cbct_dtype bt, const void* b, float* z, float* xold, const float* D, float* r,
+                float step, float mom, int nonneg, double* norm2, cudaStream_t st);
 
 // host helpers (abi.cu)
 void default_filter(int W, float* out);

@@ -51,7 +51,6 @@ struct FwdOut {
   const float* wproj;    // projection weights of the subset (CBSubsetWeightOperator; nullable)
 };
 
-constexpr uint32_t kWaitLimit = 1u << 22;
 
 // Sample range of a ray restricted to the box grown by half a voxel: samples
 // outside it touch only border texels and add exactly 0.  Returns false when
@@ -392,7 +391,7 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
     const int slot = i % kNStage;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;
@@ -698,7 +697,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
     const int slot = i % kPairStages;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, kWaitLimit);
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;
@@ -1076,7 +1075,7 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
     const int slot = i % kPairStages;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, kWaitLimit);
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kPairStages) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;
@@ -1377,7 +1376,7 @@ __global__ void __launch_bounds__(256, 3) fwd_fan_kernel(const __grid_constant__
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
     const int slot = i % kNStage;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, kWaitLimit);
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;

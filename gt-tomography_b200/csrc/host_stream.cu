@@ -125,6 +125,7 @@ void host_forward(cbct_plan* p, int s0, int ns, const float* vol_host, float* pr
   }
   CBCT_CUDA(cudaStreamSynchronize(pipe.copy));
   CBCT_CUDA(cudaStreamSynchronize(pipe.compute));
+  plan_check_flags(p, pipe.compute);
 }
 
 void host_backproject(cbct_plan* p, int s0, int ns, const float* proj_host, float* vol_host, const int* view_index,
@@ -167,6 +168,7 @@ void host_backproject(cbct_plan* p, int s0, int ns, const float* proj_host, floa
   CBCT_CUDA(cudaMemcpyAsync(vol_host, vol, nv * sizeof(float), cudaMemcpyDeviceToHost, pipe.compute));
   CBCT_CUDA(cudaStreamSynchronize(pipe.compute));
   CBCT_CUDA(cudaStreamSynchronize(pipe.copy));
+  plan_check_flags(p, pipe.compute);
 }
 
 }  // namespace cbct

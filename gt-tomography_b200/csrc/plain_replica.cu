@@ -311,6 +311,89 @@ void backproject(const cbct_geometry& g, const float* angles, const float* offse
   if (copy) cudaFree(copy);
 }
 
+// Device-only timing of the two reference kernels on already-built textures:
+// the cudaArray copies, uploads and texture objects are made once, outside the
+// timed launches, so the times are the kernels' own (what the reference's
+// structure costs in the kernels alone, apart from its per-call host work).
+void kernel_times(const cbct_geometry& g, const float* angles, const float* offsets, int P, const float* vol,
+                  const float* proj, float* proj_out, float* vol_out, int reps, float* ms) {
+  Uploads up(angles, offsets, P);
+  cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+  cudaArray_t varr = nullptr, parr = nullptr;
+  cudaTextureObject_t vtex = 0, ptex = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto release = [&] {
+    if (vtex) cudaDestroyTextureObject(vtex);
+    if (ptex) cudaDestroyTextureObject(ptex);
+    if (varr) cudaFreeArray(varr);
+    if (parr) cudaFreeArray(parr);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  try {
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    cudaExtent vext = make_cudaExtent(g.nx, g.ny, g.nz);
+    check(cudaMalloc3DArray(&varr, &ch, vext), "cudaMalloc3DArray");
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr((void*)vol, g.nx * sizeof(float), g.nx, g.ny);
+    cp.dstArray = varr;
+    cp.extent = vext;
+    cp.kind = cudaMemcpyDeviceToDevice;
+    check(cudaMemcpy3D(&cp), "cudaMemcpy3D");
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = varr;
+    check(cudaCreateTextureObject(&vtex, &rd, &td, nullptr), "cudaCreateTextureObject");
+    cudaExtent pext = make_cudaExtent(g.width, g.height, P);
+    check(cudaMalloc3DArray(&parr, &ch, pext, cudaArrayLayered), "cudaMalloc3DArray(layered)");
+    cudaMemcpy3DParms cq = {};
+    cq.srcPtr = make_cudaPitchedPtr((void*)proj, g.width * sizeof(float), g.width, g.height);
+    cq.dstArray = parr;
+    cq.extent = pext;
+    cq.kind = cudaMemcpyDeviceToDevice;
+    check(cudaMemcpy3D(&cq), "cudaMemcpy3D");
+    rd.res.array.array = parr;
+    check(cudaCreateTextureObject(&ptex, &rd, &td, nullptr), "cudaCreateTextureObject");
+    check(cudaEventCreate(&e0), "cudaEventCreate");
+    check(cudaEventCreate(&e1), "cudaEventCreate");
+    dim3 fb, fg, bb, bg;
+    setup_grid((size_t)g.width * g.height * P, &fb, &fg);
+    setup_grid((size_t)g.nx * g.ny * g.nz, &bb, &bg);
+    const int N = (int)(g.samples_per_pixel * float(g.nx));
+    const float3 L = make_float3(g.lx, g.ly, g.lz);
+    const float2 ps = make_float2(g.fov_u, g.fov_v);
+    auto fwd = [&] {
+      fwd_kernel<<<fg, fb>>>(proj_out, up.angles, up.offsets, L, g.width, g.height, ps, P, g.SDD, g.SAD, N, false, vtex);
+    };
+    auto bp = [&] {
+      bp_kernel<false><<<bg, bb>>>(vol_out, up.angles, up.offsets, g.nx, g.ny, g.nz, L, ps, P, g.SDD, g.SAD, false,
+                                   ptex);
+    };
+    for (int which = 0; which < 2; ++which) {
+      if (which == 0) fwd(); else bp();                  // warm-up launch
+      check(cudaGetLastError(), "plain kernel");
+      check(cudaDeviceSynchronize(), "plain kernel");
+      check(cudaEventRecord(e0, 0), "cudaEventRecord");
+      for (int r = 0; r < reps; ++r) {
+        if (which == 0) fwd(); else bp();
+      }
+      check(cudaEventRecord(e1, 0), "cudaEventRecord");
+      check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float t = 0.f;
+      check(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+      ms[which] = t / float(reps);
+    }
+  } catch (...) {
+    release();
+    throw;
+  }
+  release();
+}
+
 void osmom(const cbct_geometry& g, const float* angles, const float* offsets, int P, const int* sizes, int S,
            const int* offcorr, const float* b, float* z_out, int iters, bool nonneg, double* resid) {
   const size_t nv = (size_t)g.nx * g.ny * g.nz, plane = (size_t)g.width * g.height, np = plane * P;
@@ -556,6 +639,16 @@ cbct_status cbct_plain_osmom_solve(const cbct_geometry* g, const float* angles, 
     if (!g || !angles || !offsets || !sizes || !offcorr || !b || !z_out || S < 1)
       throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
     osmom(*g, angles, offsets, n, sizes, S, offcorr, b, z_out, iterations, nonneg != 0, resid);
+  });
+}
+
+cbct_status cbct_plain_kernel_times(const cbct_geometry* g, const float* angles, const float* offsets, int32_t n,
+                                    const float* vol, const float* proj, float* proj_out, float* vol_out, int32_t reps,
+                                    float* ms_out) {
+  return guard([&] {
+    if (!g || !angles || !offsets || !vol || !proj || !proj_out || !vol_out || !ms_out || n < 1 || reps < 1)
+      throw cbct::Error(CBCT_ERR_INVALID_ARGUMENT, "bad args");
+    kernel_times(*g, angles, offsets, n, vol, proj, proj_out, vol_out, reps, ms_out);
   });
 }
 

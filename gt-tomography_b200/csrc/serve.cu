@@ -210,6 +210,7 @@ void run_request(cbct_server* sv, Request& q, cudaStream_t st) {
   CBCT_CUDA(cudaMemcpyAsync(r.vol_host, vol, vol_bytes(g), cudaMemcpyDeviceToHost, st));
   CBCT_CUDA(cudaStreamSynchronize(st));
   q.peak = p->dev_bytes_peak;
+  plan_check_flags(p, st);   // a kernel that gave up a wait or overflowed a box fails the request
 }
 
 void worker(cbct_server* sv, int slot) {

@@ -132,10 +132,16 @@ void finalize_partials(const double* partials, int n, double* out, cudaStream_t 
 // (different streams, no ordering between them) race on it.
 constexpr int kNoAllocMaxPartials = 1024;
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxPartials];
+// The reduction's grid is capped at kRedBlocks (592) blocks, one partial each,
+// so no input size needs more partials than the array holds; the size check
+// in reduce_noalloc_launch is a guard for a future change of the launch shape.
+static_assert(kRedBlocks <= kNoAllocMaxPartials, "the static scratch must hold one partial per reduction block");
 
 // The array's name is only a host-side stand-in in host code; its device
 // address is looked up once per device, with that device current, by the first
-// call made on that device.
+// call made on that device.  The cached address assumes the device's primary
+// context lives as long as the library (no cudaDeviceReset in between, which
+// would give the array a new address).
 static double* noalloc_partials_address() {
   static std::mutex mu;
   static std::vector<double*> by_device;
@@ -432,6 +438,24 @@ static void run_ossart(cbct_plan* p, const float* b, const float* x0, float* x, 
       forward_launch_ex(p, p->n_subsets, CBCT_F32, x, r, b, nullptr, 1.f, 1, 0, 0, cost + it, st);
     }
   }
+}
+
+void osmom_precon(cbct_plan* p, float* D, cudaStream_t st) {
+  const size_t nv = vol_elems(p), np = proj_elems(p);
+  float* ws = workspace(p, nv + np);
+  float* ones = ws;
+  float* r = ws + nv;
+  fill_launch(ones, nv, 1.f, st);
+  for (int s = 0; s < p->n_subsets; ++s)
+    forward_launch_ex(p, s, CBCT_F32, ones, r + plane_elems(p) * p->first[s], nullptr, nullptr, 1.f, 1,
+                      p->offcorr[s], 0, nullptr, st);
+  backproject_recip_launch(p, p->n_subsets, r, D, st);
+}
+
+void osmom_step(cbct_plan* p, int s, cbct_dtype bt, const void* b, float* z, float* xold, const float* D, float* r,
+                float step, float mom, int nonneg, double* norm2, cudaStream_t st) {
+  forward_launch_ex(p, s, CBCT_F32, z, r, b, nullptr, 1.f, 1, p->offcorr[s], 0, norm2, st, bt);
+  backproject_mom_launch(p, s, r, z, xold, D, step, mom, nonneg, st);
 }
 
 struct GraphCache {

@@ -285,6 +285,12 @@ class Plan:
         L.call("cbct_plan_read_flags", self._h, C.cast(f, C.c_void_p), int(reset))
         return int(f[0]), int(f[1])
 
+    def check(self, stream=None):
+        """cbct_plan_check: raises CbctError (CBCT_ERR_TIMEOUT, CBCT_ERR_DEVICE_CHECK)
+        when a kernel of this plan gave up a bounded wait or recorded a range
+        violation since the last check; clears the flags."""
+        L.call("cbct_plan_check", self._h, _stream(stream))
+
     # -- operators
     def forward(self, vol, out, s=-1, accumulate=False, vol_dtype=L.CBCT_F32, stream=None):
         T = torch()
@@ -380,6 +386,22 @@ class Plan:
         L.call("cbct_osmom_solve", self._h, _ptr(b), _ptr(x0), _ptr(z_out), C.byref(prm), _ptr(resid),
                _stream(stream))
         return z_out
+
+    def osmom_precon(self, out, stream=None):
+        """cbct_osmom_precon: out = 1/max(A^T W A 1, 1e-6) (osMOMSolverD.h:115-120)."""
+        _need_cuda_f32(out, self.vol_shape, "preconditioner")
+        L.call("cbct_osmom_precon", self._h, _ptr(out), _stream(stream))
+        return out
+
+    def osmom_step(self, s, b_s, z, xold, precon, r_work, step, mom, nonneg=False, norm2=None, stream=None):
+        """cbct_osmom_step: one subset step of osMOMSolverD (residual forward
+        projection, then the back-projection with the fused update of z, xold)."""
+        bt = _storage_of(b_s, self.proj_shape(s), "b_s")
+        for t, what in ((z, "z"), (xold, "xold"), (precon, "precon")):
+            _need_cuda_f32(t, self.vol_shape, what)
+        _need_cuda_f32(r_work, self.proj_shape(s), "r_work")
+        L.call("cbct_osmom_step", self._h, int(s), bt, _ptr(b_s), _ptr(z), _ptr(xold), _ptr(precon), _ptr(r_work),
+               float(step), float(mom), int(nonneg), _ptr(norm2), _stream(stream))
 
     def ossart(self, b, x_out, x0=None, iterations=10, beta=1.0, gamma=0.0, nonneg=False, use_graph=False,
                cost=None, stream=None):

@@ -164,12 +164,39 @@ CBCT_API cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, vo
  * interpolation), 5 = the row-quad kernel (four rows per thread).  Slab, fan,
  * row-pair and row-quad results are bitwise equal. */
 #define CBCT_OPT_FORWARD_KERNEL 3
+/* CBCT_OPT_WAIT_LIMIT: polls (>= 0) a TMA-staged projector kernel spends
+ * waiting for its next shared-memory stage before it gives up (default
+ * 4194304).  A CTA that gives up records the event in the plan's flag word,
+ * waits with the default limit for the loads it still has in flight, leaves
+ * its rays or voxels unfinished and exits; the calling entry point (or
+ * cbct_plan_check) then reports CBCT_ERR_TIMEOUT.  0 makes every such wait
+ * give up at once, which is how the failure path is tested. */
+#define CBCT_OPT_WAIT_LIMIT 4
+/* CBCT_OPT_STATUS_CHECK: 1 (default) = cbct_osmom_solve, cbct_ossart_solve,
+ * cbct_fdk and cbct_fdk_ex synchronise their stream on return and report the
+ * plan's flag words as a status (CBCT_ERR_TIMEOUT, CBCT_ERR_DEVICE_CHECK),
+ * except while the stream is being captured into a CUDA graph; 0 = they stay
+ * asynchronous and the caller checks with cbct_plan_check. */
+#define CBCT_OPT_STATUS_CHECK 5
 CBCT_API cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value);
 
 /* Reads (and optionally clears) the plan's device flag words:
- * flags_out[0] = range-check violations, flags_out[1] = expired bounded waits.
+ * flags_out[0] = range-check violations and footprints that did not fit their
+ * shared-memory box, flags_out[1] = expired bounded waits.
  * Synchronises the device. */
 CBCT_API cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t reset);
+
+/* Device-side status of the plan's work (no reference counterpart: the
+ * reference's kernels have no device-side failure path).  Synchronises
+ * `stream`, reads and clears the plan's flag words and returns
+ * CBCT_ERR_TIMEOUT when a kernel's bounded wait expired, CBCT_ERR_DEVICE_CHECK
+ * when a kernel recorded a range violation or a footprint that did not fit its
+ * box (results of the calls since the last check are then not to be trusted),
+ * else CBCT_OK.  The asynchronous operators (cbct_forward, cbct_backproject,
+ * cbct_forward_residual, cbct_fdk_filter ...) leave the check to the caller;
+ * the host-array operators, the batch executor and the serving loop run it
+ * themselves. */
+CBCT_API cbct_status cbct_plan_check(cbct_plan* plan, void* stream);
 
 /* ----------------------------------------------------------------------------
  * Operators
@@ -257,7 +284,10 @@ CBCT_API cbct_status cbct_apply_mask(float* vol, const uint8_t* mask, size_t n, 
 /* Sets (or clears, with NULL) the mask the plan's back-projections apply to
  * their output (cuConebeamProjectionOperator::set_mask and the apply_mask at
  * .cpp:113-114).  The caller keeps the mask alive while the plan uses it.
- * Applies to cbct_backproject without CBCT_BP_FDK_WEIGHT and to the solvers. */
+ * Applies to cbct_backproject without CBCT_BP_FDK_WEIGHT and to the solvers.
+ * An accumulating back-projection is masked as a whole, the caller's earlier
+ * contents included (vol = mask * (vol + A^T p)), as the reference's
+ * apply_mask on the operator's output is. */
 CBCT_API cbct_status cbct_plan_set_mask(cbct_plan* plan, const uint8_t* mask);
 
 /* Projection weights of CBSubsetWeightOperator (xray/CBSubsetWeightOperator.h:11-63):
@@ -281,6 +311,29 @@ CBCT_API cbct_status cbct_forward_residual(cbct_plan* plan, int32_t s, cbct_dtyp
                                   const void* vol, const float* b, float* r, float scale,
                                   int32_t apply_offset, double* norm2_out, void* stream);
 
+/* The OS-MOM preconditioner (osMOMSolverD.h:115-120): precon_out =
+ * 1 / max(A^T (W A 1), 1e-6) over every subset of the plan, W being each
+ * subset's offset weight as its mult_MH applies it (the ones image is
+ * projected and back-projected subset by subset, as the reference's
+ * all-subset mult_M / mult_MH do).  Uses the plan's solver workspace
+ * (allocated on first use, so the first call must not be captured). */
+CBCT_API cbct_status cbct_osmom_precon(cbct_plan* plan, float* precon_out, void* stream);
+
+/* One OS-MOM subset step (osMOMSolverD.h:142-175 without regularisers) as the
+ * two kernels cbct_osmom_solve runs per subset:
+ *   r = w_off (A_s z - b_s) into r_work (W*H*|s| floats), and
+ *   norm2_out[0] = ||A_s z - b_s||^2 in FP64 when norm2_out is not NULL;
+ *   then, fused into the back-projection of r:
+ *   zt = z - step * precon * A_s^T r ; x = nonneg ? max(zt,0) : zt ;
+ *   z = x (1+mom) - mom xold ; xold = x.
+ * b_s: the subset's measured projections, of type b_dtype.  step is
+ * beta / (1 + gamma i) * n_subsets and mom = (told - 1) / t, the solver's
+ * values (:142, :155-157, :171-173).  A caller that keeps its own loop (the
+ * reference driver's osMOMSolverD) gets the solver's arithmetic per step. */
+CBCT_API cbct_status cbct_osmom_step(cbct_plan* plan, int32_t s, cbct_dtype b_dtype, const void* b_s, float* z,
+                                     float* xold, const float* precon, float* r_work, float step, float mom,
+                                     int32_t nonneg, double* norm2_out, void* stream);
+
 /* One OS-MOM update (osMOMSolverD.h:155-175 without regularisers):
  *   zt = z - step * precon * g ; x = nonneg ? max(zt,0) : zt
  *   z  = x*(1+mom) - mom*xold ; xold = x                                  */
@@ -299,7 +352,10 @@ CBCT_API cbct_status cbct_tv_step(float* x, float* P, const float* s, const floa
                                   int32_t nz, float scale, float tau, float tau_lambda, void* stream);
 
 /* FP64 reductions: kind 0 = dot(a,b), 1 = nrm2(a)^2 (sum of squares),
- * 2 = asum(a).  out_dev: one double in device memory. */
+ * 2 = asum(a).  out_dev: one double in device memory.  The per-block partial
+ * sums use a buffer taken from the device's stream-ordered memory pool on
+ * `stream` and returned in stream order (cudaMallocAsync / cudaFreeAsync), so
+ * calls on different streams or host threads never share it. */
 CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* b, size_t n,
                             double* out_dev, void* stream);
 
@@ -308,15 +364,18 @@ CBCT_API cbct_status cbct_reduce_f64(int32_t kind, const float* a, const float* 
  * cudaMalloc while it runs, such as a latency-bound caller sharing the GPU
  * with other work (cudaMalloc may wait for the whole device to go idle) or a
  * host whose device memory is owned by another allocator (a framework's
- * caching allocator) that forbids side allocations.  cbct_reduce_f64 allocates its
- * partial-sum buffer on its first call on each host thread; this entry point
- * allocates nothing and calls no allocating routine.
+ * caching allocator) that forbids side allocations.  cbct_reduce_f64 takes its
+ * partial-sum buffer from the stream-ordered pool on every call; this entry
+ * point allocates nothing and calls no allocating routine.
  * Scratch: the per-block partial sums live in a static device array of 1024
  * doubles (8 KiB) that every GPU which loads the library holds until the
- * process exits.  A call needs min(592, ceil(n/256)) of them; a call that
- * would need more than 1024 is rejected with CBCT_ERR_INVALID_ARGUMENT.
+ * process exits.  A call needs min(592, ceil(n/256)) of them: the reduction's
+ * grid is capped at 592 blocks, so every n fits (a build whose launch shape
+ * needed more than 1024 would reject the call with CBCT_ERR_INVALID_ARGUMENT).
  * Set-up: the first call on each device looks up the array's device address
  * (with that device current); make that first call before any stream capture.
+ * The looked-up address is kept for the life of the library, which assumes
+ * the device is not reset (cudaDeviceReset) in between.
  * All calls share the array: each call writes every partial it reads, so an
  * earlier call's leftovers never reach a result, but calls that overlap on the
  * GPU (different streams with no ordering between them) race on it. */

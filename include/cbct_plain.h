@@ -56,6 +56,17 @@ CBCT_API cbct_status cbct_plain_fdk(const cbct_geometry* g, const float* angles_
                                     int32_t n_views, const float* proj_host, float* vol_host, const float* filter,
                                     int32_t offset_correction, int32_t views_per_batch);
 
+/* Device-only times of the reference's two kernels (conebeam_forwards_projection_kernel,
+ * conebeam_projection.cu:412-528, and conebeam_backwards_projection_kernel<false>, :922-1037)
+ * on the same views: the volume and the projections are copied into their
+ * texture arrays once, then each kernel is launched reps times between CUDA
+ * events on the legacy stream.  proj_out (W*H*n floats) and vol_out receive the
+ * kernels' results; ms_out[0] = forward, ms_out[1] = back-projection, ms per launch. */
+CBCT_API cbct_status cbct_plain_kernel_times(const cbct_geometry* g, const float* angles_deg,
+                                             const float* offsets_xy, int32_t n_views, const float* vol,
+                                             const float* proj, float* proj_out, float* vol_out, int32_t reps,
+                                             float* ms_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -181,6 +181,16 @@ def fdk(g: Geometry, proj, angles, offsets, short_scan=False, offset_corr=False,
     return out
 
 
+def fdk_recipe(g: Geometry, proj, angles, offsets, filt=None):
+    """FDK_reconstruct_3d.cpp:152-161: FDK (hoCuConebeamProjectionOperator
+    mult_MH with filtered back-projection), then x *= <A x, p> / <A x, A x>
+    with A the operator's mult_M (no offset weight in FBP mode)."""
+    x = fdk(g, proj, angles, offsets, filt=filt)
+    ax = forward(g, x, angles, offsets)
+    p = np.asarray(proj, dtype=np.float64)
+    return x * (np.vdot(ax, p) / np.vdot(ax, ax))
+
+
 def subset_partition(n_views: int, n_subsets: int, view_bin=None):
     vb = np.zeros(n_views, dtype=np.int32) if view_bin is None else np.ascontiguousarray(view_bin, dtype=np.int32)
     order = np.zeros(n_views, dtype=np.int32)

@@ -82,3 +82,25 @@ def test_masked_osmom_matches_oracle(gtb, O, cuda):
     z = torch.empty(plan.vol_shape, dtype=torch.float32, device=cuda)
     plan.osmom(torch.from_numpy(bp.astype(np.float32)).to(cuda), z, None, 2, nonneg=True, use_graph=True)
     assert O.rel_l2(z.cpu().numpy(), zr) < 1e-4
+
+
+def test_masked_accumulating_backprojection(gtb, O, cuda):
+    """mult_MH with accumulate and a mask: the reference applies the mask to
+    the whole output after accumulating (cuConebeamProjectionOperator.cpp:113-114,
+    apply_mask on `output`), so voxels outside the mask lose the caller's
+    earlier contents too: out = mask * (incoming + A^T p)."""
+    import torch
+    case = make("offset")
+    rng = np.random.default_rng(4)
+    p = rng.uniform(0, 1, (case.angles.size, case.H, case.W))
+    mask = (rng.uniform(size=(case.nz, case.ny, case.nx)) < 0.6).astype(np.uint8)
+    incoming = rng.uniform(0.5, 1.5, (case.nz, case.ny, case.nx))
+    g = case.oracle_geom(O)
+    ref = (incoming + O.backproject(g, p, case.angles, case.offsets)) * mask
+    plan = gtb.Plan(case.cgeom(gtb), case.angles, case.offsets)
+    plan.set_mask(torch.from_numpy(mask).to(cuda))
+    out = torch.from_numpy(incoming.astype(np.float32)).to(cuda)
+    plan.backproject(torch.from_numpy(p.astype(np.float32)).to(cuda), out, accumulate=True)
+    got = out.cpu().numpy()
+    assert O.rel_l2(got, ref) < 1e-4
+    assert np.all(got[mask == 0] == 0.0)

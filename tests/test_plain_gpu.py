@@ -1,11 +1,27 @@
 """The plain reference-replica GPU path (include/cbct_plain.h).
 
 It restates the reference's CUDA kernels with hardware texture filtering, so
-it stands in for "the reference's CUDA projector outputs": it must agree with
-the oracle's texture-emulating mode closely and with the exact FP64 oracle to
-within the texture unit's 9-bit interpolation weights.  The product's FP32
-path is compared against it on identical geometry and the difference is
-bounded by the same texture-weight error."""
+it stands in for "the reference's CUDA projector outputs".  The bounds below
+are about twice the values measured on a B200 (printed by each test):
+
+  forward, plain vs the oracle's texture-emulating mode  2.1e-4 .. 2.6e-4
+  forward, plain vs exact FP64                            2.4e-4 .. 2.9e-4
+  back-projection, plain vs texture mode / exact          4.3e-4 / 5.6e-4
+  product vs plain (64^3 from 45 views)                   1.2e-4 (product vs FP64: 2.7e-6)
+  OS-MOM, 2 iterations, plain vs FP64                     3.7e-4
+  FDK (cuFFT row filter, texture back-projection) vs FP64 2.1e-3 .. 2.3e-3
+
+The texture unit interpolates with 9-bit weights (8 fractional bits): each
+tap's weight is the fraction rounded to a multiple of 1/256.  The
+texture-emulating oracle quantises its FP64 fractions the same way, but the
+replica's fractions come from FP32 fast-math coordinates that differ from the
+FP64 ones by about 1e-6 relative (1e-4 texel at 128 texels), enough to move a
+few per cent of the taps across a 1/256 step.  Those flipped steps leave the
+emulation about 2e-4 from the hardware, close to the whole quantisation
+error, so the emulation does not pin the replica much tighter than exact FP64
+does; the ramp filter's high frequencies make the FDK's share ten times
+larger.  The product's FP32 software interpolation has none of this: it is
+within 3e-6 of FP64."""
 import ctypes as C
 
 import numpy as np
@@ -52,7 +68,7 @@ def test_plain_forward_vs_oracle_modes(gtb, O, cuda, name):
     exact = O.forward(g, vol, case.angles, case.offsets, mode=0)
     e_tex, e_exact = O.rel_l2(plain, tex), O.rel_l2(plain, exact)
     print(f"{name}: plain vs texture-emulating oracle {e_tex:.2e}, vs exact FP64 {e_exact:.2e}")
-    assert e_tex < 2e-3 and e_exact < 5e-3
+    assert e_tex < 5e-4 and e_exact < 6e-4
 
 
 def test_plain_backproject_vs_oracle(gtb, O, cuda):
@@ -66,7 +82,7 @@ def test_plain_backproject_vs_oracle(gtb, O, cuda):
     exact = O.backproject(g, pw, case.angles, case.offsets, mode=0)
     e_tex, e_exact = O.rel_l2(plain, tex), O.rel_l2(plain, exact)
     print(f"plain BP vs texture-emulating oracle {e_tex:.2e}, vs exact FP64 {e_exact:.2e}")
-    assert e_tex < 2e-3 and e_exact < 5e-3
+    assert e_tex < 9e-4 and e_exact < 1.2e-3
 
 
 def test_product_path_vs_plain_path(gtb, O, cuda):
@@ -87,7 +103,7 @@ def test_product_path_vs_plain_path(gtb, O, cuda):
     d_plain, d_ours = O.rel_l2(ours, plain), O.rel_l2(ours, exact)
     print(f"product vs plain texture path {d_plain:.2e}; product vs FP64 {d_ours:.2e}; "
           f"plain vs FP64 {O.rel_l2(plain, exact):.2e}")
-    assert d_ours < 1e-4 and d_plain < 5e-3
+    assert d_ours < 1e-5 and d_plain < 2.5e-4
 
 
 def test_plain_osmom_vs_oracle(gtb, O, cuda):
@@ -112,8 +128,10 @@ def test_plain_osmom_vs_oracle(gtb, O, cuda):
            oc.ctypes.data, bt.data_ptr(), z.data_ptr(), 2, 1, resid.ctypes.data)
     e = O.rel_l2(z.cpu().numpy(), zr)
     print(f"plain OS-MOM vs FP64 oracle {e:.2e}")
-    assert e < 1e-2
-    assert np.allclose(resid, rr, rtol=2e-2)
+    assert e < 8e-4
+    r_rel = float(np.max(np.abs(resid - rr) / np.abs(rr)))
+    print(f"plain OS-MOM residual norms vs FP64: max relative difference {r_rel:.2e}")
+    assert r_rel < 2e-2
 
 
 @pytest.mark.parametrize("name,batch", [("cube", 20), ("offset", 7)])
@@ -140,4 +158,4 @@ def test_plain_fdk_vs_oracle_and_product(gtb, O, cuda, name, batch):
     plan.fdk(ph.to(cuda), prod, None, L.CBCT_FDK_OFFSET if off else 0)
     e_prod = O.rel_l2(vol.numpy(), prod.cpu().numpy())
     print(f"{name}: plain FDK vs FP64 {e_ref:.2e}, vs product {e_prod:.2e}")
-    assert e_ref < 5e-3 and e_prod < 5e-3
+    assert e_ref < 4.5e-3 and e_prod < 4.5e-3

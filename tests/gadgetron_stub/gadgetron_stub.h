@@ -29,23 +29,50 @@ struct vector_td {
 using floatd2 = vector_td<float, 2>;
 using floatd3 = vector_td<float, 3>;
 
+// Host array: owns its elements, or views memory it does not own (the
+// reference's hoCuNDArray(dims*, ptr) constructor, used for per-bin views).
 template <class T>
 class hoCuNDArray {
  public:
   hoCuNDArray() = default;
-  explicit hoCuNDArray(const std::vector<size_t>& d) : dims_(d), data_(count(d)) {}
-  T* get_data_ptr() { return data_.data(); }
+  explicit hoCuNDArray(const std::vector<size_t>& d) : dims_(d), own_(count(d)), ptr_(own_.data()) {}
+  explicit hoCuNDArray(const std::vector<size_t>* d) : hoCuNDArray(*d) {}
+  explicit hoCuNDArray(const boost::shared_ptr<std::vector<size_t>>& d) : hoCuNDArray(*d) {}
+  hoCuNDArray(const std::vector<size_t>* d, T* ptr) : dims_(*d), ptr_(ptr) {}
+  hoCuNDArray(const hoCuNDArray& o) : dims_(o.dims_), own_(o.ptr_, o.ptr_ + count(o.dims_)), ptr_(own_.data()) {}
+  hoCuNDArray& operator=(const hoCuNDArray& o) {
+    dims_ = o.dims_;
+    own_.assign(o.ptr_, o.ptr_ + count(o.dims_));
+    ptr_ = own_.data();
+    return *this;
+  }
+  T* get_data_ptr() { return ptr_; }
+  const T* get_data_ptr() const { return ptr_; }
   size_t get_size(size_t i) const { return i < dims_.size() ? dims_[i] : 1; }
-  size_t get_number_of_elements() const { return data_.size(); }
+  size_t get_number_of_dimensions() const { return dims_.size(); }
+  size_t get_number_of_elements() const { return count(dims_); }
   boost::shared_ptr<std::vector<size_t>> get_dimensions() const { return boost::make_shared<std::vector<size_t>>(dims_); }
   static size_t count(const std::vector<size_t>& d) {
     return std::accumulate(d.begin(), d.end(), size_t(1), std::multiplies<size_t>());
   }
+  hoCuNDArray& operator*=(T s) {
+    for (size_t i = 0; i < get_number_of_elements(); ++i) ptr_[i] *= s;
+    return *this;
+  }
 
  private:
   std::vector<size_t> dims_;
-  std::vector<T> data_;
+  std::vector<T> own_;
+  T* ptr_ = nullptr;
 };
+
+// Gadgetron's dot of two host arrays (hoCuNDArray_blas), here in double on the host.
+template <class T>
+T dot(hoCuNDArray<T>* a, hoCuNDArray<T>* b) {
+  double s = 0.0;
+  for (size_t i = 0; i < a->get_number_of_elements(); ++i) s += double(a->get_data_ptr()[i]) * b->get_data_ptr()[i];
+  return T(s);
+}
 
 template <class T>
 class cuNDArray {
@@ -56,6 +83,7 @@ class cuNDArray {
     if (cudaMalloc(&data_, bytes()) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
   }
   explicit cuNDArray(const std::vector<size_t>& d) : cuNDArray(&d) {}
+  explicit cuNDArray(const boost::shared_ptr<std::vector<size_t>>& d) : cuNDArray(d.get()) {}
   cuNDArray(const std::vector<size_t>& d, T* ptr) : dims_(d), data_(ptr), owned_(false) {}
   cuNDArray(const cuNDArray&) = delete;
   cuNDArray& operator=(const cuNDArray&) = delete;
@@ -94,6 +122,7 @@ template <class ARRAY>
 class subsetOperator : public linearOperator<ARRAY> {
  public:
   explicit subsetOperator(int subsets = 1) : number_of_subsets(subsets) {}
+  using linearOperator<ARRAY>::get_codomain_dimensions;
   virtual void mult_M(ARRAY* in, ARRAY* out, int subset, bool accumulate) = 0;
   virtual void mult_MH(ARRAY* in, ARRAY* out, int subset, bool accumulate) = 0;
   virtual void mult_MH_M(ARRAY* in, ARRAY* out, int subset, bool accumulate) = 0;

@@ -25,6 +25,8 @@ from .operators import (  # noqa: F401
     default_frequency_filter, fdk_reconstruct_3d, hann_ramp_filter, hoCuConebeamProjectionOperator,
     osMOMSolverD, osSARTSolver, phantom_voxelize, reduce_f64, subset_partition)
 from . import phantom  # noqa: F401
+from . import acquisition_io  # noqa: F401
+from .acquisition_io import read_real, save_real  # noqa: F401
 
 __version__ = "0.1.0"
 

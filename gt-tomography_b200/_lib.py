@@ -32,7 +32,8 @@ EXPORTED = [
     "cbct_status_string", "cbct_last_error", "cbct_version", "cbct_subset_partition",
     "cbct_default_frequency_filter", "cbct_cosine_weights", "cbct_is_short_scan",
     "cbct_offset_override", "cbct_plan_create", "cbct_plan_destroy", "cbct_plan_subset",
-    "cbct_plan_forward_variant", "cbct_plan_set_option", "cbct_plan_read_flags", "cbct_plan_check", "cbct_forward",
+    "cbct_plan_forward_variant", "cbct_plan_set_option", "cbct_plan_read_flags", "cbct_plan_check", "cbct_microbench_interp",
+    "cbct_forward",
     "cbct_backproject", "cbct_offset_correct", "cbct_fdk_filter", "cbct_fdk",
     "cbct_forward_residual", "cbct_osmom_precon", "cbct_osmom_step", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
     "cbct_osmom_solve",
@@ -122,6 +123,7 @@ _SIGS = {
     "cbct_plan_set_option": (C.c_int, [_vp, _i32, _i32]),
     "cbct_plan_read_flags": (C.c_int, [_vp, _vp, _i32]),
     "cbct_plan_check": (C.c_int, [_vp, _vp]),
+    "cbct_microbench_interp": (C.c_int, [_i32, _i32, C.POINTER(C.c_double), _vp]),
     "cbct_forward": (C.c_int, [_vp, _i32, C.c_int, _vp, _vp, _i32, _vp]),
     "cbct_backproject": (C.c_int, [_vp, _i32, _vp, _vp, _u32, _i32, _i32, _vp]),
     "cbct_offset_correct": (C.c_int, [_vp, _i32, _vp, _i32, _vp]),

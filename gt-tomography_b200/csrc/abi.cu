@@ -481,6 +481,14 @@ cbct_status cbct_plan_check(cbct_plan* plan, void* stream) {
   });
 }
 
+cbct_status cbct_microbench_interp(int32_t kind, int32_t groups, double* rate_out, void* stream) {
+  return guard([&] {
+    CBCT_REQUIRE(kind == 2 || kind == 3, "kind must be 3 (trilinear) or 2 (bilinear)");
+    CBCT_REQUIRE(groups >= 1 && rate_out, "bad arguments");
+    *rate_out = microbench_interp(kind, groups, 5, S(stream));
+  });
+}
+
 cbct_status cbct_plan_read_flags(cbct_plan* plan, int32_t* flags_out, int32_t reset) {
   return guard([&] {
     CBCT_REQUIRE(plan && flags_out, "bad arguments");

@@ -343,6 +343,10 @@ void tv_update_launch(const float* P, float* x, const float* s, const float* D, 
 void plan_autotune(cbct_plan* p, float* times, cudaStream_t st);
 void graph_cache_free(cbct_plan* p);
 
+// microbench.cu: interpolations per second of the projectors' inner operation
+// from shared memory (kind 3 = trilinear, 2 = bilinear)
+double microbench_interp(int kind, int groups, int reps, cudaStream_t st);
+
 // mask.cu
 void spacecarver_launch(cbct_plan* p, int s, const float* proj, float limit, unsigned char* mask, int combine,
                         cudaStream_t st);

@@ -17,6 +17,7 @@
 // inverse keeps the two rows apart.  The spectrum (with the 1/L scale) is
 // computed once per filter on the host in FP64.
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "device_common.cuh"
@@ -294,6 +295,307 @@ __global__ void __launch_bounds__(kRegFftThreads, CBCT_FDK_MINB) fdk_filter_reg_
   }
 }
 
+// ------------------------------------------------------------ staged register FFT filter
+// The register four-step filter above waits on its own row loads, and its
+// 32-point transforms multiply by run-time twiddles, unit ones included.
+// This version keeps every warp's next two units of rows in flight: each warp
+// owns two shared-memory stages, and one lane issues 1-D bulk copies
+// (cp.async.bulk, one per row, completing on the stage's mbarrier) for the
+// unit after next as soon as the current unit's rows are in registers, so the
+// HBM reads of later rows overlap the transforms of earlier ones.  The
+// 32-point transforms use compile-time twiddles (multiplications by 1 and -i
+// vanish) and paired FP32 adds (FADD2/FFMA2); the cosine weight is evaluated
+// in place (SAD / sqrt(SAD^2 + s^2 + t^2), the formula of
+// hoCuConebeamProjectionOperator.cpp:84-97) instead of read from a table; the
+// sin^2 offset weights of the output row are fetched before the last inverse
+// pass.  A unit is 2G consecutive rows (G transforms of two rows per warp);
+// rows sit in the stage with a padded stride so the two half-warps of a
+// 16-lane transform read different banks.
+
+// cos(m pi / 16) for 0 <= m <= 8 from its Taylor series (exact at 0 and 8).
+constexpr double cos_pi16(int m) {
+  if (m == 0) return 1.0;
+  if (m == 8) return 0.0;
+  const double x = double(m) * (3.14159265358979323846 / 16.0);
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 16; ++k) {
+    term *= -x * x / double((2 * k - 1) * (2 * k));
+    sum += term;
+  }
+  return sum;
+}
+
+// a * W_32^M (W_32 = exp(-2 pi i / 32)), or a * conj(W_32^M) when INV.
+template <int M, bool INV>
+__device__ __forceinline__ float2 tw32(float2 a) {
+  static_assert(M >= 0 && M < 16, "twiddle index");
+  if constexpr (M == 0) {
+    return a;
+  } else if constexpr (M == 8) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);   // * (+i) / * (-i)
+  } else {
+    constexpr float c = float(M <= 8 ? cos_pi16(M) : -cos_pi16(16 - M));
+    constexpr float sn = float(M <= 8 ? cos_pi16(8 - M) : cos_pi16(M - 8));   // sin(M pi / 16)
+    constexpr float wi = INV ? sn : -sn;
+    return make_float2(fmaf(a.x, c, -a.y * wi), fmaf(a.x, wi, a.y * c));
+  }
+}
+
+// Butterflies of stage LEN with offset K in every group of an N-point
+// decimation-in-time transform held in v[OFF .. OFF + N).
+template <int N, bool INV, int OFF, int NV, int LEN, int K>
+__device__ __forceinline__ void dit_k(float2 (&v)[NV]) {
+#pragma unroll
+  for (int i = 0; i < N; i += LEN) {
+    const float2 a = v[OFF + i + K];
+    const float2 b = tw32<K * (32 / LEN), INV>(v[OFF + i + K + LEN / 2]);
+    v[OFF + i + K] = __fadd2_rn(a, b);
+    v[OFF + i + K + LEN / 2] = __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+  }
+}
+
+template <int N, bool INV, int OFF, int NV, int LEN, int... Ks>
+__device__ __forceinline__ void dit_stage(float2 (&v)[NV], std::integer_sequence<int, Ks...>) {
+  (dit_k<N, INV, OFF, NV, LEN, Ks>(v), ...);
+}
+
+template <int N, bool INV, int OFF, int NV, int LEN>
+__device__ __forceinline__ void dit_stages(float2 (&v)[NV]) {
+  if constexpr (LEN <= N) {
+    dit_stage<N, INV, OFF, NV, LEN>(v, std::make_integer_sequence<int, LEN / 2>{});
+    dit_stages<N, INV, OFF, NV, LEN * 2>(v);
+  }
+}
+
+// In-register N-point DFT (N = 16 or 32), natural order in and out.
+template <int N, bool INV, int OFF, int NV>
+__device__ __forceinline__ void fft_ct(float2 (&v)[NV]) {
+  constexpr int bits = N == 16 ? 4 : 5;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = brev_bits(i, bits);
+    if (j > i) {
+      const float2 t = v[OFF + i];
+      v[OFF + i] = v[OFF + j];
+      v[OFF + j] = t;
+    }
+  }
+  dit_stages<N, INV, OFF, NV, 2>(v);
+}
+
+// Cosine weight evaluated in place: w(u, v) = SAD / sqrt(SAD^2 + s^2 + t^2),
+// s = su u + bu, t = sv v + bv.
+struct CosWeight {
+  int on;
+  float sad, sad2;
+  float su, bu, sv, bv;
+};
+
+#ifndef CBCT_FDK_ASYNC_WARPS
+#define CBCT_FDK_ASYNC_WARPS 6
+#endif
+constexpr int kAsyncWarps = CBCT_FDK_ASYNC_WARPS;
+
+struct AsyncLayout {
+  size_t stage_bytes, stages, tbuf, tw, spec, bars, total;
+};
+
+template <class T, int TL>
+__host__ __device__ inline AsyncLayout async_layout(int Wp) {
+  constexpr int G = 32 / TL, L = 32 * TL;
+  AsyncLayout a{};
+  a.stage_bytes = (size_t)2 * G * Wp * sizeof(T);
+  a.stages = 0;
+  a.tbuf = a.stages + (size_t)kAsyncWarps * 2 * a.stage_bytes;
+  a.tw = a.tbuf + sizeof(float2) * (size_t)kAsyncWarps * G * 32 * (TL + 1);
+  a.spec = a.tw + sizeof(float2) * 32 * TL;
+  a.bars = a.spec + sizeof(float) * L;
+  a.total = a.bars + sizeof(uint64_t) * 2 * kAsyncWarps;
+  return a;
+}
+
+// Detector row and view of a row index, advanced by a fixed stride without a
+// division per step: row r = p H + v.
+struct RowPos {
+  int p, v;
+  __device__ __forceinline__ void advance(int dp, int dv, int H) {
+    p += dp;
+    v += dv;
+    if (v >= H) {
+      v -= H;
+      ++p;
+    }
+  }
+};
+
+// One transform's two rows, loaded from the stage with the pre-weights:
+// x[TL n1 + j] for n1 < 16 (the rest is the zero padding).  Rows past the end
+// of the projections, and samples past the row's end, are zero (selects, no
+// branches; every shared-memory read stays inside the kernel's allocation).
+template <class T, int TL, bool COS, bool PK, bool FULL>
+__device__ __forceinline__ void load_pair(float2 (&v)[32], const T* sa, const T* sb, int j, int W, bool oka, bool okb,
+                                          const CosWeight& cw, float qa, float qb, const float* pka,
+                                          const float* pkb) {
+#pragma unroll
+  for (int n1 = 0; n1 < 32; ++n1) {
+    if (n1 >= 16) {
+      v[n1] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const int n = TL * n1 + j;
+    float xa = sm_f(sa[n]), xb = sm_f(sb[n]);
+    if (COS) {
+      const float su = fmaf(float(n), cw.su, cw.bu);
+      xa *= cw.sad * rsqrtf(fmaf(su, su, qa));
+      xb *= cw.sad * rsqrtf(fmaf(su, su, qb));
+    }
+    if (PK) {
+      const int nc = FULL ? n : min(n, W - 1);
+      xa *= __ldg(pka + nc);
+      xb *= __ldg(pkb + nc);
+    }
+    const bool in_row = FULL || n < W;
+    v[n1] = make_float2((oka && in_row) ? xa : 0.f, (okb && in_row) ? xb : 0.f);
+  }
+}
+
+template <class T, int TL, bool COS, bool FULL>
+__global__ void __launch_bounds__(kAsyncWarps * 32, 2) fdk_filter_async_kernel(
+    const T* __restrict__ in, float* __restrict__ out, int W, int H, int rows, int Wp,
+    const float* __restrict__ spec, const float2* __restrict__ twL, CosWeight cw, const float* __restrict__ parker,
+    const float* __restrict__ post, unsigned wait_limit, int* flags) {
+  constexpr int G = 32 / TL, L = 32 * TL, S = TL + 1, RU = 2 * G;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const AsyncLayout lay = async_layout<T, TL>(Wp);
+  float2* const tbuf = reinterpret_cast<float2*>(smem + lay.tbuf);
+  float2* const stw = reinterpret_cast<float2*>(smem + lay.tw);
+  float* const sspec = reinterpret_cast<float*>(smem + lay.spec);
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + lay.bars);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane / TL, j = lane % TL;
+  for (int i = threadIdx.x; i < 32 * TL; i += kAsyncWarps * 32) stw[i] = twL[i];
+  for (int i = threadIdx.x; i < L; i += kAsyncWarps * 32) sspec[i] = spec[i];
+  if (lane == 0) {
+    mbar_init(&bars[2 * warp], 1);
+    mbar_init(&bars[2 * warp + 1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // From here on every warp works alone.
+  unsigned char* const my_st = smem + lay.stages + (size_t)warp * 2 * lay.stage_bytes;
+  float2* const buf = tbuf + ((size_t)warp * G + g) * 32 * S;
+  const int nunits = (rows + RU - 1) / RU;
+  const int w0 = blockIdx.x * kAsyncWarps + warp, nw = gridDim.x * kAsyncWarps;
+  auto issue = [&](int unit, int st) {
+    const int r0 = unit * RU;
+    const int nr = rows - r0 < RU ? rows - r0 : RU;
+    uint64_t* bar = &bars[2 * warp + st];
+    mbar_arrive_expect_tx(bar, uint32_t(nr) * uint32_t(W * sizeof(T)));
+    for (int r = 0; r < nr; ++r)
+      bulk_load(my_st + st * lay.stage_bytes + (size_t)r * Wp * sizeof(T), in + (size_t)(r0 + r) * W,
+                uint32_t(W * sizeof(T)), bar);
+  };
+  if (lane == 0) {
+    if (w0 < nunits) issue(w0, 0);
+    if (w0 + nw < nunits) issue(w0 + nw, 1);
+  }
+  // Row a of this lane's transform and its stride per unit step.
+  RowPos pos{(w0 * RU + 2 * g) / H, (w0 * RU + 2 * g) % H};
+  const int step_p = (nw * RU) / H, step_v = (nw * RU) % H;
+  int it = 0;
+  for (int unit = w0; unit < nunits; unit += nw, ++it, pos.advance(step_p, step_v, H)) {
+    const int st = it & 1;
+    const bool ok = mbar_wait_bounded(&bars[2 * warp + st], (it >> 1) & 1, wait_limit);
+    if (__any_sync(0xffffffffu, !ok)) {
+      // Give up: record it, let the copies in flight land (default limit), leave.
+      if (lane == 0) {
+        atomicAdd(&flags[1], 1);
+        (void)mbar_wait_bounded(&bars[2 * warp + st], (it >> 1) & 1, kWaitLimit);
+        if (unit + nw < nunits) (void)mbar_wait_bounded(&bars[2 * warp + (st ^ 1)], ((it + 1) >> 1) & 1, kWaitLimit);
+      }
+      __syncwarp();
+      return;
+    }
+    const int ra = unit * RU + 2 * g;
+    const bool oka = ra < rows, okb = ra + 1 < rows;
+    const int pa = pos.p, vra = pos.v;
+    const int pb = vra + 1 < H ? pa : pa + 1, vrb = vra + 1 < H ? vra + 1 : 0;
+    const T* sa = reinterpret_cast<const T*>(my_st + st * lay.stage_bytes) + (size_t)(2 * g) * Wp;
+    const T* sb = sa + Wp;
+    const float ta = fmaf(float(vra), cw.sv, cw.bv), tb = fmaf(float(vrb), cw.sv, cw.bv);
+    const float qa = fmaf(ta, ta, cw.sad2), qb = fmaf(tb, tb, cw.sad2);
+    float2 v[32];
+    if (parker) {
+      // Parker rows of the pair's views (rows outside the projections read view 0's).
+      const float* pka = parker + (size_t)(oka ? pa : 0) * W;
+      const float* pkb = parker + (size_t)(okb ? pb : 0) * W;
+      load_pair<T, TL, COS, true, FULL>(v, sa, sb, j, W, oka, okb, cw, qa, qb, pka, pkb);
+    } else {
+      load_pair<T, TL, COS, false, FULL>(v, sa, sb, j, W, oka, okb, cw, qa, qb, nullptr, nullptr);
+    }
+    __syncwarp();
+    if (lane == 0 && unit + 2 * nw < nunits) {
+      fence_proxy_async();   // the stage's reads above come before the copy that refills it
+      issue(unit + 2 * nw, st);
+    }
+    fft_ct<32, false, 0>(v);                             // v[k1]
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul(v[k1], stw[k1 * TL + j]);
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) buf[k1 * S + j] = v[k1];
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int n2 = 0; n2 < TL; ++n2) v[c * TL + n2] = buf[(j + c * TL) * S + n2];
+    fft_ct<TL, false, 0>(v);
+    if constexpr (G > 1) fft_ct<TL, false, TL>(v);
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int k2 = 0; k2 < TL; ++k2) {
+        const float h = sspec[(j + c * TL) + 32 * k2];
+        v[c * TL + k2] = __fmul2_rn(v[c * TL + k2], make_float2(h, h));
+      }
+    fft_ct<TL, true, 0>(v);
+    if constexpr (G > 1) fft_ct<TL, true, TL>(v);
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+#pragma unroll
+      for (int n2 = 0; n2 < TL; ++n2) buf[(j + c * TL) * S + n2] = v[c * TL + n2];
+    __syncwarp();
+    // Offset weights of the output row a, fetched ahead of the last pass (row b
+    // shares them unless the pair straddles two views).
+    float pwa[16];
+    const float* pob = post ? post + (size_t)(okb ? pb : 0) * W : nullptr;
+    if (post) {
+      const float* poa = post + (size_t)(oka ? pa : 0) * W;
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) pwa[n1] = __ldg(poa + (FULL ? TL * n1 + j : min(TL * n1 + j, W - 1)));
+    } else {
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) pwa[n1] = 1.f;
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) {
+      const float2 w = stw[k1 * TL + j];
+      v[k1] = cmul(buf[k1 * S + j], make_float2(w.x, -w.y));
+    }
+    __syncwarp();
+    fft_ct<32, true, 0>(v);                              // y[TL n1 + j] at v[n1]
+    float* oa = out + (size_t)ra * W;
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+      const int n = TL * n1 + j;
+      if (FULL || n < W) {
+        if (oka) oa[n] = v[n1].x * pwa[n1];
+        if (okb) oa[W + n] = v[n1].y * (pb == pa || !pob ? pwa[n1] : __ldg(pob + n));
+      }
+    }
+  }
+}
+
 // FP64 spectrum of the row filter on an L-point grid, scaled by 1/L.
 std::vector<float> filter_spectrum(const float* H, int W, int L) {
   std::vector<double> h(W);
@@ -461,11 +763,65 @@ static void fdk_filter_reg(const void* in, float* out, int W, int H, long rows, 
   check_launch("fdk_filter_reg_kernel");
 }
 
+// Row stride (elements) of a stage: W plus padding that keeps rows 16-byte
+// aligned and puts the two rows read together by the half-warps of a 16-lane
+// transform 16 banks apart.
 template <class T>
-static void fdk_filter_typed(const void* in, float* out, int W, int H, long rows, const FdkState* f,
+static int async_row_stride(int W, int TL) {
+  if (TL == 32) return W;   // one transform per warp: its two rows are read one at a time
+  const int step = 16 / (int)sizeof(T);
+  for (int pad = step; pad <= 8 * step; pad += step) {
+    const int words = int(2 * (W + pad) * sizeof(T) / 4);
+    if (words % 32 == 16) return W + pad;
+  }
+  return W + step;
+}
+
+// The staged filter for L = 512 / 1024 when rows can be bulk-copied (16-byte
+// aligned rows); returns false to fall back to the register filter.
+template <class T, int TL>
+static bool fdk_filter_async(cbct_plan* p, const void* in, float* out, int W, int H, long rows, const FdkState* f,
+                             bool cosine, const float* pk, const float* post, cudaStream_t st) {
+  if ((W * sizeof(T)) % 16 != 0 || (reinterpret_cast<uintptr_t>(in) % 16) != 0) return false;
+  const int Wp = async_row_stride<T>(W, TL);
+  const AsyncLayout lay = async_layout<T, TL>(Wp);
+  if (lay.total > (size_t)kSmemBudget) return false;
+  if (rows > (long)INT32_MAX / 2) return false;
+  const bool full = W == 16 * TL;
+  auto k = cosine ? (full ? fdk_filter_async_kernel<T, TL, true, true> : fdk_filter_async_kernel<T, TL, true, false>)
+                  : (full ? fdk_filter_async_kernel<T, TL, false, true> : fdk_filter_async_kernel<T, TL, false, false>);
+  ensure_smem_attr((const void*)k, lay.total);
+  int dev = 0, sms = 0, per_sm = 0;
+  CBCT_CUDA(cudaGetDevice(&dev));
+  CBCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CBCT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kAsyncWarps * 32, lay.total));
+  if (per_sm < 1) return false;
+  const long units = (rows + 2 * (32 / TL) - 1) / (2 * (32 / TL));
+  const int blocks = (int)std::max<long>(1, std::min<long>((long)sms * per_sm, (units + kAsyncWarps - 1) / kAsyncWarps));
+  CosWeight cw{};
+  const cbct_geometry& g = p->g;
+  cw.on = cosine ? 1 : 0;
+  cw.sad = g.SAD;
+  cw.sad2 = float(double(g.SAD) * g.SAD);
+  cw.su = float(double(g.SAD) * g.fov_u / (double(g.SDD) * W));
+  cw.bu = float(-0.5 * double(g.SAD) * g.fov_u / g.SDD);
+  cw.sv = float(double(g.SAD) * g.fov_v / (double(g.SDD) * H));
+  cw.bv = float(-0.5 * double(g.SAD) * g.fov_v / g.SDD);
+  k<<<blocks, kAsyncWarps * 32, lay.total, st>>>(static_cast<const T*>(in), out, W, H, (int)rows, Wp, f->t.spec,
+                                                  f->t.twL, cw, pk, post, p->gc.wait_limit, p->d_flags);
+  check_launch("fdk_filter_async_kernel");
+  return true;
+}
+
+template <class T>
+static void fdk_filter_typed(cbct_plan* p, const void* in, float* out, int W, int H, long rows, const FdkState* f,
                              const float* pre, const float* pk, const float* post, cudaStream_t st) {
   const int L = f->L;
 #ifndef CBCT_FDK_RADIX2_ONLY
+#ifndef CBCT_FDK_NO_ASYNC
+  if (L == 1024 && fdk_filter_async<T, 32>(p, in, out, W, H, rows, f, pre != nullptr, pk, post, st)) return;
+  if (L == 512 && fdk_filter_async<T, 16>(p, in, out, W, H, rows, f, pre != nullptr, pk, post, st)) return;
+#endif
   if (L == 1024) return fdk_filter_reg<T, 32>(in, out, W, H, rows, f, pre, pk, post, st);
   if (L == 512) return fdk_filter_reg<T, 16>(in, out, W, H, rows, f, pre, pk, post, st);
 #endif
@@ -495,9 +851,9 @@ void fdk_filter_launch(cbct_plan* p, int s, const void* in, float* out, const fl
     throw Error(CBCT_ERR_UNSUPPORTED, "cbct_fdk_filter without CBCT_FDK_RAMP is not implemented");
   }
   switch (in_dtype) {
-    case CBCT_F32: fdk_filter_typed<float>(in, out, W, H, rows, f, pre, pk, post, st); break;
-    case CBCT_F16: fdk_filter_typed<__half>(in, out, W, H, rows, f, pre, pk, post, st); break;
-    case CBCT_BF16: fdk_filter_typed<__nv_bfloat16>(in, out, W, H, rows, f, pre, pk, post, st); break;
+    case CBCT_F32: fdk_filter_typed<float>(p, in, out, W, H, rows, f, pre, pk, post, st); break;
+    case CBCT_F16: fdk_filter_typed<__half>(p, in, out, W, H, rows, f, pre, pk, post, st); break;
+    case CBCT_BF16: fdk_filter_typed<__nv_bfloat16>(p, in, out, W, H, rows, f, pre, pk, post, st); break;
     default: throw Error(CBCT_ERR_INVALID_ARGUMENT, "unknown projection storage type");
   }
 }

@@ -121,6 +121,26 @@ class CBCT_acquisition:
     def set_projections(self, p):
         self.projections = p
 
+    def load(self, filename):
+        """CBCT_acquisition::load (xray/CBCT_acquisition.h:178-303): the HDF5
+        acquisition layout, geometry version 2, projection version 1."""
+        from .acquisition_io import load_acquisition
+        SAD, SDD, fov, angles, offsets, proj = load_acquisition(filename)
+        self.geometry = CBCT_geometry(SAD, SDD, (float(fov[0]), float(fov[1])), angles, offsets)
+        self.projections = proj
+
+    def save(self, filename):
+        """CBCT_acquisition::save (xray/CBCT_acquisition.h:305-322)."""
+        from .acquisition_io import save_acquisition
+        g = self.geometry
+        save_acquisition(filename, g.SAD, g.SDD, g.FOV, g.angles, g.offsets, self.projections)
+
+    @classmethod
+    def from_file(cls, filename):
+        acq = cls(CBCT_geometry())
+        acq.load(filename)
+        return acq
+
 
 class CBCT_binning:
     """CBCT_binning (xray/CBCT_binning.h:18-172): lists of view indices per bin."""
@@ -143,6 +163,15 @@ class CBCT_binning:
     def get_3d_binning(self):
         allv = sorted({v for b in self.bins for v in b})
         return CBCT_binning([allv])
+
+    def load(self, filename):
+        """CBCT_binning::load (xray/CBCT_binning.h:106-148)."""
+        from .acquisition_io import load_binning
+        self.bins = load_binning(filename)
+
+    def save(self, filename):
+        from .acquisition_io import save_binning
+        save_binning(filename, self.bins)
 
 
 # ----------------------------------------------------------------- host helpers

@@ -180,6 +180,16 @@ CBCT_API cbct_status cbct_plan_autotune(cbct_plan* plan, float* times_ms_out, vo
 #define CBCT_OPT_STATUS_CHECK 5
 CBCT_API cbct_status cbct_plan_set_option(cbct_plan* plan, int32_t option, int32_t value);
 
+/* On-chip ceiling of the projectors' inner operation (no reference
+ * counterpart; a measurement of this library): FP32 software interpolation
+ * from a shared-memory box at the projectors' access pattern and arithmetic,
+ * with nothing else in the loop, over four waves of resident thread blocks.
+ * kind 3 = trilinear (the forward projectors' ray sample), 2 = bilinear (the
+ * back-projector's voxel-view update); groups = loop trips per thread (8
+ * samples per trip for kind 3, 16 for kind 2).  rate_out = interpolations per
+ * second (CUDA events, warm-up launch first).  Synchronises `stream`. */
+CBCT_API cbct_status cbct_microbench_interp(int32_t kind, int32_t groups, double* rate_out, void* stream);
+
 /* Reads (and optionally clears) the plan's device flag words:
  * flags_out[0] = range-check violations and footprints that did not fit their
  * shared-memory box, flags_out[1] = expired bounded waits.

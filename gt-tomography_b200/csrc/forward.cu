@@ -274,7 +274,7 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
 template <class V>
 constexpr int slab_min_blocks() { return sizeof(V) == 4 ? 3 : 4; }
 
-template <class V, int BX, bool CHECK>
+template <class V, int BX, bool CHECK, int NS>
 __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
                                                        const __grid_constant__ CUtensorMap map_t,
                                                        const V* __restrict__ vol,
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
     sh.mlo = INT_MAX;
     sh.mhi = INT_MIN;
     sh.abort_flag = 0;
-    for (int s = 0; s < kNStage; ++s) mbar_init(&sh.bars[s], 1);
+    for (int s = 0; s < NS; ++s) mbar_init(&sh.bars[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -376,12 +376,12 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
   auto issue = [&](int i) {
     int oe, od, oz, m;
     origin(i, oe, od, oz, m);
-    uint64_t* bar = &sh.bars[i % kNStage];
+    uint64_t* bar = &sh.bars[i % NS];
     mbar_arrive_expect_tx(bar, box_bytes);
-    tma_load_3d(smem_raw + (i % kNStage) * stage_stride, map, oe, od, oz, bar);
+    tma_load_3d(smem_raw + (i % NS) * stage_stride, map, oe, od, oz, bar);
   };
   if (tid == 0) {
-    for (int i = 0; i < min(kNStage, nslab); ++i) issue(i);
+    for (int i = 0; i < min(NS, nslab); ++i) issue(i);
   }
 
   float acc = 0.f;
@@ -390,8 +390,8 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
   int bad = 0;
   int done = 0;
   for (int i = 0; i < nslab; ++i) {
-    const int slot = i % kNStage;
-    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / kNStage) & 1, gc.wait_limit);
+    const int slot = i % NS;
+    const bool ok = mbar_wait_bounded(&sh.bars[slot], (i / NS) & 1, gc.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) { atomicAdd(&flags[1], 1); sh.abort_flag = 1; }
       break;
@@ -416,15 +416,15 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
                                          bad);
     }
     __syncthreads();
-    if (tid == 0 && i + kNStage < nslab) {
+    if (tid == 0 && i + NS < nslab) {
       fence_proxy_async();
-      issue(i + kNStage);
+      issue(i + NS);
     }
   }
   if (sh.abort_flag && tid == 0) {
     // Drain loads still in flight (bounded) before the CTA exits.
-    for (int i = done; i < min(done + kNStage, nslab); ++i)
-      (void)mbar_wait_bounded(&sh.bars[i % kNStage], (i / kNStage) & 1, kWaitLimit);
+    for (int i = done; i < min(done + NS, nslab); ++i)
+      (void)mbar_wait_bounded(&sh.bars[i % NS], (i / NS) & 1, kWaitLimit);
   }
   if (CHECK) {
     if (hit && kf != Nf) bad = 1;  // every sample of a hit ray must be consumed
@@ -1491,16 +1491,19 @@ void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim
   const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
   const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
                                   volT ? p->g.nx : p->g.ny, p->g.nz, b);
-  const size_t smem = kNStage * ((b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127)) + 128;
-  if (p->debug_checks) {
-    auto k = fwd_slab_kernel<V, BX, true>;
-    ensure_smem_attr((const void*)k, smem);
-    k<<<grid, 256, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
-  } else {
-    auto k = fwd_slab_kernel<V, BX, false>;
-    ensure_smem_attr((const void*)k, smem);
-    k<<<grid, 256, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
-  }
+  // Two stages while they leave the register-bound number of CTAs per SM;
+  // boxes so large that they would not (small volumes under detectors of
+  // about one pixel per voxel) stage one slab at a time, and the other CTAs'
+  // samples cover each CTA's wait.
+  const size_t stage = (b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127);
+  const size_t per_cta = sizeof(SlabShared) + 1024 + 128;
+  const bool two = (2 * stage + per_cta) * slab_min_blocks<V>() <= size_t(228) * 1024;
+  const size_t smem = (two ? 2 : 1) * stage + 128;
+  auto pick = [&](auto k2, auto k1) { return two ? k2 : k1; };
+  auto k = p->debug_checks ? pick(fwd_slab_kernel<V, BX, true, 2>, fwd_slab_kernel<V, BX, true, 1>)
+                           : pick(fwd_slab_kernel<V, BX, false, 2>, fwd_slab_kernel<V, BX, false, 1>);
+  ensure_smem_attr((const void*)k, smem);
+  k<<<grid, 256, smem, st>>>(mv, mt, vol, p->d_views + first, p->gc, b.bz, o, p->d_flags);
   check_launch("fwd_slab_kernel");
 }
 
@@ -1642,8 +1645,10 @@ void launch_typed(cbct_plan* p, int s, const void* vol_v, const FwdOut& o, cudaS
 
 template <class V, int BX>
 void prepare_width(size_t smem) {
-  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, false>, smem);
-  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, true>, smem);
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, false, 2>, smem);
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, true, 2>, smem);
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, false, 1>, smem);
+  ensure_smem_attr((const void*)fwd_slab_kernel<V, BX, true, 1>, smem);
 }
 
 template <class V, int BX>

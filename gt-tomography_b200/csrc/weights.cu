@@ -17,6 +17,7 @@
 // inverse keeps the two rows apart.  The spectrum (with the 1/L scale) is
 // computed once per filter on the host in FP64.
 #include <cmath>
+#include <map>
 #include <utility>
 #include <vector>
 
@@ -596,21 +597,65 @@ __global__ void __launch_bounds__(kAsyncWarps * 32, 2) fdk_filter_async_kernel(
   }
 }
 
+// In-place radix-2 FFT in double on the host (n a power of two), forward sign.
+static void fft_host(std::vector<double>& re, std::vector<double>& im) {
+  const size_t n = re.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  const double pi = 3.14159265358979323846;
+  for (size_t len = 2; len <= n; len <<= 1) {
+    const double ang = -2.0 * pi / double(len);
+    for (size_t k = 0; k < len / 2; ++k) {
+      const double wr = std::cos(ang * double(k)), wi = std::sin(ang * double(k));
+      for (size_t i = k; i < n; i += len) {
+        const size_t q = i + len / 2;
+        const double xr = re[q] * wr - im[q] * wi, xi = re[q] * wi + im[q] * wr;
+        re[q] = re[i] - xr;
+        im[q] = im[i] - xi;
+        re[i] += xr;
+        im[i] += xi;
+      }
+    }
+  }
+}
+
 // FP64 spectrum of the row filter on an L-point grid, scaled by 1/L.
+// h[j] = (1/2W) (H[0] + (-1)^j H[W] + 2 sum_k H[k] cos(pi j k / W)), |j| < W, is
+// summed with the angle-addition recurrence (exact cosines every 32 steps),
+// and the spectrum of the even kernel on L points is one FFT of length L.
 std::vector<float> filter_spectrum(const float* H, int W, int L) {
   std::vector<double> h(W);
   const double pi = 3.14159265358979323846;
   for (int j = 0; j < W; ++j) {
     double s = H[0] + ((j & 1) ? -1.0 : 1.0) * H[W];
-    for (int k = 1; k < W; ++k) s += 2.0 * H[k] * std::cos(pi * double((long)j * k % (2L * W)) / W);
+    const double th = pi * double(j) / W, c1 = std::cos(th), s1 = std::sin(th);
+    double c = c1, sn = s1;
+    for (int k = 1; k < W; ++k) {
+      if ((k & 31) == 0) {
+        const double a = pi * double((long)j * k % (2L * W)) / W;
+        c = std::cos(a);
+        sn = std::sin(a);
+      }
+      s += 2.0 * H[k] * c;
+      const double cn = c * c1 - sn * s1;
+      sn = sn * c1 + c * s1;
+      c = cn;
+    }
     h[j] = s / (2.0 * W);
   }
+  std::vector<double> re(L, 0.0), im(L, 0.0);
+  re[0] = h[0];
+  for (int j = 1; j < W; ++j) re[j] = re[L - j] = h[j];
+  fft_host(re, im);
   std::vector<float> spec(L);
-  for (int k = 0; k < L; ++k) {
-    double s = h[0];
-    for (int j = 1; j < W; ++j) s += 2.0 * h[j] * std::cos(2.0 * pi * double((long)j * k % L) / L);
-    spec[k] = float(s / L);
-  }
+  for (int k = 0; k < L; ++k) spec[k] = float(re[k] / L);
   return spec;
 }
 
@@ -645,6 +690,69 @@ void fdk_state_free(cbct_plan* p) {
   plan_dealloc(p, f->t.post);
   delete f;
   p->fdk_state = nullptr;
+}
+
+// Parker weights per (view, u) in FP64 (conebeam_projection.cu:169-194); the
+// fan angle of each column is evaluated once per column.
+static void build_parker(cbct_plan* p, FdkState* f) {
+  if (f->t.parker) return;
+  const int W = p->g.width, P = p->n_views;
+  const double pi = 3.14159265358979323846, eps = 0.001, q = 0.1;
+  const double delta = std::atan(p->g.fov_u / (2.0 * double(p->g.SDD)));
+  const double tand = std::tan(delta);
+  auto S = [&](double b) { return b <= -0.5 ? 0.0 : (b < 0.5 ? 0.5 * (1 + std::sin(pi * b)) : 1.0); };
+  std::vector<double> alpha(W), bp(W), bm(W);
+  for (int u = 0; u < W; ++u) {
+    alpha[u] = -std::atan((double(u) / W - 0.5) * 2.0 * tand);
+    bp[u] = q * (2 * (delta - alpha[u]) + eps);
+    bm[u] = q * (2 * (delta + alpha[u]) + eps);
+  }
+  std::vector<float> pk((size_t)W * P);
+  parallel_for(P, [&](int lo, int hi, int) {
+    for (int v = lo; v < hi; ++v) {
+      const double beta = p->angles[v] * (pi / 180.0);
+      for (int u = 0; u < W; ++u) {
+        const double a = alpha[u];
+        const double om = 0.5 * (S(beta / bp[u] - 0.5) + S((beta + 2 * (a - delta) - eps) / bp[u] + 0.5) -
+                                 S((beta - pi + 2 * a) / bm[u] - 0.5) - S((beta - pi - 2 * delta - eps) / bm[u] + 0.5));
+        pk[(size_t)v * W + u] = float(om);
+      }
+    }
+  });
+  f->t.parker = plan_alloc_n<float>(p, pk.size());
+  plan_upload(p, f->t.parker, pk.data(), sizeof(float) * pk.size());
+}
+
+// sin^2 offset weights per (view, u) in FP64 (conebeam_projection.cu:245-259);
+// views with the same offset share one computed row.
+static void build_post(cbct_plan* p, FdkState* f) {
+  if (f->t.post) return;
+  const int W = p->g.width, P = p->n_views;
+  const double pi = 3.14159265358979323846, fov = p->g.fov_u;
+  std::vector<float> po((size_t)W * P);
+  std::map<float, int> row_of;
+  for (int v = 0; v < P; ++v) {
+    const float key = p->offsets[2 * (size_t)v];
+    auto it = row_of.find(key);
+    if (it != row_of.end()) {
+      std::copy(po.begin() + (size_t)it->second * W, po.begin() + (size_t)(it->second + 1) * W, po.begin() + (size_t)v * W);
+      continue;
+    }
+    row_of[key] = v;
+    const double o = key, sg = o / std::fabs(o), omega = fov / 2.0 - std::fabs(o);
+    for (int u = 0; u < W; ++u) {
+      const double t = (fov * (double(u) / W - 0.5) + o) * sg;
+      double w = 1.0;
+      if (std::fabs(t) <= omega) {
+        const double sw = std::sin(pi * (t + omega) / (4 * omega));
+        w = sw * sw;
+      }
+      if (t < -omega) w = 0.0;
+      po[(size_t)v * W + u] = float(w);
+    }
+  }
+  f->t.post = plan_alloc_n<float>(p, po.size());
+  plan_upload(p, f->t.post, po.data(), sizeof(float) * po.size());
 }
 
 static FdkState* fdk_state(cbct_plan* p, const float* filter) {
@@ -689,39 +797,14 @@ static FdkState* fdk_state(cbct_plan* p, const float* filter) {
       }
     f->t.cosw = plan_alloc_n<float>(p, cw.size());
     plan_upload(p, f->t.cosw, cw.data(), sizeof(float) * cw.size());
-    // Parker weights per (view, u) in FP64 (conebeam_projection.cu:169-194).
-    std::vector<float> pk((size_t)W * P), po((size_t)W * P);
-    const double eps = 0.001, q = 0.1;
-    const double delta = std::atan(p->g.fov_u / (2.0 * SDD));
-    const double tand = std::tan(delta);
-    auto S = [&](double b) { return b <= -0.5 ? 0.0 : (b < 0.5 ? 0.5 * (1 + std::sin(pi * b)) : 1.0); };
-    for (int v = 0; v < P; ++v) {
-      const double beta = p->angles[v] * (pi / 180.0);
-      const double o = p->offsets[2 * v];
-      const double sg = o / std::fabs(o);
-      const double omega = p->g.fov_u / 2.0 - std::fabs(o);
-      for (int u = 0; u < W; ++u) {
-        const double alpha = -std::atan((double(u) / W - 0.5) * 2.0 * tand);
-        const double bp = q * (2 * (delta - alpha) + eps), bm = q * (2 * (delta + alpha) + eps);
-        const double om = 0.5 * (S(beta / bp - 0.5) + S((beta + 2 * (alpha - delta) - eps) / bp + 0.5) -
-                                 S((beta - pi + 2 * alpha) / bm - 0.5) -
-                                 S((beta - pi - 2 * delta - eps) / bm + 0.5));
-        pk[(size_t)v * W + u] = float(om);
-        // sin^2 offset weight (conebeam_projection.cu:245-259)
-        const double t = (p->g.fov_u * (double(u) / W - 0.5) + o) * sg;
-        double w = 1.0;
-        if (std::fabs(t) <= omega) {
-          const double sw = std::sin(pi * (t + omega) / (4 * omega));
-          w = sw * sw;
-        }
-        if (t < -omega) w = 0.0;
-        po[(size_t)v * W + u] = float(w);
+    // The weight tables this plan's geometry calls for are made now (plan
+    // set-up, outside any stream capture); others on first use.
+    if (short_scan_rule(p->g, p->angles.data(), P)) build_parker(p, f);
+    for (int v = 0; v < P; ++v)
+      if (p->offsets[2 * (size_t)v] != 0.f) {
+        build_post(p, f);
+        break;
       }
-    }
-    f->t.parker = plan_alloc_n<float>(p, pk.size());
-    plan_upload(p, f->t.parker, pk.data(), sizeof(float) * pk.size());
-    f->t.post = plan_alloc_n<float>(p, po.size());
-    plan_upload(p, f->t.post, po.data(), sizeof(float) * po.size());
   }
   std::vector<float> want(W + 1);
   if (filter) std::copy(filter, filter + W + 1, want.begin());
@@ -843,6 +926,8 @@ void fdk_filter_launch(cbct_plan* p, int s, const void* in, float* out, const fl
   FdkState* f = fdk_state(p, filter);
   const long rows = (long)H * cnt;
   const float* pre = (flags & CBCT_FDK_COSINE) ? f->t.cosw : nullptr;
+  if (flags & CBCT_FDK_PARKER) build_parker(p, f);
+  if (flags & CBCT_FDK_OFFSET) build_post(p, f);
   const float* pk = (flags & CBCT_FDK_PARKER) ? f->t.parker + (size_t)first * W : nullptr;
   const float* post = (flags & CBCT_FDK_OFFSET) ? f->t.post + (size_t)first * W : nullptr;
   if (!(flags & CBCT_FDK_RAMP)) {

@@ -834,6 +834,10 @@ __device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, fl
 }
 
 // The quad's samples inside one slab, each ray's values added in ray order.
+#ifndef CBCT_QUAD_UNROLL
+#define CBCT_QUAD_UNROLL 1
+#endif
+
 template <class V, int BX, int SGN, bool CHECK>
 __device__ __forceinline__ void quad_samples(const V* __restrict__ s, float& kf, float Nf, float ce0, float cd0,
                                              float dce, float dcd, float idcd, float4 z0, float4 dz, float lo,
@@ -847,7 +851,23 @@ __device__ __forceinline__ void quad_samples(const V* __restrict__ s, float& kf,
   ke = fminf(fmaxf(ke, kf), Nf);
   while (ke > kf && out_at(ke - 1.f)) ke -= 1.f;
   while (ke < Nf && !out_at(ke)) ke += 1.f;
-  for (float k = kf; k < ke; k += 1.f) {
+  float k = kf;
+#if CBCT_QUAD_UNROLL > 1
+  // Two quad-samples evaluated before they are added (in ray order).
+  for (; k + 1.f < ke; k += 2.f) {
+    const float4 v0 = quad_eval<V, BX, CHECK>(s, k, c0, dc, z0, dz, cmo, maxidx, bad);
+    const float4 v1 = quad_eval<V, BX, CHECK>(s, k + 1.f, c0, dc, z0, dz, cmo, maxidx, bad);
+    acc.x += v0.x;
+    acc.y += v0.y;
+    acc.z += v0.z;
+    acc.w += v0.w;
+    acc.x += v1.x;
+    acc.y += v1.y;
+    acc.z += v1.z;
+    acc.w += v1.w;
+  }
+#endif
+  for (; k < ke; k += 1.f) {
     const float4 v = quad_eval<V, BX, CHECK>(s, k, c0, dc, z0, dz, cmo, maxidx, bad);
     acc.x += v.x;
     acc.y += v.y;

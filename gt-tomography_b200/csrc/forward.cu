@@ -822,15 +822,18 @@ __device__ __forceinline__ float4 quad_eval(const V* __restrict__ s, float k, fl
   const float2 td = make_float2(aed.y, aed.y);
   const float2 d01 = lerp2(make_float2(e0.x, e1.x), make_float2(e0.y, e1.y), td);   // planes fz, fz + 1
   const float2 d23 = lerp2(make_float2(e2.x, e3.x), make_float2(e2.y, e3.y), td);   // planes fz + 2, fz + 3
+  // Each ray lerps between two consecutive planes of the four: base value and
+  // difference picked by its plane offset (the same subtraction hi - lo for
+  // every ray that uses the pair, so the result is unchanged).
+  const float g0 = d01.y - d01.x, g1 = d23.x - d01.y, g2 = d23.y - d23.x;
   auto ray = [&](float sk, float cz, float fz) {
     const float lo = sk < 0.5f ? d01.x : (sk < 1.5f ? d01.y : d23.x);
-    const float hi = sk < 0.5f ? d01.y : (sk < 1.5f ? d23.x : d23.y);
-    return fmaf(cz - fz, hi - lo, lo);
+    const float gd = sk < 0.5f ? g0 : (sk < 1.5f ? g1 : g2);
+    return fmaf(cz - fz, gd, lo);
   };
   // the second-lowest ray is under one texel above the lowest: planes fz, fz + 1 or fz + 1, fz + 2
-  const float lo1 = s1 < 0.5f ? d01.x : d01.y, hi1 = s1 < 0.5f ? d01.y : d23.x;
-  return make_float4(fmaf(c0z - f0, d01.y - d01.x, d01.x), fmaf(c1z - f1, hi1 - lo1, lo1), ray(s2, c2z, f2),
-                     ray(s3, c3z, f3));
+  const float lo1 = s1 < 0.5f ? d01.x : d01.y, g1s = s1 < 0.5f ? g0 : g1;
+  return make_float4(fmaf(c0z - f0, g0, d01.x), fmaf(c1z - f1, g1s, lo1), ray(s2, c2z, f2), ray(s3, c3z, f3));
 }
 
 // The quad's samples inside one slab, each ray's values added in ray order.

@@ -393,9 +393,18 @@ struct CosWeight {
 };
 
 #ifndef CBCT_FDK_ASYNC_WARPS
-#define CBCT_FDK_ASYNC_WARPS 6
+#define CBCT_FDK_ASYNC_WARPS 8
 #endif
 constexpr int kAsyncWarps = CBCT_FDK_ASYNC_WARPS;
+// Stages per warp: with two, a unit's rows are in flight for two units'
+// compute; with one, for one (the copy is issued as soon as the rows are read).
+#ifndef CBCT_FDK_ASYNC_STAGES
+#define CBCT_FDK_ASYNC_STAGES 1
+#endif
+constexpr int kAsyncStages = CBCT_FDK_ASYNC_STAGES;
+#ifndef CBCT_FDK_ASYNC_MINB
+#define CBCT_FDK_ASYNC_MINB 2
+#endif
 
 struct AsyncLayout {
   size_t stage_bytes, stages, tbuf, tw, spec, bars, total;
@@ -407,11 +416,11 @@ __host__ __device__ inline AsyncLayout async_layout(int Wp) {
   AsyncLayout a{};
   a.stage_bytes = (size_t)2 * G * Wp * sizeof(T);
   a.stages = 0;
-  a.tbuf = a.stages + (size_t)kAsyncWarps * 2 * a.stage_bytes;
+  a.tbuf = a.stages + (size_t)kAsyncWarps * kAsyncStages * a.stage_bytes;
   a.tw = a.tbuf + sizeof(float2) * (size_t)kAsyncWarps * G * 32 * (TL + 1);
   a.spec = a.tw + sizeof(float2) * 32 * TL;
   a.bars = a.spec + sizeof(float) * L;
-  a.total = a.bars + sizeof(uint64_t) * 2 * kAsyncWarps;
+  a.total = a.bars + sizeof(uint64_t) * kAsyncStages * kAsyncWarps;
   return a;
 }
 
@@ -461,7 +470,7 @@ __device__ __forceinline__ void load_pair(float2 (&v)[32], const T* sa, const T*
 }
 
 template <class T, int TL, bool COS, bool FULL>
-__global__ void __launch_bounds__(kAsyncWarps * 32, 2) fdk_filter_async_kernel(
+__global__ void __launch_bounds__(kAsyncWarps * 32, CBCT_FDK_ASYNC_MINB) fdk_filter_async_kernel(
     const T* __restrict__ in, float* __restrict__ out, int W, int H, int rows, int Wp,
     const float* __restrict__ spec, const float2* __restrict__ twL, CosWeight cw, const float* __restrict__ parker,
     const float* __restrict__ post, unsigned wait_limit, int* flags) {
@@ -477,42 +486,45 @@ __global__ void __launch_bounds__(kAsyncWarps * 32, 2) fdk_filter_async_kernel(
   for (int i = threadIdx.x; i < 32 * TL; i += kAsyncWarps * 32) stw[i] = twL[i];
   for (int i = threadIdx.x; i < L; i += kAsyncWarps * 32) sspec[i] = spec[i];
   if (lane == 0) {
-    mbar_init(&bars[2 * warp], 1);
-    mbar_init(&bars[2 * warp + 1], 1);
+    for (int q = 0; q < kAsyncStages; ++q) mbar_init(&bars[kAsyncStages * warp + q], 1);
     fence_mbar_init();
   }
   __syncthreads();
   // From here on every warp works alone.
-  unsigned char* const my_st = smem + lay.stages + (size_t)warp * 2 * lay.stage_bytes;
+  unsigned char* const my_st = smem + lay.stages + (size_t)warp * kAsyncStages * lay.stage_bytes;
   float2* const buf = tbuf + ((size_t)warp * G + g) * 32 * S;
   const int nunits = (rows + RU - 1) / RU;
   const int w0 = blockIdx.x * kAsyncWarps + warp, nw = gridDim.x * kAsyncWarps;
   auto issue = [&](int unit, int st) {
     const int r0 = unit * RU;
     const int nr = rows - r0 < RU ? rows - r0 : RU;
-    uint64_t* bar = &bars[2 * warp + st];
+    uint64_t* bar = &bars[kAsyncStages * warp + st];
     mbar_arrive_expect_tx(bar, uint32_t(nr) * uint32_t(W * sizeof(T)));
     for (int r = 0; r < nr; ++r)
       bulk_load(my_st + st * lay.stage_bytes + (size_t)r * Wp * sizeof(T), in + (size_t)(r0 + r) * W,
                 uint32_t(W * sizeof(T)), bar);
   };
-  if (lane == 0) {
-    if (w0 < nunits) issue(w0, 0);
-    if (w0 + nw < nunits) issue(w0 + nw, 1);
-  }
+  if (lane == 0)
+    for (int q = 0; q < kAsyncStages; ++q)
+      if (w0 + q * nw < nunits) issue(w0 + q * nw, q);
   // Row a of this lane's transform and its stride per unit step.
   RowPos pos{(w0 * RU + 2 * g) / H, (w0 * RU + 2 * g) % H};
   const int step_p = (nw * RU) / H, step_v = (nw * RU) % H;
   int it = 0;
   for (int unit = w0; unit < nunits; unit += nw, ++it, pos.advance(step_p, step_v, H)) {
-    const int st = it & 1;
-    const bool ok = mbar_wait_bounded(&bars[2 * warp + st], (it >> 1) & 1, wait_limit);
+    const int st = it % kAsyncStages;
+    const uint32_t par = (it / kAsyncStages) & 1;
+    const bool ok = mbar_wait_bounded(&bars[kAsyncStages * warp + st], par, wait_limit);
     if (__any_sync(0xffffffffu, !ok)) {
       // Give up: record it, let the copies in flight land (default limit), leave.
       if (lane == 0) {
         atomicAdd(&flags[1], 1);
-        (void)mbar_wait_bounded(&bars[2 * warp + st], (it >> 1) & 1, kWaitLimit);
-        if (unit + nw < nunits) (void)mbar_wait_bounded(&bars[2 * warp + (st ^ 1)], ((it + 1) >> 1) & 1, kWaitLimit);
+        for (int q = 0; q < kAsyncStages; ++q) {
+          const int iq = it + q;
+          if (unit + q * nw < nunits)
+            (void)mbar_wait_bounded(&bars[kAsyncStages * warp + iq % kAsyncStages], (iq / kAsyncStages) & 1,
+                                    kWaitLimit);
+        }
       }
       __syncwarp();
       return;
@@ -535,9 +547,9 @@ __global__ void __launch_bounds__(kAsyncWarps * 32, 2) fdk_filter_async_kernel(
       load_pair<T, TL, COS, false, FULL>(v, sa, sb, j, W, oka, okb, cw, qa, qb, nullptr, nullptr);
     }
     __syncwarp();
-    if (lane == 0 && unit + 2 * nw < nunits) {
+    if (lane == 0 && unit + kAsyncStages * nw < nunits) {
       fence_proxy_async();   // the stage's reads above come before the copy that refills it
-      issue(unit + 2 * nw, st);
+      issue(unit + kAsyncStages * nw, st);
     }
     fft_ct<32, false, 0>(v);                             // v[k1]
 #pragma unroll

@@ -4,7 +4,9 @@
 // thread-local message; nothing throws across the boundary.  Host-side setup
 // logic restates the reference's operator setup (cited per function).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -275,10 +277,27 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   // Plans that never project forward skip the box sizing (a host loop over
   // every view, tile and slab); a forward call on them takes the gather kernel.
   if (!forward_buffers) p->fwd_pref = 2;
+#ifdef CBCT_SETUP_TIMING
+  // Build-time switch: the set-up phases' host times on stderr.
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+  const auto t0 = now();
+  forward_choose_variant(p.get());
+  const auto t1 = now();
+  if (forward_buffers) forward_prepare(p.get());
+  const auto t2 = now();
+  backproject_choose_variant(p.get());
+  const auto t3 = now();
+  backproject_prepare(p.get());
+  const auto t4 = now();
+  std::fprintf(stderr, "plan set-up ms: forward_choose %.1f forward_prepare %.1f bp_choose %.1f bp_prepare %.1f\n",
+               ms(t0, t1), ms(t1, t2), ms(t2, t3), ms(t3, t4));
+#else
   forward_choose_variant(p.get());
   if (forward_buffers) forward_prepare(p.get());
   backproject_choose_variant(p.get());
   backproject_prepare(p.get());
+#endif
   return p.release();
 }
 

@@ -24,8 +24,15 @@ CBCT_OPT_FORCE_GATHER = 2
 CBCT_OPT_FORWARD_KERNEL = 3
 CBCT_OPT_WAIT_LIMIT = 4
 CBCT_OPT_STATUS_CHECK = 5
+CBCT_ERR_INVALID_ARGUMENT = 1
+CBCT_ERR_CUDA = 2
+CBCT_ERR_OUT_OF_MEMORY = 3
+CBCT_ERR_UNSUPPORTED = 4
 CBCT_ERR_DEVICE_CHECK = 5
 CBCT_ERR_TIMEOUT = 6
+CBCT_ERR_BUDGET = 7
+CBCT_ERR_CANCELLED = 8
+CBCT_ERR_INTERNAL = 9
 
 # Every symbol the header declares (checked by the CPU tests).
 EXPORTED = [
@@ -37,7 +44,7 @@ EXPORTED = [
     "cbct_backproject", "cbct_offset_correct", "cbct_fdk_filter", "cbct_fdk",
     "cbct_forward_residual", "cbct_osmom_precon", "cbct_osmom_step", "cbct_osmom_update", "cbct_reduce_f64", "cbct_reduce_f64_noalloc",
     "cbct_osmom_solve",
-    "cbct_ossart_solve", "cbct_batch_osmom", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
+    "cbct_ossart_solve", "cbct_batch_osmom", "cbct_batch_osmom_fused", "cbct_phantom_voxelize", "cbct_phantom_project", "cbct_convert",
     "cbct_spacecarver", "cbct_apply_mask", "cbct_plan_set_mask", "cbct_plan_set_projection_weights",
     "cbct_fdk_filter_ex", "cbct_fdk_ex", "cbct_host_forward", "cbct_host_backproject", "cbct_plan_set_bins",
     "cbct_tv_step", "cbct_plan_autotune",
@@ -138,6 +145,7 @@ _SIGS = {
     "cbct_osmom_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
     "cbct_ossart_solve": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(CbctSolverParams), _vp, _vp]),
     "cbct_batch_osmom": (C.c_int, [C.POINTER(CbctBatchItem), _i32, _i32, _vp]),
+    "cbct_batch_osmom_fused": (C.c_int, [C.POINTER(CbctBatchItem), _i32, _vp]),
     "cbct_phantom_voxelize": (C.c_int, [_gp, _vp, _i32, _i32, _vp, _vp]),
     "cbct_phantom_project": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp]),
     "cbct_convert": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp]),

@@ -887,6 +887,10 @@ cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_
   return guard([&] { batch_osmom(items, n, n_streams, S(stream)); });
 }
 
+cbct_status cbct_batch_osmom_fused(const cbct_batch_item* items, int32_t n, void* stream) {
+  return guard([&] { batch_osmom_fused(items, n, S(stream)); });
+}
+
 cbct_status cbct_phantom_voxelize(const cbct_geometry* g, const float* ell, int32_t n, int32_t ss, float* vol,
                                   void* stream) {
   return guard([&] {

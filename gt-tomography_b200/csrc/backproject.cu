@@ -166,24 +166,23 @@ struct BpView {
   float cs, sn, ox, oy;
 };
 
+// One CTA's work: the kTX x kTY x kZT voxel block (bi, bj, bk) over the views
+// of the call.  Shared by the one-scan kernel (block = blockIdx) and the
+// work-list kernel over many scans (block = the item's); base_ptr is the
+// 128-byte aligned dynamic shared memory, bars/abort_flag the CTA's statics.
 template <int EPI, bool FDK, int BU>
-__global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
-                                                           const ViewParams* __restrict__ views, int n_views,
-                                                           GridConst gc, BpEpi e, int BV, int* flags) {
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ uint64_t bars[2];
-  __shared__ int abort_flag;
-  unsigned char* base_ptr =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+__device__ __forceinline__ void bp_tma_body(const CUtensorMap* map, const ViewParams* __restrict__ views,
+                                            int n_views, const GridConst& gc, const BpEpi& e, int BV, int* flags,
+                                            int bi, int bj, int bk, unsigned char* base_ptr, uint64_t* bars,
+                                            int& abort_flag) {
   const uint32_t box_bytes = uint32_t(BU * BV * 4);
   const uint32_t stage_stride = (box_bytes + 127u) & ~127u;
-  float* stage0 = reinterpret_cast<float*>(base_ptr);
   BpView* tv = reinterpret_cast<BpView*>(base_ptr + 2 * stage_stride);
   int2* org = reinterpret_cast<int2*>(tv + n_views);     // per view: (u origin, v origin)
   int2* ext = org + n_views;                             // per view: (max u, max v) for checks
   const int tid = threadIdx.x;
   const int nthr = kTX * kTY;
-  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY, k0 = blockIdx.z * kZT;
+  const int i0 = bi * kTX, j0 = bj * kTY, k0 = bk * kZT;
 
   for (int q = tid; q < n_views; q += nthr) {
     const ViewParams& vp = views[q];
@@ -230,7 +229,7 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
   auto issue = [&](int pv) {
     uint64_t* bar = &bars[pv & 1];
     mbar_arrive_expect_tx(bar, box_bytes);
-    tma_load_3d(base_ptr + (pv & 1) * stage_stride, &map, org[pv].x, org[pv].y, pv, bar);
+    tma_load_3d(base_ptr + (pv & 1) * stage_stride, map, org[pv].x, org[pv].y, pv, bar);
   };
   if (tid == 0) {
     for (int pv = 0; pv < min(2, n_views); ++pv) issue(pv);
@@ -296,7 +295,7 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
   }
   if (abort_flag && tid == 0) {
     for (int pv = done; pv < min(done + 2, n_views); ++pv)
-      (void)mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kWaitLimit);
+      if (!mbar_wait_bounded(&bars[pv & 1], (pv >> 1) & 1, kWaitLimit)) abort_flag = 2;
   }
   if (i >= gc.nx || j >= gc.ny) return;
   const size_t base = ((size_t)k0 * gc.ny + j) * gc.nx + i;
@@ -308,23 +307,118 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
   }
 }
 
+template <int EPI, bool FDK, int BU>
+__global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                           const ViewParams* __restrict__ views, int n_views,
+                                                           GridConst gc, BpEpi e, int BV, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ uint64_t bars[2];
+  __shared__ int abort_flag;
+  unsigned char* base_ptr =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  bp_tma_body<EPI, FDK, BU>(&map, views, n_views, gc, e, BV, flags, blockIdx.x, blockIdx.y, blockIdx.z, base_ptr,
+                            bars, abort_flag);
+}
+
+// One scan's entry in the work list of bp_tma_multi_kernel: the arguments of
+// its one-scan launch and where its CTAs start in the list.
+struct alignas(128) BpScanRec {
+  CUtensorMap map;             // the subset's projections (W, H, views), box BU x BV
+  const ViewParams* views;
+  int* flags;
+  GridConst gc;
+  BpEpi e;
+  int n_views, BV;
+  int tx, ty;                  // CTA grid of the scan (x, y; z follows)
+  int base;                    // work-list index of the scan's first CTA
+};
+
+// Work-list (persistent) back-projector over many scans of one box width:
+// resident CTAs take work-list items (one voxel block of one scan) from an
+// atomic counter until the list is empty; the item runs the one-scan kernel's
+// body, so every voxel gets the same arithmetic as in a launch of its own.
+// Items are numbered scan by scan, CTA-grid order (x fastest) inside a scan.
+template <int EPI, bool FDK, int BU>
+__global__ void __launch_bounds__(kTX * kTY) bp_tma_multi_kernel(const BpScanRec* __restrict__ recs, int n_recs,
+                                                                 int total, int* __restrict__ counter) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  __shared__ uint64_t bars[2];
+  __shared__ int abort_flag;
+  __shared__ int item;
+  __shared__ int base[kMultiMaxRecs];
+  unsigned char* base_ptr =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  for (int i = threadIdx.x; i < n_recs; i += blockDim.x) base[i] = recs[i].base;
+  int next = 0, last = -1;
+#if CBCT_MULTI_MODE == 0
+  if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+#endif
+  for (;;) {
+#if CBCT_MULTI_MODE == 1
+    if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+#elif CBCT_MULTI_MODE == 2
+    if (threadIdx.x == 0) item = next == 0 ? blockIdx.x : total;
+#endif
+    __syncthreads();
+    const int t = item;
+    if (t >= total) break;
+#if CBCT_MULTI_MODE == 0
+    // The next item is claimed now; the atomic's round trip overlaps this one.
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+#elif CBCT_MULTI_MODE == 2
+    next = 1;
+#endif
+    const int lo = find_rec(base, n_recs, t);
+    const BpScanRec& R = recs[lo];
+    int l = t - base[lo];
+    const int bi = l % R.tx;
+    l /= R.tx;
+    const int bj = l % R.ty, bk = l / R.ty;
+    if (threadIdx.x == 0 && lo != last) {   // the thread that issues the TMA loads
+      tensormap_acquire(&R.map);
+      last = lo;
+    }
+    bp_tma_body<EPI, FDK, BU>(&R.map, R.views, R.n_views, R.gc, R.e, R.BV, R.flags, bi, bj, bk, base_ptr, bars,
+                              abort_flag);
+    __syncthreads();
+    // A wait that gave up is counted in the scan's flag word and its loads
+    // drained; only a CTA whose drain also gave up (a copy may still land in
+    // its shared memory) stops taking items.
+    const bool ok = abort_flag != 2;
+    if (threadIdx.x == 0) {
+      mbar_inval(&bars[0]);
+      mbar_inval(&bars[1]);
+#if CBCT_MULTI_MODE == 0
+      item = next;
+#endif
+    }
+    if (!ok) break;
+  }
+}
+
 size_t bp_tma_smem(const cbct_plan* p, int n_views) {
   const size_t stage = ((size_t)p->bp_box.bx * p->bp_box.by * 4 + 127) & ~size_t(127);
   return 128 + 2 * stage + (size_t)n_views * (sizeof(BpView) + 2 * sizeof(int2));
 }
 
-template <int EPI, bool FDK, int BU>
-void launch_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const BpEpi& e, cudaStream_t st) {
+// Tensor map of cnt projections (W x H, fp32) with the plan's detector box.
+CUtensorMap make_bp_map(const cbct_plan* p, const float* proj, int cnt) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
   cuuint64_t dims[3] = {(cuuint64_t)p->g.width, (cuuint64_t)p->g.height, (cuuint64_t)cnt};
   cuuint64_t strides[2] = {(cuuint64_t)p->g.width * 4, (cuuint64_t)p->g.width * p->g.height * 4};
-  cuuint32_t box[3] = {(cuuint32_t)BU, (cuuint32_t)p->bp_box.by, 1};
+  cuuint32_t box[3] = {(cuuint32_t)p->bp_box.bx, (cuuint32_t)p->bp_box.by, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult res = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(proj), dims,
                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (res != CUDA_SUCCESS) throw Error(CBCT_ERR_CUDA, "cuTensorMapEncodeTiled (projections) failed");
+  return m;
+}
+
+template <int EPI, bool FDK, int BU>
+void launch_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const BpEpi& e, cudaStream_t st) {
+  const CUtensorMap m = make_bp_map(p, proj, cnt);
   dim3 block(kTX * kTY);
   dim3 grid((p->g.nx + kTX - 1) / kTX, (p->g.ny + kTY - 1) / kTY, (p->g.nz + kZT - 1) / kZT);
   const size_t smem = bp_tma_smem(p, cnt);
@@ -518,6 +612,93 @@ void backproject_step_launch(cbct_plan* p, int s, const float* proj, const float
   e.aux = precon;
   e.scale = step;
   launch_bp<kStep, false>(p, s, proj, e, st);
+}
+
+namespace {
+
+// Work-list launch of one box width: records at A.dev + off.
+template <int EPI, int BU>
+void add_bp_group(WorkArena& A, const std::vector<BpScanRec>& recs, int total, size_t smem) {
+  auto k = bp_tma_multi_kernel<EPI, false, BU>;
+  ensure_smem_attr((const void*)k, smem);
+  const size_t off = A.add(recs.data(), recs.size() * sizeof(BpScanRec));
+  const int ci = A.n_counters++;
+  const int grid = CBCT_MULTI_MODE == 2 ? total : std::min(total, resident_grid((const void*)k, kTX * kTY, smem));
+  const int n = (int)recs.size();
+  A.ops.push_back([&A, k, off, ci, grid, n, total, smem](cudaStream_t st) {
+    k<<<grid, kTX * kTY, smem, st>>>(reinterpret_cast<const BpScanRec*>(A.dev + off), n, total, A.counter(ci));
+    check_launch("bp_tma_multi_kernel");
+  });
+}
+
+template <int EPI>
+void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
+  std::vector<BpScanRec> groups[5];
+  int totals[5] = {0, 0, 0, 0, 0};
+  size_t smem[5] = {0, 0, 0, 0, 0};
+  auto flush = [&](int c) {
+    if (groups[c].empty()) return;
+    switch (kBoxWidths[c]) {
+      case 40: add_bp_group<EPI, 40>(A, groups[c], totals[c], smem[c]); break;
+      case 56: add_bp_group<EPI, 56>(A, groups[c], totals[c], smem[c]); break;
+      case 72: add_bp_group<EPI, 72>(A, groups[c], totals[c], smem[c]); break;
+      case 104: add_bp_group<EPI, 104>(A, groups[c], totals[c], smem[c]); break;
+      case 136: add_bp_group<EPI, 136>(A, groups[c], totals[c], smem[c]); break;
+      default: throw Error(CBCT_ERR_INTERNAL, "unsupported back-projection box width");
+    }
+    groups[c].clear();
+    totals[c] = 0;
+    smem[c] = 0;
+  };
+  for (const MultiBpJob& j : jobs) {
+    cbct_plan* p = j.p;
+    BpEpi e{};
+    e.mask = p->d_mask;
+    e.vol = j.vol;
+    e.xold = j.xold;
+    e.aux = j.aux;
+    e.scale = j.step;
+    e.mom = j.mom;
+    e.nonneg = j.nonneg;
+    const int first = p->first[j.s], cnt = p->count[j.s];
+    if (cnt == 0) continue;
+    int w = -1;
+    for (int c = 0; c < 5; ++c)
+      if (kBoxWidths[c] == p->bp_box.bx) w = c;
+    const bool tma = p->bp_variant == 1 && cnt <= p->bp_max_views &&
+                     (reinterpret_cast<uintptr_t>(j.proj) % 16) == 0 && w >= 0;
+    if (!tma) {
+      const int s = j.s;
+      const float* proj = j.proj;
+      A.ops.push_back([p, s, proj, e](cudaStream_t st) { launch_bp<EPI, false>(p, s, proj, e, st); });
+      continue;
+    }
+    BpScanRec r;
+    std::memset(&r, 0, sizeof(r));
+    r.map = make_bp_map(p, j.proj, cnt);
+    r.views = p->d_views + first;
+    r.flags = p->d_flags;
+    r.gc = p->gc;
+    r.e = e;
+    r.n_views = cnt;
+    r.BV = p->bp_box.by;
+    r.tx = (p->g.nx + kTX - 1) / kTX;
+    r.ty = (p->g.ny + kTY - 1) / kTY;
+    const int tz = (p->g.nz + kZT - 1) / kZT;
+    if ((int)groups[w].size() == kMultiMaxRecs) flush(w);
+    r.base = totals[w];
+    totals[w] += r.tx * r.ty * tz;
+    smem[w] = std::max(smem[w], bp_tma_smem(p, cnt));
+    groups[w].push_back(r);
+  }
+  for (int c = 0; c < 5; ++c) flush(c);
+}
+
+}  // namespace
+
+void backproject_multi(WorkArena& A, int kind, const std::vector<MultiBpJob>& jobs) {
+  if (kind == 0) backproject_multi_t<kRecip>(A, jobs);
+  else backproject_multi_t<kMom>(A, jobs);
 }
 
 }  // namespace cbct

@@ -5,6 +5,8 @@
 #include <cudaTypedefs.h>
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
+#include <functional>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -378,6 +380,75 @@ void fdk_run(cbct_plan* p, const void* proj, float* vol, const float* filter, ui
 void osmom_precon(cbct_plan* p, float* D, cudaStream_t st);
 void osmom_step(cbct_plan* p, int s, cbct_dtype bt, const void* b, float* z, float* xold, const float* D, float* r,
                 float step, float mom, int nonneg, double* norm2, cudaStream_t st);
+
+// ---------------------------------------------------------- work-list launches
+// The fused batch solver (multi.cu) runs every step of many scans as one
+// launch per kernel kind whose CTAs work through a list of (scan, tile)
+// items.  A schedule is built on the host first: launch records go into
+// `host` (128-byte aligned, as the tensor maps inside them need), and `ops`
+// holds the work in order, each op issuing its launches on the stream it is
+// given and finding its records at `dev` + offset.  The records are then
+// uploaded once and the ops captured into one CUDA graph.  Every work-list
+// launch has its own item counter after the records; the first op zeroes them.
+struct WorkArena {
+  std::vector<unsigned char> host;
+  unsigned char* dev = nullptr;
+  int n_counters = 0;
+  std::vector<std::function<void(cudaStream_t)>> ops;
+  size_t add(const void* rec, size_t bytes) {
+    const size_t off = (host.size() + 127) & ~size_t(127);
+    host.resize(off + bytes);
+    std::memcpy(host.data() + off, rec, bytes);
+    return off;
+  }
+  size_t counters_offset() const { return (host.size() + 127) & ~size_t(127); }
+  int* counter(int i) const { return reinterpret_cast<int*>(dev + counters_offset()) + i; }
+  size_t bytes() const { return counters_offset() + sizeof(int) * (size_t)std::max(n_counters, 1); }
+};
+
+// Resident CTAs per SM of `func` at `threads` x `smem`, times the SMs: the
+// grid of a work-list launch.
+int resident_grid(const void* func, int threads, size_t smem);
+
+// One scan's part of a work-list forward residual launch: r_s = w (A_s vol - b_s),
+// the one-scan call forward_launch_ex(p, s, CBCT_F32, vol, out, b, NULL, 1, 1,
+// apply_offset, 0, norm2_out, st, b_dtype).
+struct MultiFwdJob {
+  cbct_plan* p;
+  int s;
+  const float* vol;
+  float* out;
+  const void* b;
+  cbct_dtype b_dtype;
+  int apply_offset;
+  double* norm2_out;
+};
+// Adds the launches of `jobs` to the schedule: the scans whose plans use the
+// TMA slab, row-pair or row-quad kernel are grouped by kernel and box width,
+// one work-list launch per group; the others get their one-scan launch.
+void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs);
+
+// One scan's part of a work-list back-projection over subset s of p:
+// kind 0 = preconditioner (vol = 1/max(A^T proj, 1e-6)), kind 1 = OS-MOM
+// update of (vol = z, xold) with precon aux, step, mom, nonneg.
+struct MultiBpJob {
+  cbct_plan* p;
+  int s;
+  const float* proj;
+  float* vol;
+  float* xold;
+  const float* aux;
+  float step, mom;
+  int nonneg;
+};
+void backproject_multi(WorkArena& A, int kind, const std::vector<MultiBpJob>& jobs);
+
+// multi.cu: the fused batch solver (cbct_batch_osmom_fused)
+void batch_osmom_fused(const cbct_batch_item* items, int n, cudaStream_t st);
+// solver.cu: the plan's solver workspace of at least `elems` floats (grown on
+// demand, kept), and a fill of n floats with v.
+float* solver_workspace(cbct_plan* p, size_t elems);
+void fill_launch(float* x, size_t n, float v, cudaStream_t st);
 
 // host helpers (abi.cu)
 void default_filter(int W, float* out);

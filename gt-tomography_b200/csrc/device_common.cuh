@@ -147,6 +147,40 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
+// Retires an mbarrier with no pending arrivals or copies, so that the CTA of
+// a work-list kernel may initialise it again for its next item.
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Scans per work-list launch (their first-item indices are kept in shared
+// memory by every CTA).
+constexpr int kMultiMaxRecs = 128;
+// Item assignment of the work-list kernels: 0 = resident CTAs, the next item
+// claimed from the counter while the current one runs; 1 = resident CTAs,
+// claimed when the current one is done; 2 = one CTA per item (no loop).
+#ifndef CBCT_MULTI_MODE
+#define CBCT_MULTI_MODE 0
+#endif
+
+// Index of the last entry of base[0..n) (ascending) that is <= t.
+__device__ __forceinline__ int find_rec(const int* base, int n, int t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Orders this thread's later TMA reads of a tensor map that sits in global
+// memory (written by a host copy before the launch) after its generic-proxy
+// contents.
+__device__ __forceinline__ void tensormap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(map) : "memory");
+}
+
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }

@@ -29,6 +29,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "device_common.cuh"
 
@@ -115,8 +116,25 @@ __device__ __forceinline__ double fwd_store(const FwdOut& o, const GridConst& gc
   return sq;
 }
 
+// Index of a CTA of a one-scan launch in launch order (x fastest).
+__device__ __forceinline__ size_t launch_block_id() {
+  return ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+}
+
+// Tile of one CTA: detector tile (x, y) of view z of the call, and its index
+// among the call's tiles in launch order (its partial-sum slot).
+struct TileId {
+  int x, y, z;
+  size_t bid;
+};
+
+__device__ __forceinline__ TileId launch_tile() {
+  return TileId{int(blockIdx.x), int(blockIdx.y), int(blockIdx.z), launch_block_id()};
+}
+
 // Deterministic block sum of sq; one partial per block in launch order.
-__device__ __forceinline__ void fwd_block_partial(const FwdOut& o, double sq, double* sh_red, int tid) {
+__device__ __forceinline__ void fwd_block_partial(const FwdOut& o, double sq, double* sh_red, int tid,
+                                                  size_t bid) {
   if (o.partials != nullptr) {
     double t = warp_sum(sq);
     const int w = tid >> 5, l = tid & 31;
@@ -125,10 +143,7 @@ __device__ __forceinline__ void fwd_block_partial(const FwdOut& o, double sq, do
     if (tid < 32) {
       double q = (l < (int)(blockDim.x * blockDim.y) / 32) ? sh_red[l] : 0.0;
       q = warp_sum(q);
-      if (tid == 0) {
-        const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        o.partials[bid] = q;
-      }
+      if (tid == 0) o.partials[bid] = q;
     }
   }
 }
@@ -136,9 +151,9 @@ __device__ __forceinline__ void fwd_block_partial(const FwdOut& o, double sq, do
 // Epilogue shared by the per-ray variants.  All threads of the block must call it.
 __device__ __forceinline__ void fwd_epilogue(const FwdOut& o, const GridConst& gc, const ViewParams& vp,
                                              int p, int u, int v, bool active, float val,
-                                             double* sh_red, int tid) {
+                                             double* sh_red, int tid, size_t bid) {
   const double sq = active ? fwd_store(o, gc, vp, p, u, v, val) : 0.0;
-  fwd_block_partial(o, sq, sh_red, tid);
+  fwd_block_partial(o, sq, sh_red, tid, bid);
 }
 
 // ------------------------------------------------------------------ gather
@@ -159,7 +174,7 @@ __global__ void __launch_bounds__(256) fwd_gather_kernel(const V* __restrict__ v
     int k0, k1;
     if (grown_range(vp, gc, u, v, r, k0, k1)) val = march_global(vol, gc, r, k0, k1) * r.delta;
   }
-  fwd_epilogue(o, gc, vp, p, u, v, active, val, sh_red, tid);
+  fwd_epilogue(o, gc, vp, p, u, v, active, val, sh_red, tid, launch_block_id());
 }
 
 // ------------------------------------------------------------------ transpose
@@ -274,24 +289,21 @@ __device__ __forceinline__ void slab_samples(const V* __restrict__ s, float& kf,
 template <class V>
 constexpr int slab_min_blocks() { return sizeof(V) == 4 ? 3 : 4; }
 
+// One CTA of the slab kernel: ray tile `tile` of the call.  Shared by the
+// one-scan kernel and the work-list kernel over many scans; smem_raw is the
+// 128-byte aligned dynamic shared memory (TMA destinations).
 template <class V, int BX, bool CHECK, int NS>
-__global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
-                                                       const __grid_constant__ CUtensorMap map_t,
-                                                       const V* __restrict__ vol,
-                                                       const ViewParams* __restrict__ views, GridConst gc,
-                                                       int BZ, FwdOut o, int* flags) {
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ SlabShared sh;
-  // TMA destinations are 128-byte aligned (128 extra bytes are requested).
-  unsigned char* smem_raw =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+__device__ __forceinline__ void fwd_slab_body(const CUtensorMap* map_v, const CUtensorMap* map_t,
+                                              const V* __restrict__ vol, const ViewParams* __restrict__ views,
+                                              const GridConst& gc, int BZ, const FwdOut& o, int* flags,
+                                              const TileId& tile, unsigned char* smem_raw, SlabShared& sh) {
   constexpr int BXY = BX * kBoxY;
-  const ViewParams vp = views[blockIdx.z];
+  const ViewParams vp = views[tile.z];
   const int dom = vp.dom;
-  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const CUtensorMap* map = dom ? map_v : map_t;
   const int tid = threadIdx.x;
-  const int p = blockIdx.z;
-  const int u0 = blockIdx.x * kTU, v0 = blockIdx.y * kTV;
+  const int p = tile.z;
+  const int u0 = tile.x * kTU, v0 = tile.y * kTV;
   const int u = u0 + (tid % kTU), v = v0 + (tid / kTU);
   const bool active = (u < gc.W) && (v < gc.H);
   const Ray r = make_ray(vp, gc, min(u, gc.W - 1), min(v, gc.H - 1));
@@ -424,7 +436,7 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
   if (sh.abort_flag && tid == 0) {
     // Drain loads still in flight (bounded) before the CTA exits.
     for (int i = done; i < min(done + NS, nslab); ++i)
-      (void)mbar_wait_bounded(&sh.bars[i % NS], (i / NS) & 1, kWaitLimit);
+      if (!mbar_wait_bounded(&sh.bars[i % NS], (i / NS) & 1, kWaitLimit)) sh.abort_flag = 2;
   }
   if (CHECK) {
     if (hit && kf != Nf) bad = 1;  // every sample of a hit ray must be consumed
@@ -438,7 +450,21 @@ __global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(con
     int k0, k1;
     if (grown_range(vp, gc, u, v, r, k0, k1)) val = march_global(vol, gc, r, k0, k1) * r.delta;
   }
-  fwd_epilogue(o, gc, vp, p, u, v, active, val, sh.red, tid);
+  fwd_epilogue(o, gc, vp, p, u, v, active, val, sh.red, tid, tile.bid);
+}
+
+template <class V, int BX, bool CHECK, int NS>
+__global__ void __launch_bounds__(256, slab_min_blocks<V>()) fwd_slab_kernel(const __grid_constant__ CUtensorMap map_v,
+                                                       const __grid_constant__ CUtensorMap map_t,
+                                                       const V* __restrict__ vol,
+                                                       const ViewParams* __restrict__ views, GridConst gc,
+                                                       int BZ, FwdOut o, int* flags) {
+  // TMA destinations are 128-byte aligned (128 extra bytes are requested).
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  __shared__ SlabShared sh;
+  fwd_slab_body<V, BX, CHECK, NS>(&map_v, &map_t, vol, views, gc, BZ, o, flags, launch_tile(), smem_raw, sh);
 }
 
 // ------------------------------------------------------------------ row pairs
@@ -554,22 +580,20 @@ constexpr int pair_min_blocks() {
 #endif
 }
 
+// One CTA of the row-pair kernel (see fwd_slab_body).
 template <class V, int BX, bool CHECK>
-__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
-    fwd_pair_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
-                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
-                    int nsl_max, FwdOut o, int* flags) {
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ PairShared sh;
-  unsigned char* smem_raw =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+__device__ __forceinline__ void fwd_pair_body(const CUtensorMap* map_v, const CUtensorMap* map_t,
+                                              const V* __restrict__ vol, const ViewParams* __restrict__ views,
+                                              const GridConst& gc, int BZ, int nsl_max, const FwdOut& o,
+                                              int* flags, const TileId& tile, unsigned char* smem_raw,
+                                              PairShared& sh) {
   constexpr int BXY = BX * kPairBoxY;
-  const ViewParams vp = views[blockIdx.z];
+  const ViewParams vp = views[tile.z];
   const int dom = vp.dom;
-  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const CUtensorMap* map = dom ? map_v : map_t;
   const int tid = threadIdx.x;
-  const int p = blockIdx.z;
-  const int u0 = blockIdx.x * kPU, v0 = blockIdx.y * kPV;
+  const int p = tile.z;
+  const int u0 = tile.x * kPU, v0 = tile.y * kPV;
   const int u = u0 + (tid % kPU), va = v0 + 2 * (tid / kPU), vb = va + 1;
   const bool act_a = (u < gc.W) && (va < gc.H), act_b = (u < gc.W) && (vb < gc.H);
   const int uc = min(u, gc.W - 1);
@@ -746,7 +770,7 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   }
   if (sh.abort_flag && tid == 0) {
     for (int i = done; i < min(done + kPairStages, nslab); ++i)
-      (void)mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit);
+      if (!mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit)) sh.abort_flag = 2;
   }
   if (CHECK) {
     // every sample of a hit ray must be consumed
@@ -767,7 +791,19 @@ __global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
   double sq = 0.0;
   if (act_a) sq += fwd_store(o, gc, vp, p, u, va, vala);
   if (act_b) sq += fwd_store(o, gc, vp, p, u, vb, valb);
-  fwd_block_partial(o, sq, sh.red, tid);
+  fwd_block_partial(o, sq, sh.red, tid, tile.bid);
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<V>())
+    fwd_pair_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
+                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
+                    int nsl_max, FwdOut o, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  __shared__ PairShared sh;
+  fwd_pair_body<V, BX, CHECK>(&map_v, &map_t, vol, views, gc, BZ, nsl_max, o, flags, launch_tile(), smem_raw, sh);
 }
 
 // ------------------------------------------------------------------ row quads
@@ -949,22 +985,20 @@ constexpr int quad_min_blocks() {
 #endif
 }
 
+// One CTA of the row-quad kernel (see fwd_slab_body).
 template <class V, int BX, bool CHECK>
-__global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
-    fwd_quad_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
-                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
-                    int nsl_max, FwdOut o, int* flags) {
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  __shared__ PairShared sh;
-  unsigned char* smem_raw =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+__device__ __forceinline__ void fwd_quad_body(const CUtensorMap* map_v, const CUtensorMap* map_t,
+                                              const V* __restrict__ vol, const ViewParams* __restrict__ views,
+                                              const GridConst& gc, int BZ, int nsl_max, const FwdOut& o,
+                                              int* flags, const TileId& tile, unsigned char* smem_raw,
+                                              PairShared& sh) {
   constexpr int BXY = BX * kQuadBoxY;
-  const ViewParams vp = views[blockIdx.z];
+  const ViewParams vp = views[tile.z];
   const int dom = vp.dom;
-  const CUtensorMap* map = dom ? &map_v : &map_t;
+  const CUtensorMap* map = dom ? map_v : map_t;
   const int tid = threadIdx.x;
-  const int p = blockIdx.z;
-  const int u0 = blockIdx.x * kQU, v0 = blockIdx.y * kQV;
+  const int p = tile.z;
+  const int u0 = tile.x * kQU, v0 = tile.y * kQV;
   const int u = u0 + (tid % kQU), vq = v0 + 4 * (tid / kQU);
   const int uc = min(u, gc.W - 1);
   const float Nf = float(gc.N);
@@ -1139,7 +1173,7 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
   }
   if (sh.abort_flag && tid == 0) {
     for (int i = done; i < min(done + kPairStages, nslab); ++i)
-      (void)mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit);
+      if (!mbar_wait_bounded(&sh.bars[i % kPairStages], (i / kPairStages) & 1, kWaitLimit)) sh.abort_flag = 2;
   }
   if (CHECK) {
     // every sample of a hit ray must be consumed
@@ -1169,7 +1203,19 @@ __global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
       val = march_global(vol, gc, r[i], k0, k1) * r[i].delta;
     if (act[i]) sq += fwd_store(o, gc, vp, p, u, vq + i, val);
   }
-  fwd_block_partial(o, sq, sh.red, tid);
+  fwd_block_partial(o, sq, sh.red, tid, tile.bid);
+}
+
+template <class V, int BX, bool CHECK>
+__global__ void __launch_bounds__(kQuadThreads, quad_min_blocks<V>())
+    fwd_quad_kernel(const __grid_constant__ CUtensorMap map_v, const __grid_constant__ CUtensorMap map_t,
+                    const V* __restrict__ vol, const ViewParams* __restrict__ views, GridConst gc, int BZ,
+                    int nsl_max, FwdOut o, int* flags) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  __shared__ PairShared sh;
+  fwd_quad_body<V, BX, CHECK>(&map_v, &map_t, vol, views, gc, BZ, nsl_max, o, flags, launch_tile(), smem_raw, sh);
 }
 
 // ------------------------------------------------------------------ fan
@@ -1458,7 +1504,7 @@ __global__ void __launch_bounds__(256, 3) fwd_fan_kernel(const __grid_constant__
   __syncthreads();
   const int tu = tid % kFU, tv = tid / kFU;
   const int eu = u0 + tu, ev = v0 + tv;
-  fwd_epilogue(o, gc, vp, p, eu, ev, eu < gc.W && ev < gc.H, sh.tile[tv][tu], sh.red, tid);
+  fwd_epilogue(o, gc, vp, p, eu, ev, eu < gc.W && ev < gc.H, sh.tile[tv][tu], sh.red, tid, launch_block_id());
 }
 
 // ------------------------------------------------------------------ host
@@ -1467,6 +1513,104 @@ CUtensorMapDataType tma_dtype(cbct_dtype dt) {
     case CBCT_F32: return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     case CBCT_F16: return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     default: return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  }
+}
+
+// ------------------------------------------------------------------ work list
+// Work-list (persistent) forward projector over many scans: resident CTAs
+// take items -- one ray tile of one view of one scan -- from an atomic counter
+// until the list is empty and run the one-scan kernel's body on them, so every
+// ray gets the arithmetic of its own launch.  A scan's items are numbered in
+// its one-scan launch order (x fastest), which is also its partial-sum slot.
+enum { kVarSlab1 = 0, kVarSlab2 = 1, kVarPair = 2, kVarQuad = 3 };
+
+struct alignas(128) FwdScanRec {
+  CUtensorMap map_v, map_t;    // volume and x/y-transposed volume, the plan's box
+  const void* vol;
+  const ViewParams* views;     // the subset's views
+  int* flags;
+  GridConst gc;
+  FwdOut o;
+  int BZ, nsl_max;
+  int tx, ty;                  // ray tiles per view (x, y)
+  int base;                    // work-list index of the scan's first tile
+};
+
+template <int VAR>
+constexpr int var_threads() { return VAR == kVarPair ? kPairThreads : VAR == kVarQuad ? kQuadThreads : 256; }
+template <int VAR, class V>
+constexpr int var_min_blocks() {
+  return VAR == kVarPair ? pair_min_blocks<V>() : VAR == kVarQuad ? quad_min_blocks<V>() : slab_min_blocks<V>();
+}
+
+template <int VAR, class V, int BX>
+__global__ void __launch_bounds__(var_threads<VAR>(), var_min_blocks<VAR, V>())
+    fwd_multi_kernel(const FwdScanRec* __restrict__ recs, int n_recs, int total, int* __restrict__ counter) {
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  using Shared = typename std::conditional<VAR <= kVarSlab2, SlabShared, PairShared>::type;
+  __shared__ Shared sh;
+  __shared__ int item;
+  __shared__ int base[kMultiMaxRecs];
+  constexpr int kBars = VAR == kVarSlab1 ? 1 : VAR == kVarSlab2 ? 2 : kPairStages;
+  for (int i = threadIdx.x; i < n_recs; i += blockDim.x) base[i] = recs[i].base;
+  int next = 0, last = -1;
+#if CBCT_MULTI_MODE == 0
+  if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+#endif
+  for (;;) {
+#if CBCT_MULTI_MODE == 1
+    if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+#elif CBCT_MULTI_MODE == 2
+    if (threadIdx.x == 0) item = next == 0 ? blockIdx.x : total;
+#endif
+    __syncthreads();
+    const int t = item;
+    if (t >= total) break;
+#if CBCT_MULTI_MODE == 0
+    // The next item is claimed now; the atomic's round trip overlaps this one.
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+#elif CBCT_MULTI_MODE == 2
+    next = 1;
+#endif
+    const int lo = find_rec(base, n_recs, t);
+    const FwdScanRec& R = recs[lo];
+    int l = t - base[lo];
+    TileId tile;
+    tile.bid = (size_t)l;
+    tile.x = l % R.tx;
+    l /= R.tx;
+    tile.y = l % R.ty;
+    tile.z = l / R.ty;
+    if (threadIdx.x == 0 && lo != last) {   // the thread that issues the TMA loads
+      tensormap_acquire(&R.map_v);
+      tensormap_acquire(&R.map_t);
+      last = lo;
+    }
+    const V* vol = static_cast<const V*>(R.vol);
+    if constexpr (VAR == kVarSlab1)
+      fwd_slab_body<V, BX, false, 1>(&R.map_v, &R.map_t, vol, R.views, R.gc, R.BZ, R.o, R.flags, tile, smem_raw, sh);
+    else if constexpr (VAR == kVarSlab2)
+      fwd_slab_body<V, BX, false, 2>(&R.map_v, &R.map_t, vol, R.views, R.gc, R.BZ, R.o, R.flags, tile, smem_raw, sh);
+    else if constexpr (VAR == kVarPair)
+      fwd_pair_body<V, BX, false>(&R.map_v, &R.map_t, vol, R.views, R.gc, R.BZ, R.nsl_max, R.o, R.flags, tile,
+                                  smem_raw, sh);
+    else
+      fwd_quad_body<V, BX, false>(&R.map_v, &R.map_t, vol, R.views, R.gc, R.BZ, R.nsl_max, R.o, R.flags, tile,
+                                  smem_raw, sh);
+    __syncthreads();
+    // A wait that gave up is counted in the scan's flag word and its loads
+    // drained; only a CTA whose drain also gave up (a copy may still land in
+    // its shared memory) stops taking items.
+    const bool ok = sh.abort_flag != 2;
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < kBars; ++i) mbar_inval(&sh.bars[i]);
+#if CBCT_MULTI_MODE == 0
+      item = next;
+#endif
+    }
+    if (!ok) break;
   }
 }
 
@@ -1507,6 +1651,19 @@ static size_t pair_smem(const SlabBox& b, size_t es, int nsl) {
 template <class V>
 const SlabBox& box_for(const cbct_plan* p) { return sizeof(V) == 4 ? p->slab : p->slab16; }
 
+// Two stages while they leave the register-bound number of CTAs per SM;
+// boxes so large that they would not (small volumes under detectors of about
+// one pixel per voxel) stage one slab at a time, and the other CTAs' samples
+// cover each CTA's wait.  Returns the stages and sets the dynamic shared memory.
+template <class V>
+int slab_stages(const SlabBox& b, size_t& smem) {
+  const size_t stage = (b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127);
+  const size_t per_cta = sizeof(SlabShared) + 1024 + 128;
+  const bool two = (2 * stage + per_cta) * slab_min_blocks<V>() <= size_t(228) * 1024;
+  smem = (two ? 2 : 1) * stage + 128;
+  return two ? 2 : 1;
+}
+
 template <class V, int BX>
 void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim3 grid, int first,
                  cudaStream_t st, cbct_dtype dt) {
@@ -1514,14 +1671,8 @@ void launch_slab(cbct_plan* p, const V* vol, const V* volT, const FwdOut& o, dim
   const CUtensorMap mv = make_map(dt, vol, p->g.nx, p->g.ny, p->g.nz, b);
   const CUtensorMap mt = make_map(dt, volT ? (const void*)volT : (const void*)vol, volT ? p->g.ny : p->g.nx,
                                   volT ? p->g.nx : p->g.ny, p->g.nz, b);
-  // Two stages while they leave the register-bound number of CTAs per SM;
-  // boxes so large that they would not (small volumes under detectors of
-  // about one pixel per voxel) stage one slab at a time, and the other CTAs'
-  // samples cover each CTA's wait.
-  const size_t stage = (b.bx * b.by * b.bz * sizeof(V) + 127) & ~size_t(127);
-  const size_t per_cta = sizeof(SlabShared) + 1024 + 128;
-  const bool two = (2 * stage + per_cta) * slab_min_blocks<V>() <= size_t(228) * 1024;
-  const size_t smem = (two ? 2 : 1) * stage + 128;
+  size_t smem = 0;
+  const bool two = slab_stages<V>(b, smem) == 2;
   auto pick = [&](auto k2, auto k1) { return two ? k2 : k1; };
   auto k = p->debug_checks ? pick(fwd_slab_kernel<V, BX, true, 2>, fwd_slab_kernel<V, BX, true, 1>)
                            : pick(fwd_slab_kernel<V, BX, false, 2>, fwd_slab_kernel<V, BX, false, 1>);
@@ -1969,6 +2120,139 @@ void forward_launch_ex(cbct_plan* p, int s, cbct_dtype dt, const void* vol, floa
     default: throw Error(CBCT_ERR_INVALID_ARGUMENT, "unknown volume dtype");
   }
   if (norm2_out) finalize_partials(p->d_partials, (int)nblocks, norm2_out, st);
+}
+
+namespace {
+
+template <int VAR, int BX>
+void add_fwd_group(WorkArena& A, const std::vector<FwdScanRec>& recs, int total, size_t smem) {
+  auto k = fwd_multi_kernel<VAR, float, BX>;
+  ensure_smem_attr((const void*)k, smem);
+  const size_t off = A.add(recs.data(), recs.size() * sizeof(FwdScanRec));
+  const int ci = A.n_counters++;
+  const int threads = var_threads<VAR>();
+  const int grid = CBCT_MULTI_MODE == 2 ? total : std::min(total, resident_grid((const void*)k, threads, smem));
+  const int n = (int)recs.size();
+  A.ops.push_back([&A, k, off, ci, grid, threads, n, total, smem](cudaStream_t st) {
+    k<<<grid, threads, smem, st>>>(reinterpret_cast<const FwdScanRec*>(A.dev + off), n, total, A.counter(ci));
+    check_launch("fwd_multi_kernel");
+  });
+}
+
+template <int VAR>
+void add_fwd_group_w(WorkArena& A, int c, const std::vector<FwdScanRec>& g, int total, size_t smem) {
+  switch (kBoxWidths[c]) {
+    case 40: add_fwd_group<VAR, 40>(A, g, total, smem); break;
+    case 56: add_fwd_group<VAR, 56>(A, g, total, smem); break;
+    case 72: add_fwd_group<VAR, 72>(A, g, total, smem); break;
+    case 104: add_fwd_group<VAR, 104>(A, g, total, smem); break;
+    case 136: add_fwd_group<VAR, 136>(A, g, total, smem); break;
+    default: throw Error(CBCT_ERR_INTERNAL, "unsupported forward box width");
+  }
+}
+
+}  // namespace
+
+void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
+  std::vector<FwdScanRec> groups[4][5];
+  int totals[4][5] = {};
+  size_t smem[4][5] = {};
+  auto flush = [&](int v, int c) {
+    if (groups[v][c].empty()) return;
+    if (v == kVarSlab1) add_fwd_group_w<kVarSlab1>(A, c, groups[v][c], totals[v][c], smem[v][c]);
+    else if (v == kVarSlab2) add_fwd_group_w<kVarSlab2>(A, c, groups[v][c], totals[v][c], smem[v][c]);
+    else if (v == kVarPair) add_fwd_group_w<kVarPair>(A, c, groups[v][c], totals[v][c], smem[v][c]);
+    else add_fwd_group_w<kVarQuad>(A, c, groups[v][c], totals[v][c], smem[v][c]);
+    groups[v][c].clear();
+    totals[v][c] = 0;
+    smem[v][c] = 0;
+  };
+  std::vector<std::function<void(cudaStream_t)>> after;
+  for (const MultiFwdJob& j : jobs) {
+    cbct_plan* p = j.p;
+    const int s = j.s, first = p->first[s], cnt = p->count[s];
+    if (cnt == 0) continue;
+    const bool tma = p->fwd_variant >= 1 && ((size_t)p->g.nx * 4) % 16 == 0 && ((size_t)p->g.ny * 4) % 16 == 0 &&
+                     (reinterpret_cast<uintptr_t>(j.vol) % 16 == 0) && (!p->subset_has_xdom[s] || p->d_volT);
+    const int fv = p->fwd_variant;
+    if (!tma || fv == 2 || p->debug_checks) {
+      const MultiFwdJob jj = j;
+      A.ops.push_back([jj](cudaStream_t st) {
+        forward_launch_ex(jj.p, jj.s, CBCT_F32, jj.vol, jj.out, jj.b, nullptr, 1.f, kModeResidual, jj.apply_offset,
+                          0, jj.norm2_out, st, jj.b_dtype);
+      });
+      continue;
+    }
+    const float* volT = nullptr;
+    if (p->subset_has_xdom[s]) {
+      float* t = static_cast<float*>(p->d_volT);
+      const float* vol = j.vol;
+      const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz;
+      A.ops.push_back([vol, t, nx, ny, nz](cudaStream_t st) {
+        dim3 tg((nx + 31) / 32, (ny + 31) / 32, nz);
+        transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, st>>>(vol, t, nx, ny);
+        check_launch("transpose_xy_kernel");
+      });
+      volT = t;
+    }
+    FwdOut o{};
+    o.out = j.out;
+    o.b = j.b;
+    o.b_dtype = j.b_dtype;
+    o.pw = nullptr;
+    o.scale = 1.f;
+    o.mode = kModeResidual;
+    o.apply_offset = j.apply_offset;
+    o.accumulate = 0;
+    o.partials = nullptr;
+    o.wproj = p->d_pweights ? p->d_pweights + (size_t)p->g.width * p->g.height * first : nullptr;
+    const int nsl = slabs_max(p->g);
+    int var, TU, TV;
+    SlabBox b;
+    size_t sm = 0;
+    if (fv == 4) {
+      b = p->quad; var = kVarQuad; TU = kQU; TV = kQV; sm = pair_smem(b, 4, nsl);
+    } else if (fv == 3) {
+      b = p->pair; var = kVarPair; TU = kPU; TV = kPV; sm = pair_smem(b, 4, nsl);
+    } else {
+      b = p->slab; TU = kTU; TV = kTV;
+      var = slab_stages<float>(b, sm) == 2 ? kVarSlab2 : kVarSlab1;
+    }
+    int w = -1;
+    for (int c = 0; c < 5; ++c)
+      if (kBoxWidths[c] == b.bx) w = c;
+    if (w < 0) throw Error(CBCT_ERR_INTERNAL, "unsupported forward box width");
+    FwdScanRec r;
+    std::memset(&r, 0, sizeof(r));
+    r.map_v = make_map(CBCT_F32, j.vol, p->g.nx, p->g.ny, p->g.nz, b);
+    r.map_t = make_map(CBCT_F32, volT ? (const void*)volT : (const void*)j.vol, volT ? p->g.ny : p->g.nx,
+                       volT ? p->g.nx : p->g.ny, p->g.nz, b);
+    r.vol = j.vol;
+    r.views = p->d_views + first;
+    r.flags = p->d_flags;
+    r.gc = p->gc;
+    r.BZ = b.bz;
+    r.nsl_max = nsl;
+    r.tx = (p->g.width + TU - 1) / TU;
+    r.ty = (p->g.height + TV - 1) / TV;
+    const int nblocks = r.tx * r.ty * cnt;
+    if (j.norm2_out) {
+      if ((size_t)nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");
+      o.partials = p->d_partials;
+      double* part = p->d_partials;
+      double* out = j.norm2_out;
+      after.push_back([part, nblocks, out](cudaStream_t st) { finalize_partials(part, nblocks, out, st); });
+    }
+    r.o = o;
+    if ((int)groups[var][w].size() == kMultiMaxRecs) flush(var, w);
+    r.base = totals[var][w];
+    totals[var][w] += nblocks;
+    smem[var][w] = std::max(smem[var][w], sm);
+    groups[var][w].push_back(r);
+  }
+  for (int v = 0; v < 4; ++v)
+    for (int c = 0; c < 5; ++c) flush(v, c);
+  for (auto& f : after) A.ops.push_back(std::move(f));
 }
 
 }  // namespace cbct

@@ -215,6 +215,8 @@ static float* workspace(cbct_plan* p, size_t elems) {
   return p->ws;
 }
 
+float* solver_workspace(cbct_plan* p, size_t elems) { return workspace(p, elems); }
+
 static void run_osmom(cbct_plan* p, const void* b, const float* x0, float* z, const cbct_solver_params& prm,
                       double* resid, float* xold, float* D, float* r, void* shadow, cudaStream_t st) {
   const cbct_dtype bt = prm.proj_storage;

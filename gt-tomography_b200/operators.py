@@ -461,13 +461,17 @@ def osmom_update(z, xold, precon, g, step, mom, nonneg=False, stream=None):
            int(nonneg), _stream(stream))
 
 
-def batch_osmom(jobs, n_streams=8, stream=None):
+def batch_osmom(jobs, n_streams=8, stream=None, fused=False):
     """Solves independent OS-MOM problems concurrently (cbct_batch_osmom).
 
     jobs: sequence of dicts with keys plan, b, z (outputs) and optionally x0,
     iterations, beta, gamma, nonneg, storage, refine_every, resid.  Each result
     is bitwise identical to solving that job alone.  Starts after the work on
-    the current stream and returns when every job has finished."""
+    the current stream and returns when every job has finished.
+
+    fused=True advances the jobs in lockstep through persistent work-list
+    launches captured in one graph (cbct_batch_osmom_fused; fp32 volume
+    storage); n_streams is then unused."""
     items = (L.CbctBatchItem * len(jobs))()
     for i, j in enumerate(jobs):
         prm = L.CbctSolverParams(int(j.get("iterations", 10)), float(j.get("beta", 1.0)), float(j.get("gamma", 0.0)),
@@ -476,7 +480,10 @@ def batch_osmom(jobs, n_streams=8, stream=None):
                                  _storage_of(j["b"], j["plan"].proj_shape(-1), "b"))
         items[i] = L.CbctBatchItem(j["plan"].handle.value, _ptr(j["b"]), _ptr(j.get("x0")), _ptr(j["z"]), prm,
                                    _ptr(j.get("resid")))
-    L.call("cbct_batch_osmom", items, len(jobs), int(n_streams), _stream(stream))
+    if fused:
+        L.call("cbct_batch_osmom_fused", items, len(jobs), _stream(stream))
+    else:
+        L.call("cbct_batch_osmom", items, len(jobs), int(n_streams), _stream(stream))
 
 
 def tv_step(x, P, s, D, scale, tau, tau_lambda, stream=None):

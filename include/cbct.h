@@ -460,6 +460,20 @@ typedef struct {
  * No counterpart in the reference (its drivers reconstruct one scan per process). */
 CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream);
 
+/* The same reconstructions advanced in lockstep through work-list launches:
+ * step k runs subset k mod S_i of iteration k / S_i of every item that has
+ * one.  A step is one persistent forward launch per projector kind and box
+ * width and one persistent back-projection (OS-MOM update fused) per box width
+ * over all those items; resident CTAs take (scan, tile) items from a counter
+ * until the list is empty.  The whole schedule, preconditioner included, is
+ * captured and replayed as one CUDA graph.  Items may differ in volume,
+ * detector, views, subsets and iterations.  Each result is bitwise identical
+ * to cbct_osmom_solve of the item alone.  Requires params.storage = CBCT_F32,
+ * no bins and no regulariser (CBCT_ERR_UNSUPPORTED otherwise).  Items must not
+ * share plans or outputs; ordering as cbct_batch_osmom.
+ * No counterpart in the reference. */
+CBCT_API cbct_status cbct_batch_osmom_fused(const cbct_batch_item* items, int32_t n, void* stream);
+
 /* ----------------------------------------------------------------------------
  * Host-array operators streamed in batches of views
  *

@@ -38,6 +38,14 @@ def test_status_strings(gtb):
     assert lib.cbct_status_string(0) == b"CBCT_OK"
     assert lib.cbct_status_string(1) == b"CBCT_ERR_INVALID_ARGUMENT"
     assert b"sm_100a" in lib.cbct_version()
+    # the binding's status constants are the header's enum
+    txt = open(os.path.join(ROOT, "include", "cbct.h")).read()
+    enum = dict((k, int(v)) for k, v in re.findall(r"\b(CBCT_(?:OK|ERR_\w+))\s*=\s*(\d+)", txt))
+    assert len(enum) == 10
+    for k, v in enum.items():
+        if k != "CBCT_OK":
+            assert getattr(gtb._lib, k) == v, k
+        assert lib.cbct_status_string(v) == k.encode()
 
 
 def test_subset_partition_matches_oracle(gtb, O):

@@ -4,6 +4,7 @@
 // thread-local message; nothing throws across the boundary.  Host-side setup
 // logic restates the reference's operator setup (cited per function).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -234,7 +235,9 @@ cbct_plan* plan_create(const cbct_geometry* g, const float* angles, const float*
   CBCT_REQUIRE(angles && offsets, "angles/offsets are NULL");
   CBCT_REQUIRE(n_subsets >= 1, "n_subsets must be >= 1");
   CBCT_REQUIRE(n_subsets == 1 || subset_sizes, "subset_sizes is NULL with several subsets");
+  static std::atomic<uint64_t> serials{0};
   std::unique_ptr<cbct_plan, void (*)(cbct_plan*)> p(new cbct_plan(), plan_free);
+  p->serial = ++serials;
   p->g = *g;
   p->gc = make_grid(*g);
   p->n_views = n_views;

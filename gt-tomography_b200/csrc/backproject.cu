@@ -349,26 +349,14 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_multi_kernel(const BpScanRec
   unsigned char* base_ptr =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
   for (int i = threadIdx.x; i < n_recs; i += blockDim.x) base[i] = recs[i].base;
-  int next = 0, last = -1;
-#if CBCT_MULTI_MODE == 0
-  if (threadIdx.x == 0) item = atomicAdd(counter, 1);
-#endif
+  int last = -1;
   for (;;) {
-#if CBCT_MULTI_MODE == 1
     if (threadIdx.x == 0) item = atomicAdd(counter, 1);
-#elif CBCT_MULTI_MODE == 2
-    if (threadIdx.x == 0) item = next == 0 ? blockIdx.x : total;
-#endif
     __syncthreads();
     const int t = item;
     if (t >= total) break;
-#if CBCT_MULTI_MODE == 0
-    // The next item is claimed now; the atomic's round trip overlaps this one.
-    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
-#elif CBCT_MULTI_MODE == 2
-    next = 1;
-#endif
-    const int lo = find_rec(base, n_recs, t);
+    // Broadcast: the compiler may then keep the record's fields uniform.
+    const int lo = __shfl_sync(0xffffffffu, find_rec(base, n_recs, t), 0);
     const BpScanRec& R = recs[lo];
     int l = t - base[lo];
     const int bi = l % R.tx;
@@ -388,9 +376,6 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_multi_kernel(const BpScanRec
     if (threadIdx.x == 0) {
       mbar_inval(&bars[0]);
       mbar_inval(&bars[1]);
-#if CBCT_MULTI_MODE == 0
-      item = next;
-#endif
     }
     if (!ok) break;
   }
@@ -623,12 +608,24 @@ void add_bp_group(WorkArena& A, const std::vector<BpScanRec>& recs, int total, s
   ensure_smem_attr((const void*)k, smem);
   const size_t off = A.add(recs.data(), recs.size() * sizeof(BpScanRec));
   const int ci = A.n_counters++;
-  const int grid = CBCT_MULTI_MODE == 2 ? total : std::min(total, resident_grid((const void*)k, kTX * kTY, smem));
+  const int grid = std::min(total, resident_grid((const void*)k, kTX * kTY, smem));
   const int n = (int)recs.size();
   A.ops.push_back([&A, k, off, ci, grid, n, total, smem](cudaStream_t st) {
     k<<<grid, kTX * kTY, smem, st>>>(reinterpret_cast<const BpScanRec*>(A.dev + off), n, total, A.counter(ci));
     check_launch("bp_tma_multi_kernel");
   });
+}
+
+template <int EPI>
+const void* bp_multi_ptr(int c) {
+  switch (kBoxWidths[c]) {
+    case 40: return (const void*)bp_tma_multi_kernel<EPI, false, 40>;
+    case 56: return (const void*)bp_tma_multi_kernel<EPI, false, 56>;
+    case 72: return (const void*)bp_tma_multi_kernel<EPI, false, 72>;
+    case 104: return (const void*)bp_tma_multi_kernel<EPI, false, 104>;
+    case 136: return (const void*)bp_tma_multi_kernel<EPI, false, 136>;
+    default: throw Error(CBCT_ERR_INTERNAL, "unsupported back-projection box width");
+  }
 }
 
 template <int EPI>
@@ -667,7 +664,15 @@ void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
       if (kBoxWidths[c] == p->bp_box.bx) w = c;
     const bool tma = p->bp_variant == 1 && cnt <= p->bp_max_views &&
                      (reinterpret_cast<uintptr_t>(j.proj) % 16) == 0 && w >= 0;
-    if (!tma) {
+    const int tx = (p->g.nx + kTX - 1) / kTX, ty = (p->g.ny + kTY - 1) / kTY, tz = (p->g.nz + kZT - 1) / kZT;
+    bool own = !tma;
+    if (tma) {
+      const void* kfn = bp_multi_ptr<EPI>(w);
+      const size_t sm = bp_tma_smem(p, cnt);
+      ensure_smem_attr(kfn, sm);
+      own = tx * ty * tz >= kMultiFillWaves * resident_grid(kfn, kTX * kTY, sm);
+    }
+    if (own) {
       const int s = j.s;
       const float* proj = j.proj;
       A.ops.push_back([p, s, proj, e](cudaStream_t st) { launch_bp<EPI, false>(p, s, proj, e, st); });
@@ -682,9 +687,8 @@ void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
     r.e = e;
     r.n_views = cnt;
     r.BV = p->bp_box.by;
-    r.tx = (p->g.nx + kTX - 1) / kTX;
-    r.ty = (p->g.ny + kTY - 1) / kTY;
-    const int tz = (p->g.nz + kZT - 1) / kZT;
+    r.tx = tx;
+    r.ty = ty;
     if ((int)groups[w].size() == kMultiMaxRecs) flush(w);
     r.base = totals[w];
     totals[w] += r.tx * r.ty * tz;

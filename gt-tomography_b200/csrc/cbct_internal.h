@@ -250,6 +250,11 @@ struct cbct_plan {
   float* ws = nullptr;
   size_t ws_elems = 0;
 
+  // Identity for caches that outlive one call: serial is unique per plan in
+  // the process; generation grows with every change of the plan's state
+  // (options, mask, bins, weights, autotuning: every graph_cache_free).
+  uint64_t serial = 0, generation = 0;
+
   int debug_checks = 0;
   int force_gather = 0;
   int status_check = 1;     // CBCT_OPT_STATUS_CHECK: solve/FDK entry points read the flag words on return
@@ -407,8 +412,19 @@ struct WorkArena {
 };
 
 // Resident CTAs per SM of `func` at `threads` x `smem`, times the SMs: the
-// grid of a work-list launch.
+// grid of a work-list launch (cached per kernel and size).
 int resident_grid(const void* func, int threads, size_t smem);
+
+// A scan whose own launch would fill the GPU for this many waves of resident
+// CTAs keeps its one-scan launch in the fused schedule: its last partial wave
+// is a small share of it, and the one-scan kernel reads its arguments from the
+// constant bank instead of holding a work-list record's fields in registers
+// (measured: the work-list kernels run 2-7 % slower per item; at 4 waves a
+// partial last wave costs more, at 16 less).
+#ifndef CBCT_MULTI_FILL_WAVES
+#define CBCT_MULTI_FILL_WAVES 16
+#endif
+constexpr int kMultiFillWaves = CBCT_MULTI_FILL_WAVES;
 
 // One scan's part of a work-list forward residual launch: r_s = w (A_s vol - b_s),
 // the one-scan call forward_launch_ex(p, s, CBCT_F32, vol, out, b, NULL, 1, 1,

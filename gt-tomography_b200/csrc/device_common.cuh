@@ -155,13 +155,7 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
 
 // Scans per work-list launch (their first-item indices are kept in shared
 // memory by every CTA).
-constexpr int kMultiMaxRecs = 128;
-// Item assignment of the work-list kernels: 0 = resident CTAs, the next item
-// claimed from the counter while the current one runs; 1 = resident CTAs,
-// claimed when the current one is done; 2 = one CTA per item (no loop).
-#ifndef CBCT_MULTI_MODE
-#define CBCT_MULTI_MODE 0
-#endif
+constexpr int kMultiMaxRecs = 64;
 
 // Index of the last entry of base[0..n) (ascending) that is <= t.
 __device__ __forceinline__ int find_rec(const int* base, int n, int t) {

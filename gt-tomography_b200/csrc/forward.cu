@@ -180,12 +180,12 @@ __global__ void __launch_bounds__(256) fwd_gather_kernel(const V* __restrict__ v
 // ------------------------------------------------------------------ transpose
 // volT[k][i][j] = vol[k][j][i]: the volume seen with x and y exchanged.
 template <class V>
-__global__ void transpose_xy_kernel(const V* __restrict__ in, V* __restrict__ out, int nx, int ny) {
-  __shared__ V tile[32][33];
+__device__ __forceinline__ void transpose_tile(const V* __restrict__ in, V* __restrict__ out, int nx, int ny, int bx,
+                                               int by, int bz, V (&tile)[32][33]) {
   const size_t plane = (size_t)nx * ny;
-  const V* src = in + blockIdx.z * plane;
-  V* dst = out + blockIdx.z * plane;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const V* src = in + bz * plane;
+  V* dst = out + bz * plane;
+  const int x0 = bx * 32, y0 = by * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int x = x0 + threadIdx.x, y = y0 + j;
     if (x < nx && y < ny) tile[j][threadIdx.x] = src[(size_t)y * nx + x];
@@ -195,6 +195,38 @@ __global__ void transpose_xy_kernel(const V* __restrict__ in, V* __restrict__ ou
     const int y = y0 + threadIdx.x, x = x0 + j;
     if (x < nx && y < ny) dst[(size_t)x * ny + y] = tile[threadIdx.x][j];
   }
+}
+
+template <class V>
+__global__ void transpose_xy_kernel(const V* __restrict__ in, V* __restrict__ out, int nx, int ny) {
+  __shared__ V tile[32][33];
+  transpose_tile<V>(in, out, nx, ny, blockIdx.x, blockIdx.y, blockIdx.z, tile);
+}
+
+// x/y transposes of many scans' volumes in one launch: one CTA per 32x32 tile
+// of one plane of one scan, scans numbered in order.
+struct TransposeRec {
+  const float* in;
+  float* out;
+  int nx, ny;
+  int tx, ty;            // tiles per plane (x, y)
+  int base;              // index of the scan's first CTA
+};
+
+__global__ void transpose_multi_kernel(const TransposeRec* __restrict__ recs, int n_recs) {
+  __shared__ float tile[32][33];
+  int lo = 0, hi = n_recs - 1;
+  const int t = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (recs[mid].base <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const TransposeRec& R = recs[lo];
+  int l = t - R.base;
+  const int bx = l % R.tx;
+  l /= R.tx;
+  transpose_tile<float>(R.in, R.out, R.nx, R.ny, bx, l % R.ty, l / R.ty, tile);
 }
 
 // ------------------------------------------------------------------ slab/TMA
@@ -1555,26 +1587,14 @@ __global__ void __launch_bounds__(var_threads<VAR>(), var_min_blocks<VAR, V>())
   __shared__ int base[kMultiMaxRecs];
   constexpr int kBars = VAR == kVarSlab1 ? 1 : VAR == kVarSlab2 ? 2 : kPairStages;
   for (int i = threadIdx.x; i < n_recs; i += blockDim.x) base[i] = recs[i].base;
-  int next = 0, last = -1;
-#if CBCT_MULTI_MODE == 0
-  if (threadIdx.x == 0) item = atomicAdd(counter, 1);
-#endif
+  int last = -1;
   for (;;) {
-#if CBCT_MULTI_MODE == 1
     if (threadIdx.x == 0) item = atomicAdd(counter, 1);
-#elif CBCT_MULTI_MODE == 2
-    if (threadIdx.x == 0) item = next == 0 ? blockIdx.x : total;
-#endif
     __syncthreads();
     const int t = item;
     if (t >= total) break;
-#if CBCT_MULTI_MODE == 0
-    // The next item is claimed now; the atomic's round trip overlaps this one.
-    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
-#elif CBCT_MULTI_MODE == 2
-    next = 1;
-#endif
-    const int lo = find_rec(base, n_recs, t);
+    // Broadcast: the compiler may then keep the record's fields uniform.
+    const int lo = __shfl_sync(0xffffffffu, find_rec(base, n_recs, t), 0);
     const FwdScanRec& R = recs[lo];
     int l = t - base[lo];
     TileId tile;
@@ -1606,9 +1626,6 @@ __global__ void __launch_bounds__(var_threads<VAR>(), var_min_blocks<VAR, V>())
     const bool ok = sh.abort_flag != 2;
     if (threadIdx.x == 0) {
       for (int i = 0; i < kBars; ++i) mbar_inval(&sh.bars[i]);
-#if CBCT_MULTI_MODE == 0
-      item = next;
-#endif
     }
     if (!ok) break;
   }
@@ -2131,12 +2148,33 @@ void add_fwd_group(WorkArena& A, const std::vector<FwdScanRec>& recs, int total,
   const size_t off = A.add(recs.data(), recs.size() * sizeof(FwdScanRec));
   const int ci = A.n_counters++;
   const int threads = var_threads<VAR>();
-  const int grid = CBCT_MULTI_MODE == 2 ? total : std::min(total, resident_grid((const void*)k, threads, smem));
+  const int grid = std::min(total, resident_grid((const void*)k, threads, smem));
   const int n = (int)recs.size();
   A.ops.push_back([&A, k, off, ci, grid, threads, n, total, smem](cudaStream_t st) {
     k<<<grid, threads, smem, st>>>(reinterpret_cast<const FwdScanRec*>(A.dev + off), n, total, A.counter(ci));
     check_launch("fwd_multi_kernel");
   });
+}
+
+template <int VAR>
+const void* fwd_multi_ptr_v(int c) {
+  switch (kBoxWidths[c]) {
+    case 40: return (const void*)fwd_multi_kernel<VAR, float, 40>;
+    case 56: return (const void*)fwd_multi_kernel<VAR, float, 56>;
+    case 72: return (const void*)fwd_multi_kernel<VAR, float, 72>;
+    case 104: return (const void*)fwd_multi_kernel<VAR, float, 104>;
+    case 136: return (const void*)fwd_multi_kernel<VAR, float, 136>;
+    default: throw Error(CBCT_ERR_INTERNAL, "unsupported forward box width");
+  }
+}
+
+const void* fwd_multi_ptr(int var, int c) {
+  return var == kVarSlab1 ? fwd_multi_ptr_v<kVarSlab1>(c) : var == kVarSlab2 ? fwd_multi_ptr_v<kVarSlab2>(c)
+         : var == kVarPair ? fwd_multi_ptr_v<kVarPair>(c) : fwd_multi_ptr_v<kVarQuad>(c);
+}
+
+int var_threads_of(int var) {
+  return var == kVarPair ? var_threads<kVarPair>() : var == kVarQuad ? var_threads<kVarQuad>() : 256;
 }
 
 template <int VAR>
@@ -2157,8 +2195,23 @@ void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
   std::vector<FwdScanRec> groups[4][5];
   int totals[4][5] = {};
   size_t smem[4][5] = {};
+  // Transposes of the volumes the next launches read, one launch for all.
+  std::vector<TransposeRec> tr;
+  int tr_total = 0;
+  auto flush_transposes = [&]() {
+    if (tr.empty()) return;
+    const size_t off = A.add(tr.data(), tr.size() * sizeof(TransposeRec));
+    const int n = (int)tr.size(), total = tr_total;
+    A.ops.push_back([&A, off, n, total](cudaStream_t st) {
+      transpose_multi_kernel<<<total, dim3(32, 8), 0, st>>>(reinterpret_cast<const TransposeRec*>(A.dev + off), n);
+      check_launch("transpose_multi_kernel");
+    });
+    tr.clear();
+    tr_total = 0;
+  };
   auto flush = [&](int v, int c) {
     if (groups[v][c].empty()) return;
+    flush_transposes();
     if (v == kVarSlab1) add_fwd_group_w<kVarSlab1>(A, c, groups[v][c], totals[v][c], smem[v][c]);
     else if (v == kVarSlab2) add_fwd_group_w<kVarSlab2>(A, c, groups[v][c], totals[v][c], smem[v][c]);
     else if (v == kVarPair) add_fwd_group_w<kVarPair>(A, c, groups[v][c], totals[v][c], smem[v][c]);
@@ -2175,37 +2228,16 @@ void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
     const bool tma = p->fwd_variant >= 1 && ((size_t)p->g.nx * 4) % 16 == 0 && ((size_t)p->g.ny * 4) % 16 == 0 &&
                      (reinterpret_cast<uintptr_t>(j.vol) % 16 == 0) && (!p->subset_has_xdom[s] || p->d_volT);
     const int fv = p->fwd_variant;
-    if (!tma || fv == 2 || p->debug_checks) {
-      const MultiFwdJob jj = j;
+    auto one_scan = [&A](const MultiFwdJob& jj) {
       A.ops.push_back([jj](cudaStream_t st) {
         forward_launch_ex(jj.p, jj.s, CBCT_F32, jj.vol, jj.out, jj.b, nullptr, 1.f, kModeResidual, jj.apply_offset,
                           0, jj.norm2_out, st, jj.b_dtype);
       });
+    };
+    if (!tma || fv == 2 || p->debug_checks) {
+      one_scan(j);
       continue;
     }
-    const float* volT = nullptr;
-    if (p->subset_has_xdom[s]) {
-      float* t = static_cast<float*>(p->d_volT);
-      const float* vol = j.vol;
-      const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz;
-      A.ops.push_back([vol, t, nx, ny, nz](cudaStream_t st) {
-        dim3 tg((nx + 31) / 32, (ny + 31) / 32, nz);
-        transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, st>>>(vol, t, nx, ny);
-        check_launch("transpose_xy_kernel");
-      });
-      volT = t;
-    }
-    FwdOut o{};
-    o.out = j.out;
-    o.b = j.b;
-    o.b_dtype = j.b_dtype;
-    o.pw = nullptr;
-    o.scale = 1.f;
-    o.mode = kModeResidual;
-    o.apply_offset = j.apply_offset;
-    o.accumulate = 0;
-    o.partials = nullptr;
-    o.wproj = p->d_pweights ? p->d_pweights + (size_t)p->g.width * p->g.height * first : nullptr;
     const int nsl = slabs_max(p->g);
     int var, TU, TV;
     SlabBox b;
@@ -2222,6 +2254,36 @@ void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
     for (int c = 0; c < 5; ++c)
       if (kBoxWidths[c] == b.bx) w = c;
     if (w < 0) throw Error(CBCT_ERR_INTERNAL, "unsupported forward box width");
+    const int tx = (p->g.width + TU - 1) / TU, ty = (p->g.height + TV - 1) / TV;
+    const int nblocks = tx * ty * cnt;
+    {
+      const void* kfn = fwd_multi_ptr(var, w);
+      ensure_smem_attr(kfn, sm);
+      if (nblocks >= kMultiFillWaves * resident_grid(kfn, var_threads_of(var), sm)) {
+        one_scan(j);
+        continue;
+      }
+    }
+    const float* volT = nullptr;
+    if (p->subset_has_xdom[s]) {
+      float* t = static_cast<float*>(p->d_volT);
+      if ((int)tr.size() == kMultiMaxRecs) flush_transposes();
+      TransposeRec q{j.vol, t, p->g.nx, p->g.ny, (p->g.nx + 31) / 32, (p->g.ny + 31) / 32, tr_total};
+      tr_total += q.tx * q.ty * p->g.nz;
+      tr.push_back(q);
+      volT = t;
+    }
+    FwdOut o{};
+    o.out = j.out;
+    o.b = j.b;
+    o.b_dtype = j.b_dtype;
+    o.pw = nullptr;
+    o.scale = 1.f;
+    o.mode = kModeResidual;
+    o.apply_offset = j.apply_offset;
+    o.accumulate = 0;
+    o.partials = nullptr;
+    o.wproj = p->d_pweights ? p->d_pweights + (size_t)p->g.width * p->g.height * first : nullptr;
     FwdScanRec r;
     std::memset(&r, 0, sizeof(r));
     r.map_v = make_map(CBCT_F32, j.vol, p->g.nx, p->g.ny, p->g.nz, b);
@@ -2233,9 +2295,8 @@ void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
     r.gc = p->gc;
     r.BZ = b.bz;
     r.nsl_max = nsl;
-    r.tx = (p->g.width + TU - 1) / TU;
-    r.ty = (p->g.height + TV - 1) / TV;
-    const int nblocks = r.tx * r.ty * cnt;
+    r.tx = tx;
+    r.ty = ty;
     if (j.norm2_out) {
       if ((size_t)nblocks > p->n_partials) throw Error(CBCT_ERR_INTERNAL, "partials buffer too small");
       o.partials = p->d_partials;
@@ -2252,6 +2313,7 @@ void forward_multi(WorkArena& A, const std::vector<MultiFwdJob>& jobs) {
   }
   for (int v = 0; v < 4; ++v)
     for (int c = 0; c < 5; ++c) flush(v, c);
+  flush_transposes();
   for (auto& f : after) A.ops.push_back(std::move(f));
 }
 

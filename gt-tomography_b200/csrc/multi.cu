@@ -11,7 +11,11 @@
 // captured in one CUDA graph.  Each CTA item runs the one-scan kernels' body,
 // so every result is bitwise the one-scan solve's.
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 #ifdef CBCT_SETUP_TIMING
 #include <chrono>
@@ -23,11 +27,22 @@
 namespace cbct {
 
 int resident_grid(const void* func, int threads, size_t smem) {
-  int dev = 0, sms = 0, nb = 0;
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+  int dev = 0;
   CBCT_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, func, threads, smem);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int sms = 0, nb = 0;
   CBCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   CBCT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, func, threads, smem));
   if (nb < 1) throw Error(CBCT_ERR_INTERNAL, "work-list kernel does not fit an SM");
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = nb * sms;
   return nb * sms;
 }
 
@@ -42,8 +57,12 @@ struct ItemState {
   double t = 1.0, told = 1.0;
 };
 
-// Device memory and graph of one fused run, released on every exit path.
+// Records and instantiated graph of one fused schedule, released on every
+// exit path.  The last one is kept and replayed when the next call has the
+// same key: the same plans in the same states (serial, generation, device
+// buffers) with the same arrays and parameters.
 struct FusedRun {
+  std::vector<uint64_t> key;
   unsigned char* dev = nullptr;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
@@ -55,6 +74,17 @@ struct FusedRun {
     if (dev) cudaFree(dev);
   }
 };
+
+std::mutex g_fused_mu;
+std::unique_ptr<FusedRun> g_fused_last;
+
+uint64_t bits_of(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uint64_t>&& key);
 
 }  // namespace
 
@@ -91,6 +121,46 @@ void batch_osmom_fused(const cbct_batch_item* items, int n, cudaStream_t st) {
     S.push_back(s);
   }
 
+  int device = 0;
+  CBCT_CUDA(cudaGetDevice(&device));
+  std::vector<uint64_t> key = {(uint64_t)device, (uint64_t)n};
+  for (const ItemState& s : S) {
+    const cbct_plan* p = s.p;
+    const cbct_solver_params& prm = s.it->params;
+    for (uint64_t v : {p->serial, p->generation, (uint64_t)s.it->b, (uint64_t)s.it->x0, (uint64_t)s.it->z_out,
+                       (uint64_t)s.it->resid_norm2_out, (uint64_t)prm.iterations, bits_of(prm.beta),
+                       bits_of(prm.gamma), (uint64_t)prm.non_negativity, (uint64_t)prm.proj_storage,
+                       (uint64_t)s.xold, (uint64_t)p->d_volT, (uint64_t)p->d_partials, (uint64_t)p->d_flags,
+                       (uint64_t)p->d_views, (uint64_t)p->d_mask, (uint64_t)p->d_pweights})
+      key.push_back(v);
+  }
+  std::lock_guard<std::mutex> lock(g_fused_mu);
+  if (!g_fused_last || g_fused_last->key != key) {
+    g_fused_last.reset();
+    g_fused_last = build_fused(S, std::move(key));
+  }
+  CBCT_CUDA(cudaGraphLaunch(g_fused_last->exec, st));
+  CBCT_CUDA(cudaStreamSynchronize(st));
+  // Device-side status of every item; the first failing item's is returned.
+  std::string first_msg;
+  cbct_status first = CBCT_OK;
+  for (int i = 0; i < n; ++i) {
+    try {
+      plan_check_flags(items[i].plan, st);
+    } catch (const Error& e) {
+      if (first == CBCT_OK) {
+        first = e.status;
+        first_msg = "batch item " + std::to_string(i) + ": " + e.what();
+      }
+    }
+  }
+  if (first != CBCT_OK) throw Error(first, first_msg);
+}
+
+namespace {
+
+// The fused schedule of the items, captured and instantiated.
+std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uint64_t>&& key) {
 #ifdef CBCT_SETUP_TIMING
   const auto t0 = std::chrono::steady_clock::now();
 #endif
@@ -165,45 +235,30 @@ void batch_osmom_fused(const cbct_batch_item* items, int n, cudaStream_t st) {
   auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
   const auto t1 = now();
 #endif
-  FusedRun run;
-  CBCT_CUDA(cudaMalloc(&run.dev, A.bytes()));
-  A.dev = run.dev;
-  if (!A.host.empty()) CBCT_CUDA(cudaMemcpy(run.dev, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
-  CBCT_CUDA(cudaStreamCreateWithFlags(&run.cap, cudaStreamNonBlocking));
-  CBCT_CUDA(cudaStreamBeginCapture(run.cap, cudaStreamCaptureModeThreadLocal));
+  auto run = std::make_unique<FusedRun>();
+  run->key = std::move(key);
+  CBCT_CUDA(cudaMalloc(&run->dev, A.bytes()));
+  A.dev = run->dev;
+  if (!A.host.empty()) CBCT_CUDA(cudaMemcpy(run->dev, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
+  CBCT_CUDA(cudaStreamCreateWithFlags(&run->cap, cudaStreamNonBlocking));
+  CBCT_CUDA(cudaStreamBeginCapture(run->cap, cudaStreamCaptureModeThreadLocal));
   try {
-    for (auto& op : A.ops) op(run.cap);
+    for (auto& op : A.ops) op(run->cap);
   } catch (...) {
-    cudaStreamEndCapture(run.cap, &run.graph);
+    cudaStreamEndCapture(run->cap, &run->graph);
     throw;
   }
-  CBCT_CUDA(cudaStreamEndCapture(run.cap, &run.graph));
-  CBCT_CUDA(cudaGraphInstantiate(&run.exec, run.graph, 0));
-#ifdef CBCT_SETUP_TIMING
-  const auto t2 = now();
-#endif
-  CBCT_CUDA(cudaGraphLaunch(run.exec, st));
-  CBCT_CUDA(cudaStreamSynchronize(st));
+  CBCT_CUDA(cudaStreamEndCapture(run->cap, &run->graph));
+  CBCT_CUDA(cudaGraphInstantiate(&run->exec, run->graph, 0));
 #ifdef CBCT_SETUP_TIMING
   size_t nodes = 0;
-  cudaGraphGetNodes(run.graph, nullptr, &nodes);
-  std::fprintf(stderr, "fused: schedule %.1f ms, upload+capture+instantiate %.1f ms (%zu nodes, %zu record bytes), "
-               "run %.1f ms\n", ms(t0, t1), ms(t1, t2), nodes, A.host.size(), ms(t2, now()));
+  cudaGraphGetNodes(run->graph, nullptr, &nodes);
+  std::fprintf(stderr, "fused: schedule %.1f ms, upload+capture+instantiate %.1f ms (%zu nodes, %zu record bytes)\n",
+               ms(t0, t1), ms(t1, now()), nodes, A.host.size());
 #endif
-  // Device-side status of every item; the first failing item's is returned.
-  std::string first_msg;
-  cbct_status first = CBCT_OK;
-  for (int i = 0; i < n; ++i) {
-    try {
-      plan_check_flags(items[i].plan, st);
-    } catch (const Error& e) {
-      if (first == CBCT_OK) {
-        first = e.status;
-        first_msg = "batch item " + std::to_string(i) + ": " + e.what();
-      }
-    }
-  }
-  if (first != CBCT_OK) throw Error(first, first_msg);
+  return run;
 }
+
+}  // namespace
 
 }  // namespace cbct

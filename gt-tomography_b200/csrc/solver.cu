@@ -467,6 +467,7 @@ struct GraphCache {
 };
 
 void graph_cache_free(cbct_plan* p) {
+  ++p->generation;
   GraphCache* g = static_cast<GraphCache*>(p->graph_cache);
   if (!g) return;
   if (g->exec) cudaGraphExecDestroy(g->exec);

@@ -124,7 +124,7 @@ def test_fused_rejects(gtb, cuda):
 
 def test_fused_splits_large_groups(gtb, cuda):
     """More scans of one kernel and box width than one work-list launch holds
-    (128): the group is split over several launches, results unchanged."""
+    (64): the group is split over several launches, results unchanged."""
     import torch
     sp = gtb.phantom.uneven_scans(1, seed0=701, vol_range=(32, 32), z_range=(24, 24), view_range=(24, 24),
                                   width_range=(40, 40))[0]
@@ -139,3 +139,52 @@ def test_fused_splits_large_groups(gtb, cuda):
     gtb.batch_osmom([dict(plan=p, b=b, z=z, iterations=2, nonneg=True) for p, z in zip(plans, zs)], fused=True)
     for z in zs:
         assert torch.equal(z, ref)
+
+
+def test_fused_mixes_filling_and_small_scans(gtb, cuda):
+    """A scan whose forward launches fill the GPU for several waves keeps its
+    one-scan launches inside the fused graph; the small scans beside it go
+    through the work lists.  Both results are bitwise the solves alone."""
+    import torch
+    big = dict(seed=811, n=(128, 128, 96), P=144, W=256, H=192, pitch=1.2 * 1.5 * 128 / 256)
+    small = gtb.phantom.uneven_scans(2, seed0=812, vol_range=(32, 48), z_range=(24, 32), view_range=(20, 30),
+                                     width_range=(40, 56))
+    for sp in small:
+        sp["pitch"] *= 1.6
+    scans = [gtb.phantom.make_osmom_scan(sp, 2, 1e5, cuda) for sp in [big] + small]
+    refs, outs = [], []
+    for plan, b, _ in scans:
+        r = torch.empty(plan.vol_shape, dtype=torch.float32, device=cuda)
+        plan.osmom(b, r, None, 2, nonneg=True)
+        refs.append(r)
+        outs.append(torch.empty_like(r))
+    gtb.batch_osmom([dict(plan=s[0], b=s[1], z=z, iterations=2, nonneg=True) for s, z in zip(scans, outs)],
+                    fused=True)
+    for r, z in zip(refs, outs):
+        assert torch.equal(r, z)
+
+
+def test_fused_graph_is_reused_and_rebuilt_on_plan_change(gtb, cuda):
+    """The last fused schedule is replayed for an identical call, and rebuilt
+    when a plan changes state (here: a voxel mask set between the calls)."""
+    import torch
+    scans = _scans(gtb, cuda, 3, 901)
+    outs = [torch.empty(s[2].vol_shape, dtype=torch.float32, device=cuda) for s in scans]
+    jobs = [dict(plan=s[2], b=s[3], z=z, iterations=2, nonneg=True) for s, z in zip(scans, outs)]
+    gtb.batch_osmom(jobs, fused=True)
+    first = [z.clone() for z in outs]
+    for z in outs:
+        z.fill_(-1.0)
+    gtb.batch_osmom(jobs, fused=True)            # replayed
+    for a, z in zip(first, outs):
+        assert torch.equal(a, z)
+    plan = scans[1][2]
+    mask = torch.ones(plan.vol_shape, dtype=torch.uint8, device=cuda)
+    mask[:, :, : plan.vol_shape[2] // 2] = 0
+    plan.set_mask(mask)
+    gtb.batch_osmom(jobs, fused=True)            # rebuilt: the mask applies
+    ref = torch.empty_like(outs[1])
+    plan.osmom(scans[1][3], ref, None, 2, nonneg=True)
+    assert torch.equal(outs[1], ref)
+    assert not torch.equal(outs[1], first[1])
+    assert torch.equal(outs[0], first[0]) and torch.equal(outs[2], first[2])

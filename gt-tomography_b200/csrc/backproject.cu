@@ -23,6 +23,8 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
+#include <utility>
 
 #include "device_common.cuh"
 
@@ -165,6 +167,32 @@ constexpr int kTX = 16, kTY = 8;     // columns per CTA of the TMA back-projecto
 struct BpView {
   float cs, sn, ox, oy;
 };
+
+// Detector box widths (u, fp32 elements) the TMA back-projector is compiled
+// for; a plan takes the smallest that holds its footprints.  Rows of a box
+// sit BU floats apart, so BU mod 32 is the bank offset between the two rows a
+// bilinear tap reads.
+#ifdef CBCT_BP_WIDTHS_16
+constexpr int kBpWidths[] = {48, 80, 112, 144};      // row offset 16 banks
+#else
+constexpr int kBpWidths[] = {40, 56, 72, 104, 136};  // row offset 8 or 24 banks
+#endif
+constexpr int kNBpWidths = int(sizeof(kBpWidths) / sizeof(int));
+
+// Calls f(std::integral_constant<int, W>) for the compiled width W == w;
+// false when w is not one of them.
+template <int I = 0, class F>
+bool with_bp_width(int w, F&& f) {
+  if constexpr (I < kNBpWidths) {
+    if (w == kBpWidths[I]) {
+      f(std::integral_constant<int, kBpWidths[I]>{});
+      return true;
+    }
+    return with_bp_width<I + 1>(w, std::forward<F>(f));
+  } else {
+    return false;
+  }
+}
 
 // One CTA's work: the kTX x kTY x kZT voxel block (bi, bj, bk) over the views
 // of the call.  Shared by the one-scan kernel (block = blockIdx) and the
@@ -416,14 +444,9 @@ void launch_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const Bp
 template <int EPI, bool FDK>
 bool try_bp_tma(cbct_plan* p, int first, int cnt, const float* proj, const BpEpi& e, cudaStream_t st) {
   if (p->bp_variant != 1 || cnt > p->bp_max_views || (reinterpret_cast<uintptr_t>(proj) % 16) != 0) return false;
-  switch (p->bp_box.bx) {
-    case 40: launch_bp_tma<EPI, FDK, 40>(p, first, cnt, proj, e, st); return true;
-    case 56: launch_bp_tma<EPI, FDK, 56>(p, first, cnt, proj, e, st); return true;
-    case 72: launch_bp_tma<EPI, FDK, 72>(p, first, cnt, proj, e, st); return true;
-    case 104: launch_bp_tma<EPI, FDK, 104>(p, first, cnt, proj, e, st); return true;
-    case 136: launch_bp_tma<EPI, FDK, 136>(p, first, cnt, proj, e, st); return true;
-    default: return false;
-  }
+  return with_bp_width(p->bp_box.bx, [&](auto W) {
+    launch_bp_tma<EPI, FDK, decltype(W)::value>(p, first, cnt, proj, e, st);
+  });
 }
 
 template <int EPI, bool FDK, int BU>
@@ -515,7 +538,7 @@ void backproject_choose_variant(cbct_plan* p) {
     ev = std::max(ev, a.second);
   }
   int w = 0;
-  for (int c : kBoxWidths)
+  for (int c : kBpWidths)
     if (c >= eu + 3) { w = c; break; }
   if (w == 0 || ev > 256) return;
   p->bp_box = SlabBox{w, std::max(ev, 2), 1, 1};
@@ -528,14 +551,7 @@ void backproject_choose_variant(cbct_plan* p) {
 void backproject_prepare(cbct_plan* p) {
   if (p->bp_variant == 1) {
     const size_t sm = bp_tma_smem(p, p->bp_max_views);
-    switch (p->bp_box.bx) {
-      case 40: prepare_bp_all<40>(sm); break;
-      case 56: prepare_bp_all<56>(sm); break;
-      case 72: prepare_bp_all<72>(sm); break;
-      case 104: prepare_bp_all<104>(sm); break;
-      case 136: prepare_bp_all<136>(sm); break;
-      default: break;
-    }
+    with_bp_width(p->bp_box.bx, [&](auto W) { prepare_bp_all<decltype(W)::value>(sm); });
   }
   const size_t smem = sizeof(ViewParams) * (size_t)std::min(p->n_views, kMaxViewsSmem);
   ensure_smem_attr((const void*)bp_kernel<kStore, false>, smem);
@@ -618,31 +634,19 @@ void add_bp_group(WorkArena& A, const std::vector<BpScanRec>& recs, int total, s
 
 template <int EPI>
 const void* bp_multi_ptr(int c) {
-  switch (kBoxWidths[c]) {
-    case 40: return (const void*)bp_tma_multi_kernel<EPI, false, 40>;
-    case 56: return (const void*)bp_tma_multi_kernel<EPI, false, 56>;
-    case 72: return (const void*)bp_tma_multi_kernel<EPI, false, 72>;
-    case 104: return (const void*)bp_tma_multi_kernel<EPI, false, 104>;
-    case 136: return (const void*)bp_tma_multi_kernel<EPI, false, 136>;
-    default: throw Error(CBCT_ERR_INTERNAL, "unsupported back-projection box width");
-  }
+  const void* k = nullptr;
+  with_bp_width(kBpWidths[c], [&](auto W) { k = (const void*)bp_tma_multi_kernel<EPI, false, decltype(W)::value>; });
+  return k;
 }
 
 template <int EPI>
 void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
-  std::vector<BpScanRec> groups[5];
-  int totals[5] = {0, 0, 0, 0, 0};
-  size_t smem[5] = {0, 0, 0, 0, 0};
+  std::vector<BpScanRec> groups[kNBpWidths];
+  int totals[kNBpWidths] = {};
+  size_t smem[kNBpWidths] = {};
   auto flush = [&](int c) {
     if (groups[c].empty()) return;
-    switch (kBoxWidths[c]) {
-      case 40: add_bp_group<EPI, 40>(A, groups[c], totals[c], smem[c]); break;
-      case 56: add_bp_group<EPI, 56>(A, groups[c], totals[c], smem[c]); break;
-      case 72: add_bp_group<EPI, 72>(A, groups[c], totals[c], smem[c]); break;
-      case 104: add_bp_group<EPI, 104>(A, groups[c], totals[c], smem[c]); break;
-      case 136: add_bp_group<EPI, 136>(A, groups[c], totals[c], smem[c]); break;
-      default: throw Error(CBCT_ERR_INTERNAL, "unsupported back-projection box width");
-    }
+    with_bp_width(kBpWidths[c], [&](auto W) { add_bp_group<EPI, decltype(W)::value>(A, groups[c], totals[c], smem[c]); });
     groups[c].clear();
     totals[c] = 0;
     smem[c] = 0;
@@ -660,8 +664,8 @@ void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
     const int first = p->first[j.s], cnt = p->count[j.s];
     if (cnt == 0) continue;
     int w = -1;
-    for (int c = 0; c < 5; ++c)
-      if (kBoxWidths[c] == p->bp_box.bx) w = c;
+    for (int c = 0; c < kNBpWidths; ++c)
+      if (kBpWidths[c] == p->bp_box.bx) w = c;
     const bool tma = p->bp_variant == 1 && cnt <= p->bp_max_views &&
                      (reinterpret_cast<uintptr_t>(j.proj) % 16) == 0 && w >= 0;
     const int tx = (p->g.nx + kTX - 1) / kTX, ty = (p->g.ny + kTY - 1) / kTY, tz = (p->g.nz + kZT - 1) / kZT;
@@ -695,7 +699,7 @@ void backproject_multi_t(WorkArena& A, const std::vector<MultiBpJob>& jobs) {
     smem[w] = std::max(smem[w], bp_tma_smem(p, cnt));
     groups[w].push_back(r);
   }
-  for (int c = 0; c < 5; ++c) flush(c);
+  for (int c = 0; c < kNBpWidths; ++c) flush(c);
 }
 
 }  // namespace

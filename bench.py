@@ -666,16 +666,29 @@ def batched(args):
     print(json.dumps(batched_line(args)), flush=True)
 
 
+# Scan sets of the batched configuration: uneven_scans ranges and first seed.
+SCAN_SETS = {
+    "c4": dict(seed0=1000),
+    "small": dict(seed0=3000, vol_range=(64, 128), z_range=(64, 128), view_range=(60, 180), width_range=(128, 256)),
+    "medium": dict(seed0=3000, vol_range=(96, 160), z_range=(96, 160), view_range=(90, 360),
+                   width_range=(256, 384)),
+    "tiny": dict(seed0=3000, vol_range=(32, 64), z_range=(32, 64), view_range=(40, 120), width_range=(64, 128)),
+}
+
+
 def batched_line(args):
     """Batched reconstruction of many uneven scans (the north star's fourth
     configuration): 64 seeded scans, volumes 96..320 (z 64..320), 90..720
     views, detectors 256x192..768x576, I0 = 1e5, OS-MOM with 8 subsets x 10
     iterations, fp32.  A step solves every scan once.  Reports recon/s of the
-    batched executor and of the same solves run one scan at a time."""
+    batch executors (stream pool, fused work lists) and of the same solves run
+    one scan at a time.  --scan-sizes picks a set of smaller scans instead,
+    --executor one executor alone, --iterations the OS-MOM iterations."""
     import torch
     dev = torch.device("cuda", 0)
     gtb = _package()
-    specs = gtb.phantom.uneven_scans(args.scans, seed0=1000)
+    it = args.iterations
+    specs = gtb.phantom.uneven_scans(args.scans, **SCAN_SETS[args.scan_sizes])
     scans = [gtb.phantom.make_osmom_scan(sp, 8, 1e5, dev) for sp in specs]
     variants = {}
     if args.autotune:
@@ -686,17 +699,17 @@ def batched_line(args):
                    else "bp-global")
             variants["+".join(key)] = variants.get("+".join(key), 0) + 1
     zs = [torch.empty(pl.vol_shape, dtype=torch.float32, device=dev) for pl, _, _ in scans]
-    jobs = [dict(plan=pl, b=b, z=z, iterations=10, nonneg=True) for (pl, b, _), z in zip(scans, zs)]
+    jobs = [dict(plan=pl, b=b, z=z, iterations=it, nonneg=True) for (pl, b, _), z in zip(scans, zs)]
     stream = torch.cuda.current_stream()
     updates = 0
     for sp in specs:
         nvox = sp["n"][0] * sp["n"][1] * sp["n"][2]
         N = int(np.float32(1.5) * np.float32(sp["n"][0]))
-        updates += 11 * (sp["W"] * sp["H"] * sp["P"] * N + nvox * sp["P"])
+        updates += (it + 1) * (sp["W"] * sp["H"] * sp["P"] * N + nvox * sp["P"])
 
     def one_at_a_time():
         for j in jobs:
-            j["plan"].osmom(j["b"], j["z"], None, 10, nonneg=True, use_graph=True)
+            j["plan"].osmom(j["b"], j["z"], None, it, nonneg=True, use_graph=True)
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -707,20 +720,26 @@ def batched_line(args):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    for _ in range(max(args.warmup, 1)):
-        one_at_a_time()
+    run_pool, run_fused, run_seq = (args.executor in ("both", "pool"), args.executor in ("both", "fused"),
+                                    args.executor == "both")
+
+    def pool():
         gtb.batch_osmom(jobs, n_streams=args.streams)
+
+    def fused():
         gtb.batch_osmom(jobs, fused=True)
+
+    for _ in range(max(args.warmup, 1)):
+        for run, fn in ((run_seq, one_at_a_time), (run_pool, pool), (run_fused, fused)):
+            if run:
+                fn()
     clocks = ClockSampler(0)
     clocks.start()
-    t_pool = [timed(lambda: gtb.batch_osmom(jobs, n_streams=args.streams)) for _ in range(args.steps)]
-    t_fused = [timed(lambda: gtb.batch_osmom(jobs, fused=True)) for _ in range(args.steps)]
-    t_seq = [timed(one_at_a_time) for _ in range(args.steps)]
+    mean = lambda fn, run: sum(timed(fn) for _ in range(args.steps)) / args.steps if run else None
+    ms_p, ms_f, ms_s = mean(pool, run_pool), mean(fused, run_fused), mean(one_at_a_time, run_seq)
     clk = clocks.stop()
-    ms_p, ms_f, ms_s = (sum(t) / len(t) for t in (t_pool, t_fused, t_seq))
     # The headline is the faster executor; both are reported.
-    executor = "fused work-list" if ms_f <= ms_p else "stream pool"
-    ms_b = min(ms_p, ms_f)
+    ms_b, executor = min((t, name) for t, name in ((ms_f, "fused work-list"), (ms_p, "stream pool")) if t is not None)
     plain = None
     if args.plain_sample > 0:
         # The plain FP32 one-scan-at-a-time path (reference structure) on an
@@ -739,34 +758,40 @@ def batched_line(args):
             ocv = np.ascontiguousarray(oc, np.int32)
             zp = torch.empty_like(zs[i])
             L.call("cbct_plain_osmom_solve", C.byref(pl.g), aa.ctypes.data, oo.ctypes.data, aa.size, sz.ctypes.data,
-                   len(sz), ocv.ctypes.data, b.data_ptr(), zp.data_ptr(), 10, 1, None)
+                   len(sz), ocv.ctypes.data, b.data_ptr(), zp.data_ptr(), it, 1, None)
 
         plain_solve(idx[0])   # warm-up
         plain_ms = [timed(lambda i=i: plain_solve(i)) for i in idx]
-        ours_ms = [timed(lambda i=i: jobs[i]["plan"].osmom(jobs[i]["b"], jobs[i]["z"], None, 10, nonneg=True,
+        ours_ms = [timed(lambda i=i: jobs[i]["plan"].osmom(jobs[i]["b"], jobs[i]["z"], None, it, nonneg=True,
                                                             use_graph=True)) for i in idx]
-        est = ms_s * sum(plain_ms) / sum(ours_ms)
+        ours_all = ms_s if ms_s is not None else sum(ours_ms) * len(jobs) / len(idx)
+        est = ours_all * sum(plain_ms) / sum(ours_ms)
         plain = {"scans": idx, "ms_each": [round(t, 1) for t in plain_ms], "ours_ms_each": [round(t, 1) for t in ours_ms],
                  "ms_per_step_est": round(est, 1), "recon_per_s_est": round(len(jobs) * 1e3 / est, 3),
                  "speedup_batched_vs_plain": round(est / ms_b, 3),
                  "what": "reference structure re-hosted on B200 (texture filtering, per-call copies, host-synced "
                          "norms), timed on the sampled scans; all-scan time estimated by the sampled ratio"}
-    line = {"metric": "batched recon/s (OS-MOM, uneven scans)", "value": round(len(jobs) * 1e3 / ms_b, 3),
+    n = len(jobs)
+    leg = lambda ms, **kw: None if ms is None else dict(ms_per_step=round(ms, 1), recon_per_s=round(n * 1e3 / ms, 3),
+                                                         gups=round(updates / (ms * 1e-3) / 1e9, 2), **kw)
+    sset = SCAN_SETS[args.scan_sizes]
+    line = {"metric": "batched recon/s (OS-MOM, uneven scans)", "value": round(n * 1e3 / ms_b, 3),
             "unit": "recon/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_b, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{len(jobs)} uneven scans, OS-MOM 8 subsets x 10 iterations, fp32",
-                       "executor": executor, "streams": args.streams, "sizes": "multiples of 8; seeds 1000+i",
+            "config": {"workload": f"{n} uneven scans ({args.scan_sizes} set), OS-MOM 8 subsets x {it} iterations, "
+                                   "fp32",
+                       "scan_set": {k: v for k, v in sset.items()} if args.scan_sizes != "c4" else "c4 (seeds 1000+i)",
+                       "executor": executor, "streams": args.streams, "sizes": "multiples of 8",
                        "autotune": bool(args.autotune), "variants": variants or None},
             "gups": round(updates / (ms_b * 1e-3) / 1e9, 2),
-            "one_at_a_time": {"ms_per_step": round(ms_s, 1), "recon_per_s": round(len(jobs) * 1e3 / ms_s, 3),
-                              "gups": round(updates / (ms_s * 1e-3) / 1e9, 2)},
-            "stream_pool": {"ms_per_step": round(ms_p, 1), "recon_per_s": round(len(jobs) * 1e3 / ms_p, 3),
-                            "what": "one captured graph per scan, replayed on a pool of streams"},
-            "fused": {"ms_per_step": round(ms_f, 1), "recon_per_s": round(len(jobs) * 1e3 / ms_f, 3),
-                      "speedup_vs_stream_pool": round(ms_p / ms_f, 3),
-                      "what": "all scans in lockstep: one persistent work-list launch per projector kind and box "
-                              "width per subset step, one graph (build and capture timed)"},
-            "speedup_batched_vs_one_at_a_time": round(ms_s / ms_b, 3), "plain_path": plain, "clocks": clk}
+            "one_at_a_time": leg(ms_s),
+            "stream_pool": leg(ms_p, what="one captured graph per scan, replayed on a pool of streams"),
+            "fused": leg(ms_f, speedup_vs_stream_pool=round(ms_p / ms_f, 3) if ms_p else None,
+                         what="all scans in lockstep: one persistent work-list launch per projector kind and box "
+                              "width per subset step (scans that fill the GPU 16 waves keep one-scan launches), "
+                              "one graph, replayed while the call repeats"),
+            "speedup_batched_vs_one_at_a_time": round(ms_s / ms_b, 3) if ms_s else None, "plain_path": plain,
+            "clocks": clk}
     return line
 
 
@@ -1053,6 +1078,11 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
     ap.add_argument("--scans", type=int, default=64, help="c4: number of scans")
     ap.add_argument("--streams", type=int, default=8, help="c4: streams of the batch executor")
+    ap.add_argument("--scan-sizes", choices=list(SCAN_SETS), default="c4",
+                    help="c4: scan set (c4: the configuration's sizes; small/medium/tiny: smaller scans)")
+    ap.add_argument("--executor", choices=["both", "fused", "pool"], default="both",
+                    help="c4: batch executor(s) to time (one of them: no one-at-a-time leg)")
+    ap.add_argument("--iterations", type=int, default=10, help="c4: OS-MOM iterations")
     ap.add_argument("--requests", type=int, default=32, help="c5: requests in the arrival stream")
     ap.add_argument("--c3-iters", type=int, default=20, help="c3: OS-MOM iterations")
     ap.add_argument("--autotune", action="store_true", help="c4: autotune each scan's projector variants")

@@ -51,30 +51,55 @@ struct BpEpi {
 // With a mask, the operator's output is multiplied by it (apply_mask after
 // mult_MH, cuConebeamProjectionOperator.cpp:113-114), so the masked value of an
 // accumulating call is mask * (incoming + sum).
+// The epilogue of one voxel in two halves: the operands it reads (mask,
+// incoming volume, xold or z, preconditioner or V) are loaded first, so that a
+// thread can have the loads of several voxels in flight before any store.
+struct BpOps {
+  float m, v, x, a;
+};
+
 template <int EPI>
-__device__ __forceinline__ void bp_store(const BpEpi& e, size_t idx, float g) {
-  const float m = e.mask ? float(e.mask[idx]) : 1.f;
+__device__ __forceinline__ BpOps bp_load(const BpEpi& e, size_t idx) {
+  BpOps o;
+  o.m = e.mask ? float(e.mask[idx]) : 1.f;
+  o.v = (EPI == kMom || EPI == kSart || (EPI == kStore && e.accumulate)) ? e.vol[idx] : 0.f;
+  o.x = (EPI == kMom || EPI == kStep) ? e.xold[idx] : 0.f;
+  o.a = (EPI == kMom || EPI == kStep || EPI == kSart) ? e.aux[idx] : 0.f;
+  return o;
+}
+
+template <int EPI>
+__device__ __forceinline__ void bp_finish(const BpEpi& e, size_t idx, float g, const BpOps& o) {
   if (EPI == kStore) {
-    e.vol[idx] = e.scale * (((e.accumulate ? e.vol[idx] : 0.f) + g) * m);
+    e.vol[idx] = e.scale * (((e.accumulate ? o.v : 0.f) + g) * o.m);
     return;
   }
-  g *= m;
-  if (EPI == kStore) {
-  } else if (EPI == kRecip) {
+  g *= o.m;
+  if (EPI == kRecip) {
     e.vol[idx] = 1.f / fmaxf(g, 1e-6f);
   } else if (EPI == kMom) {
-    const float zt = fmaf(-e.scale, e.aux[idx] * g, e.vol[idx]);
+    const float zt = fmaf(-e.scale, o.a * g, o.v);
     const float xc = e.nonneg ? fmaxf(zt, 0.f) : zt;
-    e.vol[idx] = fmaf(-e.mom, e.xold[idx], xc * (1.f + e.mom));
+    e.vol[idx] = fmaf(-e.mom, o.x, xc * (1.f + e.mom));
     e.xold[idx] = xc;
   } else if (EPI == kStep) {
-    e.vol[idx] = fmaf(-e.scale, e.aux[idx] * g, e.xold[idx]);
+    e.vol[idx] = fmaf(-e.scale, o.a * g, o.x);
   } else {  // kSart
-    float xn = fmaf(e.scale, e.aux[idx] * g, e.vol[idx]);
+    float xn = fmaf(e.scale, o.a * g, o.v);
     if (e.nonneg) xn = fmaxf(xn, 0.f);
     e.vol[idx] = xn;
   }
 }
+
+template <int EPI>
+__device__ __forceinline__ void bp_store(const BpEpi& e, size_t idx, float g) {
+  bp_finish<EPI>(e, idx, g, bp_load<EPI>(e, idx));
+}
+
+// Voxels of a thread's z-run whose epilogue operands are loaded together.
+#ifndef CBCT_BP_EPI_CHUNK
+#define CBCT_BP_EPI_CHUNK 4
+#endif
 
 template <int EPI, bool FDK>
 __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const float* __restrict__ proj,
@@ -328,10 +353,18 @@ __device__ __forceinline__ void bp_tma_body(const CUtensorMap* map, const ViewPa
   if (i >= gc.nx || j >= gc.ny) return;
   const size_t base = ((size_t)k0 * gc.ny + j) * gc.nx + i;
   const size_t sz = (size_t)gc.nx * gc.ny;
+  const int nq = min(kZT, gc.nz - k0);
+  constexpr int C = CBCT_BP_EPI_CHUNK;
+  static_assert(kZT % C == 0, "epilogue chunks tile the z-run");
 #pragma unroll
-  for (int q = 0; q < kZT; ++q) {
-    if (k0 + q >= gc.nz) break;
-    bp_store<EPI>(e, base + q * sz, acc[q]);
+  for (int c0 = 0; c0 < kZT; c0 += C) {
+    BpOps ops[C];
+#pragma unroll
+    for (int q = 0; q < C; ++q)
+      if (c0 + q < nq) ops[q] = bp_load<EPI>(e, base + (c0 + q) * sz);
+#pragma unroll
+    for (int q = 0; q < C; ++q)
+      if (c0 + q < nq) bp_finish<EPI>(e, base + (c0 + q) * sz, acc[c0 + q], ops[q]);
   }
 }
 

@@ -583,11 +583,14 @@ def north_star_legs(args):
     """The batching and serving comparisons at reduced size, so that the
     default run carries them: the serving loop on the first 12 requests of the
     C5 stream (same seeds, kinds, storage and 20/s arrivals) with the plain
-    FP32 FIFO beside it, and the batch executor on the first 8 scans of the C4
+    FP32 FIFO beside it, the batch executors on the first 8 scans of the C4
     set against the same scans solved one at a time (and the plain path on
-    two of them).  The full runs are --config c5 and --config c4."""
+    two of them), and the batch executors on 64 smaller scans (64-128^3, the
+    "small" set), where the fused work lists merge the scans' partly idle
+    waves.  The full runs are --config c5 and --config c4."""
     import copy
-    out = {"sizes": "reduced: 12 served requests (C5 stream, seed 5), 8 batched scans (C4 seeds 1000..1007)"}
+    out = {"sizes": "reduced: 12 served requests (C5 stream, seed 5), 8 batched scans (C4 seeds 1000..1007); "
+                    "64 batched scans of the small set (seeds 3000..3063)"}
     try:
         a = copy.copy(args)
         a.requests, a.no_plain = 12, False
@@ -606,9 +609,19 @@ def north_star_legs(args):
         out["batched"]["executor"] = b["config"]["executor"]
     except Exception as e:
         out["batched"] = {"error": str(e)}
+    try:
+        a = copy.copy(args)
+        a.scans, a.steps, a.warmup, a.plain_sample, a.autotune, a.scan_sizes = 64, 1, 1, 0, False, "small"
+        b = batched_line(a)
+        out["batched_small"] = {k: b.get(k) for k in ("value", "unit", "one_at_a_time", "stream_pool", "fused",
+                                                      "speedup_batched_vs_one_at_a_time")}
+        out["batched_small"]["executor"] = b["config"]["executor"]
+    except Exception as e:
+        out["batched_small"] = {"error": str(e)}
     out["note"] = ("kernels here are bound on chip, not by HBM: 16-bit storage halves memory per request but "
-                   "adds a conversion per tap, and scans that fill the GPU gain nothing from running together; "
-                   "the ratios against the plain path come from its per-call host work and texture path")
+                   "adds a conversion per tap; scans that fill the GPU gain nothing from running together, "
+                   "smaller scans gain from the fused work lists; the ratios against the plain path come from "
+                   "its per-call host work and texture path")
     return out
 
 

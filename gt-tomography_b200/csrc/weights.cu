@@ -327,6 +327,28 @@ constexpr double cos_pi16(int m) {
 }
 
 // a * W_32^M (W_32 = exp(-2 pi i / 32)), or a * conj(W_32^M) when INV.
+// Build-time switches of the staged filter's arithmetic: complex products as
+// one paired multiply and one paired fused multiply-add (CBCT_FDK_PACKED_CMUL),
+// and the first butterfly stage of the zero-padded forward transform as
+// copies (CBCT_FDK_ZPAD_STAGE: a + 0 and a - 0 are a, but for the sign of a
+// zero input).
+#ifndef CBCT_FDK_PACKED_CMUL
+#define CBCT_FDK_PACKED_CMUL 0
+#endif
+#ifndef CBCT_FDK_ZPAD_STAGE
+#define CBCT_FDK_ZPAD_STAGE 1
+#endif
+
+// a * b as (a.x b.x, a.x b.y) + (-a.y b.y, a.y b.x), paired.
+__device__ __forceinline__ float2 cmul_p(float2 a, float2 b) {
+  const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
+}
+
+__device__ __forceinline__ float2 cmul_async(float2 a, float2 b) {
+  return CBCT_FDK_PACKED_CMUL ? cmul_p(a, b) : cmul(a, b);
+}
+
 template <int M, bool INV>
 __device__ __forceinline__ float2 tw32(float2 a) {
   static_assert(M >= 0 && M < 16, "twiddle index");
@@ -338,6 +360,7 @@ __device__ __forceinline__ float2 tw32(float2 a) {
     constexpr float c = float(M <= 8 ? cos_pi16(M) : -cos_pi16(16 - M));
     constexpr float sn = float(M <= 8 ? cos_pi16(8 - M) : cos_pi16(M - 8));   // sin(M pi / 16)
     constexpr float wi = INV ? sn : -sn;
+    if constexpr (CBCT_FDK_PACKED_CMUL) return cmul_p(a, make_float2(c, wi));
     return make_float2(fmaf(a.x, c, -a.y * wi), fmaf(a.x, wi, a.y * c));
   }
 }
@@ -368,8 +391,10 @@ __device__ __forceinline__ void dit_stages(float2 (&v)[NV]) {
   }
 }
 
-// In-register N-point DFT (N = 16 or 32), natural order in and out.
-template <int N, bool INV, int OFF, int NV>
+// In-register N-point DFT (N = 16 or 32), natural order in and out.  ZPAD:
+// the upper half of the input is zero, so after the bit-reversal every odd
+// position holds a zero and the first stage's butterflies are copies.
+template <int N, bool INV, int OFF, int NV, bool ZPAD = false>
 __device__ __forceinline__ void fft_ct(float2 (&v)[NV]) {
   constexpr int bits = N == 16 ? 4 : 5;
 #pragma unroll
@@ -381,7 +406,13 @@ __device__ __forceinline__ void fft_ct(float2 (&v)[NV]) {
       v[OFF + j] = t;
     }
   }
-  dit_stages<N, INV, OFF, NV, 2>(v);
+  if constexpr (ZPAD) {
+#pragma unroll
+    for (int i = 0; i < N; i += 2) v[OFF + i + 1] = v[OFF + i];
+    dit_stages<N, INV, OFF, NV, 4>(v);
+  } else {
+    dit_stages<N, INV, OFF, NV, 2>(v);
+  }
 }
 
 // Cosine weight evaluated in place: w(u, v) = SAD / sqrt(SAD^2 + s^2 + t^2),
@@ -551,9 +582,9 @@ __global__ void __launch_bounds__(kAsyncWarps * 32, CBCT_FDK_ASYNC_MINB) fdk_fil
       fence_proxy_async();   // the stage's reads above come before the copy that refills it
       issue(unit + kAsyncStages * nw, st);
     }
-    fft_ct<32, false, 0>(v);                             // v[k1]
+    fft_ct<32, false, 0, 32, CBCT_FDK_ZPAD_STAGE != 0>(v);   // v[k1]
 #pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul(v[k1], stw[k1 * TL + j]);
+    for (int k1 = 0; k1 < 32; ++k1) v[k1] = cmul_async(v[k1], stw[k1 * TL + j]);
 #pragma unroll
     for (int k1 = 0; k1 < 32; ++k1) buf[k1 * S + j] = v[k1];
     __syncwarp();
@@ -593,7 +624,7 @@ __global__ void __launch_bounds__(kAsyncWarps * 32, CBCT_FDK_ASYNC_MINB) fdk_fil
 #pragma unroll
     for (int k1 = 0; k1 < 32; ++k1) {
       const float2 w = stw[k1 * TL + j];
-      v[k1] = cmul(buf[k1 * S + j], make_float2(w.x, -w.y));
+      v[k1] = cmul_async(buf[k1 * S + j], make_float2(w.x, -w.y));
     }
     __syncwarp();
     fft_ct<32, true, 0>(v);                              // y[TL n1 + j] at v[n1]

@@ -1572,6 +1572,9 @@ template <int VAR>
 constexpr int var_threads() { return VAR == kVarPair ? kPairThreads : VAR == kVarQuad ? kQuadThreads : 256; }
 template <int VAR, class V>
 constexpr int var_min_blocks() {
+#ifdef CBCT_MULTI_PAIR_MINB
+  if (VAR == kVarPair) return CBCT_MULTI_PAIR_MINB;
+#endif
   return VAR == kVarPair ? pair_min_blocks<V>() : VAR == kVarQuad ? quad_min_blocks<V>() : slab_min_blocks<V>();
 }
 

@@ -570,8 +570,8 @@ def ours(args, wl: Workload):
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "GUPS", "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {e}"}
-    if rank == 0 and world == 1 and wl.name == "c2" and not args.no_north_star:
-        line["north_star"] = north_star_legs(args)
+    if rank == 0 and world == 1 and wl.name == "c2" and not args.no_legs:
+        line["batching_serving"] = batching_serving_legs(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -579,7 +579,7 @@ def ours(args, wl: Workload):
         torch.distributed.destroy_process_group()
 
 
-def north_star_legs(args):
+def batching_serving_legs(args):
     """The batching and serving comparisons at reduced size, so that the
     default run carries them: the serving loop on the first 12 requests of the
     C5 stream (same seeds, kinds, storage and 20/s arrivals) with the plain
@@ -690,7 +690,7 @@ SCAN_SETS = {
 
 
 def batched_line(args):
-    """Batched reconstruction of many uneven scans (the north star's fourth
+    """Batched reconstruction of many uneven scans (the batched
     configuration): 64 seeded scans, volumes 96..320 (z 64..320), 90..720
     views, detectors 256x192..768x576, I0 = 1e5, OS-MOM with 8 subsets x 10
     iterations, fp32.  A step solves every scan once.  Reports recon/s of the
@@ -809,7 +809,7 @@ def batched_line(args):
 
 
 def mixed_precision(args):
-    """Mixed-precision OS-MOM (the north star's third configuration): a 512^3
+    """Mixed-precision OS-MOM (the mixed-precision configuration): a 512^3
     phantom of 10 seeded ellipsoids plus 2000 small spheres (radius 0.5..2 mm,
     density up to 0.5/mm), 0.5 mm voxels (assumed), 720 views of 1024x768 at
     0.4 mm, Poisson noise at I0 = 5e4, 10 subsets x 20 iterations, positivity.
@@ -950,7 +950,7 @@ def served(args):
 
 
 def served_line(args):
-    """Serving loop (the north star's fifth configuration): Poisson arrivals
+    """Serving loop (the served configuration): Poisson arrivals
     at --rate requests/s of FDK (70 %, Hann-windowed ramp) and OS-MOM (30 %,
     8 subsets x 10 iterations, positivity) reconstructions with the batched
     configuration's scan shapes (seeds 2000+i), projections stored as
@@ -1107,7 +1107,7 @@ def main():
     ap.add_argument("--seed", type=int, default=5, help="c5: seed of kinds, storage and arrivals")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison leg")
-    ap.add_argument("--no-north-star", action="store_true",
+    ap.add_argument("--no-legs", action="store_true",
                     help="c2: skip the reduced serving and batching legs of the default line")
     ap.add_argument("--forward-kernel", choices=list(FORWARD_KERNELS), default="auto",
                     help="c1/c2: forward projector variant of the plan (auto: the plan's choice)")

@@ -5,11 +5,13 @@
 // cbct_osmom_solve with FP32 storage).  Step k of the batch is subset
 // k mod S_i of iteration k / S_i of every item that has one: one work-list
 // forward launch per projector kind and box width over all those items'
-// residuals, then one work-list back-projection per box width with the OS-MOM
-// update fused in.  The preconditioner is built the same way.  The whole
-// schedule (about 3 launches per step instead of 2 per item per step) is
-// captured in one CUDA graph.  Each CTA item runs the one-scan kernels' body,
-// so every result is bitwise the one-scan solve's.
+// residuals (after one launch for all the items' volume transposes), then one
+// work-list back-projection per box width with the OS-MOM update fused in.
+// An item whose own launch would fill the GPU for kMultiFillWaves waves keeps
+// its one-scan launch in the same schedule.  The preconditioner is built the
+// same way.  The whole schedule is captured in one CUDA graph, and the last
+// one is replayed while the calls repeat.  Each work-list item runs the
+// one-scan kernels' body, so every result is bitwise the one-scan solve's.
 #include <cmath>
 #include <map>
 #include <memory>

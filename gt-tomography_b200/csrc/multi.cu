@@ -77,8 +77,11 @@ struct FusedRun {
   }
 };
 
+// The kept schedule is replaced (and its graph and memory released) by the
+// next call with another key; the last one is left to the process's exit, so
+// no CUDA call runs from a static destructor after the runtime has gone.
 std::mutex g_fused_mu;
-std::unique_ptr<FusedRun> g_fused_last;
+FusedRun* g_fused_last = nullptr;
 
 uint64_t bits_of(float f) {
   uint32_t u;
@@ -138,8 +141,9 @@ void batch_osmom_fused(const cbct_batch_item* items, int n, cudaStream_t st) {
   }
   std::lock_guard<std::mutex> lock(g_fused_mu);
   if (!g_fused_last || g_fused_last->key != key) {
-    g_fused_last.reset();
-    g_fused_last = build_fused(S, std::move(key));
+    delete g_fused_last;
+    g_fused_last = nullptr;
+    g_fused_last = build_fused(S, std::move(key)).release();
   }
   CBCT_CUDA(cudaGraphLaunch(g_fused_last->exec, st));
   CBCT_CUDA(cudaStreamSynchronize(st));

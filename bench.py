@@ -800,9 +800,9 @@ def batched_line(args):
             "one_at_a_time": leg(ms_s),
             "stream_pool": leg(ms_p, what="one captured graph per scan, replayed on a pool of streams"),
             "fused": leg(ms_f, speedup_vs_stream_pool=round(ms_p / ms_f, 3) if ms_p and ms_f else None,
-                         what="all scans in lockstep: one persistent work-list launch per projector kind and box "
-                              "width per subset step (scans that fill the GPU 16 waves keep one-scan launches), "
-                              "one graph, replayed while the call repeats"),
+                         what="scans in two lockstep groups side by side: one persistent work-list launch per "
+                              "projector kind and box width per subset step (scans that fill the GPU 16 waves keep "
+                              "one-scan launches), one graph, replayed while the call repeats"),
             "speedup_batched_vs_one_at_a_time": round(ms_s / ms_b, 3) if ms_s else None, "plain_path": plain,
             "clocks": clk}
     return line

@@ -2,8 +2,9 @@
 // work-list launches.
 //
 // Every item is an independent osMOMSolverD reconstruction (the semantics of
-// cbct_osmom_solve with FP32 storage).  Step k of the batch is subset
-// k mod S_i of iteration k / S_i of every item that has one: one work-list
+// cbct_osmom_solve with FP32 storage).  The items are split into groups that
+// run side by side (CBCT_FUSED_BRANCHES); step k of a group is subset
+// k mod S_i of iteration k / S_i of every item of the group that has one: one work-list
 // forward launch per projector kind and box width over all those items'
 // residuals (after one launch for all the items' volume transposes), then one
 // work-list back-projection per box width with the OS-MOM update fused in.
@@ -12,7 +13,9 @@
 // same way.  The whole schedule is captured in one CUDA graph, and the last
 // one is replayed while the calls repeat.  Each work-list item runs the
 // one-scan kernels' body, so every result is bitwise the one-scan solve's.
+#include <algorithm>
 #include <cmath>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -65,17 +68,27 @@ struct ItemState {
 // buffers) with the same arrays and parameters.
 struct FusedRun {
   std::vector<uint64_t> key;
-  unsigned char* dev = nullptr;
-  cudaStream_t cap = nullptr;
+  std::vector<unsigned char*> dev;   // records and counters of each branch
+  std::vector<cudaStream_t> cap;     // capture streams, one per branch
+  std::vector<cudaEvent_t> ev;       // fork and join events of the capture
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~FusedRun() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (cap) cudaStreamDestroy(cap);
-    if (dev) cudaFree(dev);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    for (cudaStream_t c : cap) cudaStreamDestroy(c);
+    for (unsigned char* d : dev) cudaFree(d);
   }
 };
+
+// Branches of the fused schedule: the items are split into this many
+// lockstep groups (largest work first onto the least-loaded group) whose
+// schedules run side by side in the graph, so one group's launches fill the
+// SMs that the other group's launch tails leave idle.
+#ifndef CBCT_FUSED_BRANCHES
+#define CBCT_FUSED_BRANCHES 2
+#endif
 
 // The kept schedule is replaced (and its graph and memory released) by the
 // next call with another key; the last one is left to the process's exit, so
@@ -165,12 +178,10 @@ void batch_osmom_fused(const cbct_batch_item* items, int n, cudaStream_t st) {
 
 namespace {
 
-// The fused schedule of the items, captured and instantiated.
-std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uint64_t>&& key) {
-#ifdef CBCT_SETUP_TIMING
-  const auto t0 = std::chrono::steady_clock::now();
-#endif
-  WorkArena A;
+// Lockstep schedule of one group of items, appended to A.
+void schedule(WorkArena& A, std::vector<ItemState*>& group) {
+  std::vector<std::reference_wrapper<ItemState>> S;
+  for (ItemState* p : group) S.push_back(*p);
   A.ops.push_back([&A](cudaStream_t cs) {
     CBCT_CUDA(cudaMemsetAsync(A.dev + A.counters_offset(), 0, sizeof(int) * (size_t)std::max(A.n_counters, 1), cs));
   });
@@ -234,7 +245,38 @@ std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uin
     forward_multi(A, fj);
     backproject_multi(A, 1, bj);
   }
+}
 
+// Work of one reconstruction: forward samples + voxel-view updates.
+double item_work(const ItemState& s) {
+  const cbct_geometry& g = s.p->g;
+  const double passes = s.it->params.iterations + 1.0;
+  return passes * (double(g.width) * g.height * s.p->n_views * s.p->gc.N + double(s.nv) * s.p->n_views);
+}
+
+// The fused schedule of the items, captured and instantiated.
+std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uint64_t>&& key) {
+#ifdef CBCT_SETUP_TIMING
+  const auto t0 = std::chrono::steady_clock::now();
+#endif
+  const int nb = std::max(1, std::min<int>(CBCT_FUSED_BRANCHES, (int)S.size()));
+  std::vector<int> order(S.size());
+  for (size_t i = 0; i < S.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_work(S[a]) > item_work(S[b]); });
+  std::vector<double> load(nb, 0.0);
+  std::vector<std::vector<int>> idx(nb);
+  for (int i : order) {
+    const int b = int(std::min_element(load.begin(), load.end()) - load.begin());
+    load[b] += item_work(S[i]);
+    idx[b].push_back(i);
+  }
+  std::vector<WorkArena> A(nb);
+  for (int b = 0; b < nb; ++b) {
+    std::sort(idx[b].begin(), idx[b].end());
+    std::vector<ItemState*> group;
+    for (int i : idx[b]) group.push_back(&S[i]);
+    schedule(A[b], group);
+  }
 #ifdef CBCT_SETUP_TIMING
   // Build-time switch: host phases of the call on stderr.
   auto now = [] { return std::chrono::steady_clock::now(); };
@@ -243,24 +285,41 @@ std::unique_ptr<FusedRun> build_fused(std::vector<ItemState>& S, std::vector<uin
 #endif
   auto run = std::make_unique<FusedRun>();
   run->key = std::move(key);
-  CBCT_CUDA(cudaMalloc(&run->dev, A.bytes()));
-  A.dev = run->dev;
-  if (!A.host.empty()) CBCT_CUDA(cudaMemcpy(run->dev, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
-  CBCT_CUDA(cudaStreamCreateWithFlags(&run->cap, cudaStreamNonBlocking));
-  CBCT_CUDA(cudaStreamBeginCapture(run->cap, cudaStreamCaptureModeThreadLocal));
+  run->dev.assign(nb, nullptr);
+  run->cap.assign(nb, nullptr);
+  run->ev.assign(nb, nullptr);
+  for (int b = 0; b < nb; ++b) {
+    CBCT_CUDA(cudaMalloc(&run->dev[b], A[b].bytes()));
+    A[b].dev = run->dev[b];
+    if (!A[b].host.empty())
+      CBCT_CUDA(cudaMemcpy(run->dev[b], A[b].host.data(), A[b].host.size(), cudaMemcpyHostToDevice));
+    CBCT_CUDA(cudaStreamCreateWithFlags(&run->cap[b], cudaStreamNonBlocking));
+    CBCT_CUDA(cudaEventCreateWithFlags(&run->ev[b], cudaEventDisableTiming));
+  }
+  // Branch 0's stream starts the capture; the others fork from it and join
+  // it at the end.
+  CBCT_CUDA(cudaStreamBeginCapture(run->cap[0], cudaStreamCaptureModeThreadLocal));
   try {
-    for (auto& op : A.ops) op(run->cap);
+    CBCT_CUDA(cudaEventRecord(run->ev[0], run->cap[0]));
+    for (int b = 1; b < nb; ++b) CBCT_CUDA(cudaStreamWaitEvent(run->cap[b], run->ev[0], 0));
+    for (int b = 0; b < nb; ++b)
+      for (auto& op : A[b].ops) op(run->cap[b]);
+    for (int b = 1; b < nb; ++b) {
+      CBCT_CUDA(cudaEventRecord(run->ev[b], run->cap[b]));
+      CBCT_CUDA(cudaStreamWaitEvent(run->cap[0], run->ev[b], 0));
+    }
   } catch (...) {
-    cudaStreamEndCapture(run->cap, &run->graph);
+    cudaStreamEndCapture(run->cap[0], &run->graph);
     throw;
   }
-  CBCT_CUDA(cudaStreamEndCapture(run->cap, &run->graph));
+  CBCT_CUDA(cudaStreamEndCapture(run->cap[0], &run->graph));
   CBCT_CUDA(cudaGraphInstantiate(&run->exec, run->graph, 0));
 #ifdef CBCT_SETUP_TIMING
-  size_t nodes = 0;
+  size_t nodes = 0, bytes = 0;
   cudaGraphGetNodes(run->graph, nullptr, &nodes);
+  for (auto& a : A) bytes += a.host.size();
   std::fprintf(stderr, "fused: schedule %.1f ms, upload+capture+instantiate %.1f ms (%zu nodes, %zu record bytes)\n",
-               ms(t0, t1), ms(t1, now()), nodes, A.host.size());
+               ms(t0, t1), ms(t1, now()), nodes, bytes);
 #endif
   return run;
 }

@@ -469,9 +469,9 @@ def batch_osmom(jobs, n_streams=8, stream=None, fused=False):
     is bitwise identical to solving that job alone.  Starts after the work on
     the current stream and returns when every job has finished.
 
-    fused=True advances the jobs in lockstep through persistent work-list
-    launches captured in one graph (cbct_batch_osmom_fused; fp32 volume
-    storage); n_streams is then unused."""
+    fused=True advances the jobs in two lockstep groups through persistent
+    work-list launches captured in one graph (cbct_batch_osmom_fused; fp32
+    volume storage); n_streams is then unused."""
     items = (L.CbctBatchItem * len(jobs))()
     for i, j in enumerate(jobs):
         prm = L.CbctSolverParams(int(j.get("iterations", 10)), float(j.get("beta", 1.0)), float(j.get("gamma", 0.0)),

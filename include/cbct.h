@@ -460,9 +460,10 @@ typedef struct {
  * No counterpart in the reference (its drivers reconstruct one scan per process). */
 CBCT_API cbct_status cbct_batch_osmom(const cbct_batch_item* items, int32_t n, int32_t n_streams, void* stream);
 
-/* The same reconstructions advanced in lockstep through work-list launches:
- * step k runs subset k mod S_i of iteration k / S_i of every item that has
- * one.  A step is one persistent forward launch per projector kind and box
+/* The same reconstructions advanced in lockstep through work-list launches,
+ * the items split into two groups of about equal work whose schedules run
+ * side by side: step k of a group runs subset k mod S_i of iteration k / S_i
+ * of every item of the group that has one.  A step is one persistent forward launch per projector kind and box
  * width and one persistent back-projection (OS-MOM update fused) per box width
  * over all those items; resident CTAs take (scan, tile) items from a counter
  * until the list is empty.  The whole schedule, preconditioner included, is
